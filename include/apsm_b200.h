@@ -1,0 +1,116 @@
+/*
+ * apsm_b200 — B200 (sm_100a) APSM multiuser detector, C ABI.
+ *
+ * This is the drop-in boundary for the reference's detector API
+ * (fraunhoferhhi/libapsm, cpp/lib/noma/noma_detector.cuh:65-75).  All entry
+ * points take plain pointers and sizes; no C++ or torch types cross it.
+ *
+ * Sample layout (identical to the reference's ComplexSampleMatrix /
+ * ComplexSampleVector, cpp/lib/noma/types.cuh:95-100, flattened):
+ *   rx  : num_antennas x n complex64, antenna-major:  rx[2*(a*n + i) + {0:re, 1:im}]
+ *   tx  : P complex64 pilots per user, user-major for multi-user calls
+ *   est : S complex64 estimates per user, user-major for multi-user calls
+ *
+ * Threading: a handle is not thread-safe (as the reference detector); distinct
+ * handles may be used from distinct host threads.  Every call that takes host
+ * buffers returns after the GPU work finished (the reference's calls are
+ * synchronous too: CUDA_EventTimer::elapsed syncs, cpp/lib/cuda/cuda_eventtimer.cuh:121-128).
+ * The library never calls exit(); every failure is a status code plus a message.
+ */
+#ifndef APSM_B200_H
+#define APSM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    APSM_OK = 0,
+    APSM_ERR_INVALID_ARGUMENT = 1, /* bad pointer / size / shape (reference: std::invalid_argument or assert) */
+    APSM_ERR_INVALID_CONFIG = 2,   /* JSON config rejected (reference: std::invalid_argument from the factory) */
+    APSM_ERR_CUDA = 3,             /* CUDA runtime error (reference: CUDA_CHECK prints and exits, cuda_errorhandling.cuh:98-108) */
+    APSM_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed or would exceed the handle's memory budget */
+    APSM_ERR_UNSUPPORTED = 5,      /* valid config the B200 kernels do not implement (e.g. antenna count above the maximum) */
+    APSM_ERR_NO_DEVICE = 6         /* no usable sm_100 device */
+} apsm_status;
+
+typedef struct apsm_detector apsm_detector;
+
+/* Library version string and the device the handle runs on. */
+const char* apsm_version(void);
+
+/*
+ * Create a detector from the reference's algorithm JSON object, e.g.
+ *   {"otype":"APSM","windowSize":80,"gaussianKernelVariance":0.5,"eB":0.01}
+ * Replaces NomaDetectorFactory::build (cpp/lib/noma/noma_detector_factory.cu:57-65)
+ * and ApsmNomaDetectorFactory::build (cpp/lib/apsm/apsm_noma_detector.cu:348-383):
+ * same keys, defaults and strict key check ("Invalid key: <k>",
+ * "Unknown detect version: <v>", "Unknown algorithm: <otype>").
+ * As the reference constructor does (apsm_noma_detector.cu:79-80), a non-zero
+ * gaussianKernelVariance is multiplied by num_antennas^2.
+ * Extensions (accepted in addition to the reference's keys):
+ *   "detectVersion": "gram_bf16" | "gram_bf16x3" | "gram_tf32" | "gram_tf32x3"
+ *        tensor-core Gram detection (tcgen05); the reference's four values
+ *        ("original","oldfast","shmem","balanced") select the exact FP32 kernel.
+ * num_users: detectors that share the same received signal (one per user of
+ *   a cell, the reference CLI's -p mode, cpp/cli/detect/noma_detect.cpp:100-121);
+ *   1 gives the reference's single-user NomaDetector.
+ * err/errlen receive the message on failure (may be NULL/0).
+ */
+apsm_status apsm_create(const char* algorithm_json, uint32_t num_antennas, uint32_t num_users,
+                        apsm_detector** out, char* err, size_t errlen);
+
+/* Destroy the handle and free its device memory (reference dtor, apsm_noma_detector.cu:83-87). */
+void apsm_destroy(apsm_detector* h);
+
+/*
+ * Online training on P pilots: NomaDetector::train (noma_detector.cuh:67;
+ * apsm_noma_detector.cu:95-128 -> apsm_train.cu:80-166).
+ * rx: N x P complex, tx: num_users x P complex.  Pilots append to the
+ * detector's dictionary (capacity dictionarySize complex entries).
+ * *ms (optional) receives the GPU time of the training work (CUDA events).
+ */
+apsm_status apsm_train(apsm_detector* h, const float* rx, const float* tx, uint32_t P, float* ms);
+
+/*
+ * Detection of S data symbols: NomaDetector::detect (noma_detector.cuh:70;
+ * apsm_noma_detector.cu:130-143 -> apsm_detect.cu:948-992).
+ * rx: N x S complex, est: num_users x S complex (written).
+ */
+apsm_status apsm_detect(apsm_detector* h, const float* rx, uint32_t S, float* est, float* ms);
+
+/* NomaDetector::resetState (noma_detector.cuh:73; apsm_noma_detector.cu:89-93). */
+apsm_status apsm_reset(apsm_detector* h);
+
+/*
+ * Device-resident variants: the same work on buffers already in HBM, enqueued
+ * on `stream` (a cudaStream_t, NULL = the handle's own stream) without a host
+ * synchronisation.  Layouts as above.  No counterpart in the reference (its
+ * train/detect always copy host vectors in, cuda_matrix_host.cu:105-149).
+ */
+apsm_status apsm_train_device(apsm_detector* h, const float* d_rx, const float* d_tx, uint32_t P, void* stream);
+apsm_status apsm_detect_device(apsm_detector* h, const float* d_rx, uint32_t S, float* d_est, void* stream);
+
+/* The handle's CUDA stream (cudaStream_t) and a blocking wait on it. */
+void* apsm_stream(apsm_detector* h);
+apsm_status apsm_synchronize(apsm_detector* h);
+
+/*
+ * Model snapshot (reference: getTrainingState, apsm_noma_detector.cuh:93):
+ * rows = 2 x (complex dictionary entries in use); dict rows x 2N (Dedup real
+ * rows, oldest first), a: num_users x rows, w: num_users x 2N.  Any pointer may
+ * be NULL.  apsm_rows returns the current row count.
+ */
+uint32_t apsm_rows(const apsm_detector* h);
+apsm_status apsm_get_state(apsm_detector* h, float* dict, float* a, float* w);
+
+/* Last error message of the handle ("" if none). */
+const char* apsm_last_error(const apsm_detector* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* APSM_B200_H */

@@ -1,0 +1,73 @@
+"""ctypes binding of libapsm_b200.so (the C ABI of include/apsm_b200.h).
+
+The library is built in-tree by ``python -m libapsm_b200.build``.  There is no
+fallback: if the shared library is missing or fails to load, every detector
+call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libapsm_b200.so"
+
+APSM_OK = 0
+APSM_ERR_INVALID_ARGUMENT = 1
+APSM_ERR_INVALID_CONFIG = 2
+APSM_ERR_CUDA = 3
+APSM_ERR_OUT_OF_MEMORY = 4
+APSM_ERR_UNSUPPORTED = 5
+APSM_ERR_NO_DEVICE = 6
+
+STATUS_NAMES = {
+    APSM_OK: "APSM_OK",
+    APSM_ERR_INVALID_ARGUMENT: "APSM_ERR_INVALID_ARGUMENT",
+    APSM_ERR_INVALID_CONFIG: "APSM_ERR_INVALID_CONFIG",
+    APSM_ERR_CUDA: "APSM_ERR_CUDA",
+    APSM_ERR_OUT_OF_MEMORY: "APSM_ERR_OUT_OF_MEMORY",
+    APSM_ERR_UNSUPPORTED: "APSM_ERR_UNSUPPORTED",
+    APSM_ERR_NO_DEVICE: "APSM_ERR_NO_DEVICE",
+}
+
+# (name, restype, argtypes) of every exported entry point
+_P = ctypes.c_void_p
+_F = ctypes.POINTER(ctypes.c_float)
+_U32 = ctypes.c_uint32
+SIGNATURES = [
+    ("apsm_version", ctypes.c_char_p, []),
+    ("apsm_create", ctypes.c_int, [ctypes.c_char_p, _U32, _U32, ctypes.POINTER(_P), ctypes.c_char_p, ctypes.c_size_t]),
+    ("apsm_destroy", None, [_P]),
+    ("apsm_train", ctypes.c_int, [_P, _P, _P, _U32, _F]),
+    ("apsm_detect", ctypes.c_int, [_P, _P, _U32, _P, _F]),
+    ("apsm_reset", ctypes.c_int, [_P]),
+    ("apsm_train_device", ctypes.c_int, [_P, _P, _P, _U32, _P]),
+    ("apsm_detect_device", ctypes.c_int, [_P, _P, _U32, _P, _P]),
+    ("apsm_stream", _P, [_P]),
+    ("apsm_synchronize", ctypes.c_int, [_P]),
+    ("apsm_rows", _U32, [_P]),
+    ("apsm_get_state", ctypes.c_int, [_P, _P, _P, _P]),
+    ("apsm_last_error", ctypes.c_char_p, [_P]),
+]
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load() -> ctypes.CDLL:
+    """Load (once) and return the native library; raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"native library {LIB_PATH} is missing; build it with `python -m libapsm_b200.build`"
+            )
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib

@@ -1,0 +1,358 @@
+// apsm_detector: device state and the train / detect call sequences.
+#include "apsm_host.hpp"
+#include "apsm_kernels.cuh"
+#include "apsm_gram.cuh"
+
+#include <algorithm>
+#include <cstdlib>
+#include <string>
+
+using namespace apsm;
+
+namespace {
+
+uint32_t pow2_at_least(uint32_t x)
+{
+    uint32_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+int env_int(const char* name, int dflt)
+{
+    const char* v = std::getenv(name);
+    return v ? std::atoi(v) : dflt;
+}
+
+} // namespace
+
+#define APSM_CK(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);                            \
+    } while (0)
+
+apsm_status apsm_detector::cuda_fail(cudaError_t e, const char* what)
+{
+    cudaGetLastError(); // clear a non-sticky error
+    last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? APSM_ERR_OUT_OF_MEMORY : APSM_ERR_CUDA;
+}
+
+apsm_detector::~apsm_detector()
+{
+    if (stream) cudaStreamSynchronize(stream);
+    gram_workspace_free(gram);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+ModelParams apsm_detector::model_params() const
+{
+    ModelParams mp;
+    mp.wL = cfg.wL;
+    mp.wG = cfg.wG;
+    mp.ew = -0.5f / variance_eff;
+    mp.eB = cfg.eB;
+    return mp;
+}
+
+apsm_status apsm_detector::init(const Config& c, uint32_t num_antennas, uint32_t num_users)
+{
+    cfg = c;
+    N = num_antennas;
+    D = 2 * N;
+    Dp = row_pitch(D);
+    U = num_users;
+    if (cfg.otype != "APSM") {
+        last_error = "LLS detector is not available in this build";
+        return APSM_ERR_UNSUPPORTED;
+    }
+    if (cfg.lls_init) {
+        last_error = "llsInitialization is not available in this build";
+        return APSM_ERR_UNSUPPORTED;
+    }
+    if (cfg.norm_constraint > 0.f) {
+        last_error = "normConstraint > 0 is not available in this build";
+        return APSM_ERR_UNSUPPORTED;
+    }
+    cap = 2 * cfg.dict_size;
+    // ApsmNomaDetector constructor (apsm_noma_detector.cu:79-80)
+    variance_eff = cfg.variance;
+    if (variance_eff != 0) variance_eff *= float(N * N);
+
+    APSM_CK(cudaGetDevice(&device));
+    cudaDeviceProp prop;
+    APSM_CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) {
+        last_error = "an sm_100 (Blackwell) device is required, found sm_" + std::to_string(prop.major) +
+                     std::to_string(prop.minor);
+        return APSM_ERR_NO_DEVICE;
+    }
+    APSM_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    APSM_CK(cudaEventCreate(&ev0));
+    APSM_CK(cudaEventCreate(&ev1));
+    APSM_CK(dict_X.ensure(size_t(cap) * Dp));
+    APSM_CK(dict_nrm.ensure(cap));
+    APSM_CK(dict_y.ensure(size_t(U) * cap));
+    APSM_CK(dict_a.ensure(size_t(U) * cap));
+    APSM_CK(w.ensure(size_t(U) * D));
+    cluster = env_int("APSM_TRAIN_CLUSTER", 16);
+    return reset();
+}
+
+apsm_status apsm_detector::reset()
+{
+    // resetState (apsm_noma_detector.cu:89-93): fresh, zeroed training state
+    APSM_CK(cudaStreamSynchronize(stream));
+    used = 0;
+    APSM_CK(cudaMemsetAsync(dict_a.p, 0, sizeof(float) * size_t(U) * cap, stream));
+    APSM_CK(cudaMemsetAsync(w.p, 0, sizeof(float) * size_t(U) * D, stream));
+    APSM_CK(cudaStreamSynchronize(stream));
+    return APSM_OK;
+}
+
+apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_t P, cudaStream_t s, float* ms)
+{
+    if (variance_eff == 0.f) {
+        // the reference computes the heuristic on the host from the pilots
+        std::vector<float2> h_rx(size_t(N) * P);
+        APSM_CK(cudaMemcpyAsync(h_rx.data(), d_rx, sizeof(float2) * h_rx.size(), cudaMemcpyDeviceToHost, s));
+        APSM_CK(cudaStreamSynchronize(s));
+        std::vector<float2> shuffled = h_rx;
+        if (cfg.shuffle) {
+            std::vector<int> pm = shuffle_permutation(P);
+            for (uint32_t a = 0; a < N; ++a)
+                for (uint32_t i = 0; i < P; ++i) shuffled[size_t(a) * P + i] = h_rx[size_t(a) * P + pm[i]];
+        }
+        variance_eff = variance_heuristic(shuffled.data(), N, P);
+        if (!(variance_eff > 0.f)) {
+            last_error = "Gaussian variance heuristic produced a non-positive variance";
+            return APSM_ERR_INVALID_ARGUMENT;
+        }
+    }
+    const ModelParams mp = model_params();
+    const uint32_t rows_new = 2 * P;
+    const uint32_t nU = used + rows_new;
+    const uint32_t q2 = 2 * cfg.window;
+
+    int final_hi = 0;
+    std::vector<TrainStep> h_steps = build_schedule(cfg, used, P, cap, &final_hi);
+
+    APSM_CK(uX.ensure(size_t(nU) * Dp));
+    APSM_CK(unrm.ensure(nU));
+    APSM_CK(uy.ensure(size_t(U) * nU));
+    APSM_CK(ua.ensure(size_t(U) * nU));
+
+    const int* d_perm = nullptr;
+    if (cfg.shuffle) {
+        std::vector<int> pm = shuffle_permutation(P);
+        APSM_CK(perm.ensure(P));
+        APSM_CK(cudaMemcpyAsync(perm.p, pm.data(), sizeof(int) * P, cudaMemcpyHostToDevice, s));
+        APSM_CK(cudaStreamSynchronize(s)); // pm is a local
+        d_perm = perm.p;
+    }
+
+    // universe = dictionary rows already present, then the new pilots
+    if (used > 0) {
+        APSM_CK(cudaMemcpyAsync(uX.p, dict_X.p, sizeof(float) * size_t(used) * Dp, cudaMemcpyDeviceToDevice, s));
+        APSM_CK(cudaMemcpyAsync(unrm.p, dict_nrm.p, sizeof(float) * used, cudaMemcpyDeviceToDevice, s));
+        APSM_CK(cudaMemcpy2DAsync(uy.p, sizeof(float) * nU, dict_y.p, sizeof(float) * cap, sizeof(float) * used, U,
+                                  cudaMemcpyDeviceToDevice, s));
+        APSM_CK(cudaMemcpy2DAsync(ua.p, sizeof(float) * nU, dict_a.p, sizeof(float) * cap, sizeof(float) * used, U,
+                                  cudaMemcpyDeviceToDevice, s));
+    }
+    APSM_CK(cudaMemset2DAsync(ua.p + used, sizeof(float) * nU, 0, sizeof(float) * rows_new, U, s));
+    {
+        dim3 grid((P + kPackSamples - 1) / kPackSamples);
+        size_t sm = sizeof(float2) * N * kPackSamples;
+        pack_rows_kernel<<<grid, 256, sm, s>>>(d_rx, int(N), int(P), d_perm, uX.p, int(Dp), int(used), unrm.p);
+        APSM_CK(cudaGetLastError());
+        int nt = int(P * U);
+        gather_targets_kernel<<<(nt + 255) / 256, 256, 0, s>>>(d_tx, int(P), int(U), d_perm, uy.p, nU, int(used));
+        APSM_CK(cudaGetLastError());
+    }
+
+    APSM_CK(cudaEventRecord(ev0, s));
+    if (!h_steps.empty()) {
+        const int T = int(h_steps.size());
+        int v_first = h_steps[0].hi - h_steps[0].wk;
+        for (const auto& st : h_steps) v_first = std::min(v_first, st.hi - st.wk);
+        const int nV = int(nU) - v_first;
+        // longest kernel column (rows column_base(v) .. min(nU, v + q2), 16-byte multiple)
+        int Lk = 4;
+        for (int v = v_first; v < int(nU); ++v) {
+            int len = int(round_up(uint32_t(std::min<int>(int(nU), v + int(q2))), 4u)) - column_base(v, int(cap));
+            Lk = std::max(Lk, len);
+        }
+        // rows in flight at once: window of step t-1 up to the rows fetched for t + kLookahead
+        int span = 1, max_reveal = 0;
+        for (int t = 0; t < T; ++t) {
+            const int tp = std::max(0, t - 1), tn = std::min(T - 1, t + kLookahead);
+            span = std::max(span, h_steps[tn].hi - (h_steps[tp].hi - h_steps[tp].wk));
+            max_reveal = std::max(max_reveal, h_steps[t].hi - h_steps[t].reveal_lo);
+        }
+        APSM_CK(K.ensure(size_t(nV) * Lk));
+        APSM_CK(steps.ensure(h_steps.size()));
+        APSM_CK(cudaMemcpyAsync(steps.p, h_steps.data(), sizeof(TrainStep) * h_steps.size(), cudaMemcpyHostToDevice, s));
+        {
+            dim3 grid((Lk + 255) / 256, (nV + kGramColsPerBlock - 1) / kGramColsPerBlock);
+            gram_columns_kernel<<<grid, 256, 0, s>>>(uX.p, int(Dp), int(D), int(nU), v_first, nV, Lk, int(cap), mp, K.p);
+            APSM_CK(cudaGetLastError());
+        }
+        TrainArgs ta;
+        ta.X = uX.p;
+        ta.nrm = unrm.p;
+        ta.y = uy.p;
+        ta.a = ua.p;
+        ta.w = w.p;
+        ta.K = K.p;
+        ta.steps = steps.p;
+        ta.n_steps = T;
+        ta.nU = int(nU);
+        ta.D = int(D);
+        ta.Dp = int(Dp);
+        ta.cap = int(cap);
+        ta.q2 = int(q2);
+        ta.Lk = Lk;
+        ta.Lc = Lk;
+        ta.v_first = v_first;
+        ta.A_ring = int(pow2_at_least(cap + uint32_t(max_reveal) + 1));
+        ta.XW = int(pow2_at_least(uint32_t(span) + 1));
+        ta.used_before = int(used);
+        ta.final_hi = final_hi;
+        ta.y_stride = nU;
+        ta.a_stride = nU;
+        ta.mp = mp;
+
+        // launch shape: the largest cluster whose CTAs can hold their kernel columns
+        auto shape = [&](int C, bool staged, int* nwarps_out, int* ns_out) -> size_t {
+            int nwarps = std::max({(int(q2) + C - 1) / C, (int(D) * kWGroups + 31) / 32, 4});
+            int ns = staged ? ta.XW / C + 2 : 0;
+            *nwarps_out = nwarps;
+            *ns_out = ns;
+            return sizeof(float) * (size_t(ta.XW) * Dp + size_t(ns) * Lk + size_t(ta.A_ring) + kMaxFeatures + 2 * q2 +
+                                    size_t(nwarps) * 32 + 2 * size_t(ta.XW));
+        };
+        const size_t smem_limit = 227 * 1024;
+        int C = 16, nwarps = 0, ns = 0;
+        bool staged = true;
+        if (cluster > 0) C = std::min(16, cluster);
+        size_t smem = shape(C, true, &nwarps, &ns);
+        if (smem > smem_limit || nwarps > 32) {
+            staged = false;
+            smem = shape(C, false, &nwarps, &ns);
+        }
+        if (smem > smem_limit || nwarps > 32) {
+            last_error = "training kernel does not fit one cluster (window " + std::to_string(q2) +
+                         " rows, dictionary " + std::to_string(cap) + " rows)";
+            return APSM_ERR_UNSUPPORTED;
+        }
+        ta.NS = ns;
+        ta.users = int(U);
+        ta.prof = prof_buffer;
+        int max_clusters = 0;
+        APSM_CK(launch_train_exact(staged, C, nwarps * 32, smem, s, ta, &max_clusters));
+        if (max_clusters < 1) {
+            last_error = "training cluster of " + std::to_string(C) + " CTAs cannot be scheduled";
+            return APSM_ERR_UNSUPPORTED;
+        }
+        last_train_cluster = C;
+        last_train_staged = staged;
+    }
+    APSM_CK(cudaEventRecord(ev1, s));
+
+    // the dictionary after the sweep is the last min(final_hi, cap) universe rows
+    const uint32_t used_new = std::min<uint32_t>(uint32_t(final_hi), cap);
+    const uint32_t lo = uint32_t(final_hi) - used_new;
+    if (used_new > 0) {
+        APSM_CK(cudaMemcpyAsync(dict_X.p, uX.p + size_t(lo) * Dp, sizeof(float) * size_t(used_new) * Dp,
+                                cudaMemcpyDeviceToDevice, s));
+        APSM_CK(cudaMemcpyAsync(dict_nrm.p, unrm.p + lo, sizeof(float) * used_new, cudaMemcpyDeviceToDevice, s));
+        APSM_CK(cudaMemcpy2DAsync(dict_y.p, sizeof(float) * cap, uy.p + lo, sizeof(float) * nU, sizeof(float) * used_new,
+                                  U, cudaMemcpyDeviceToDevice, s));
+        APSM_CK(cudaMemcpy2DAsync(dict_a.p, sizeof(float) * cap, ua.p + lo, sizeof(float) * nU, sizeof(float) * used_new,
+                                  U, cudaMemcpyDeviceToDevice, s));
+    }
+    used = used_new;
+    if (ms) {
+        APSM_CK(cudaEventSynchronize(ev1));
+        APSM_CK(cudaEventElapsedTime(ms, ev0, ev1));
+    }
+    return APSM_OK;
+}
+
+apsm_status apsm_detector::detect(const float2* d_rx, uint32_t S, float2* d_est, cudaStream_t s)
+{
+    const uint32_t ns = 2 * S;
+    APSM_CK(xs.ensure(size_t(ns) * Dp));
+    {
+        dim3 grid((S + kPackSamples - 1) / kPackSamples);
+        size_t sm = sizeof(float2) * N * kPackSamples;
+        pack_rows_kernel<<<grid, 256, sm, s>>>(d_rx, int(N), int(S), nullptr, xs.p, int(Dp), 0, nullptr);
+        APSM_CK(cudaGetLastError());
+    }
+    if (cfg.detect_mode == DetectMode::Exact) {
+        DetectArgs da;
+        da.Xs = xs.p;
+        da.n_samples = int(ns);
+        da.Dp = int(Dp);
+        da.D = int(D);
+        da.dict = dict_X.p;
+        da.M = int(used);
+        da.a = dict_a.p;
+        da.a_stride = cap;
+        da.w = w.p;
+        da.users = int(U);
+        da.mp = model_params();
+        da.out = reinterpret_cast<float*>(d_est);
+        da.out_stride = ns;
+        launch_detect_exact(da, s);
+        APSM_CK(cudaGetLastError());
+        return APSM_OK;
+    }
+    return detect_gram(this, S, reinterpret_cast<float*>(d_est), s);
+}
+
+apsm_status apsm_detector::train_host(const float2* rx, const float2* tx, uint32_t P, float* ms)
+{
+    APSM_CK(rx_stage.ensure(size_t(N) * P));
+    APSM_CK(tx_stage.ensure(size_t(U) * P));
+    APSM_CK(cudaMemcpyAsync(rx_stage.p, rx, sizeof(float2) * size_t(N) * P, cudaMemcpyHostToDevice, stream));
+    APSM_CK(cudaMemcpyAsync(tx_stage.p, tx, sizeof(float2) * size_t(U) * P, cudaMemcpyHostToDevice, stream));
+    float t = 0.f;
+    apsm_status st = train(rx_stage.p, tx_stage.p, P, stream, &t);
+    if (st != APSM_OK) return st;
+    APSM_CK(cudaStreamSynchronize(stream));
+    if (ms) *ms = t;
+    return APSM_OK;
+}
+
+apsm_status apsm_detector::detect_host(const float2* rx, uint32_t S, float2* est, float* ms)
+{
+    APSM_CK(rx_stage.ensure(size_t(N) * S));
+    APSM_CK(est_stage.ensure(size_t(U) * S));
+    APSM_CK(cudaMemcpyAsync(rx_stage.p, rx, sizeof(float2) * size_t(N) * S, cudaMemcpyHostToDevice, stream));
+    APSM_CK(cudaEventRecord(ev0, stream));
+    apsm_status st = detect(rx_stage.p, S, est_stage.p, stream);
+    if (st != APSM_OK) return st;
+    APSM_CK(cudaEventRecord(ev1, stream));
+    APSM_CK(cudaMemcpyAsync(est, est_stage.p, sizeof(float2) * size_t(U) * S, cudaMemcpyDeviceToHost, stream));
+    APSM_CK(cudaStreamSynchronize(stream));
+    if (ms) APSM_CK(cudaEventElapsedTime(ms, ev0, ev1));
+    return APSM_OK;
+}
+
+apsm_status apsm_detector::get_state(float* dict, float* a_out, float* w_out)
+{
+    APSM_CK(cudaStreamSynchronize(stream));
+    if (dict && used > 0)
+        APSM_CK(cudaMemcpy2D(dict, sizeof(float) * D, dict_X.p, sizeof(float) * Dp, sizeof(float) * D, used,
+                             cudaMemcpyDeviceToHost));
+    if (a_out && used > 0)
+        APSM_CK(cudaMemcpy2D(a_out, sizeof(float) * used, dict_a.p, sizeof(float) * cap, sizeof(float) * used, U,
+                             cudaMemcpyDeviceToHost));
+    if (w_out) APSM_CK(cudaMemcpy(w_out, w.p, sizeof(float) * size_t(U) * D, cudaMemcpyDeviceToHost));
+    return APSM_OK;
+}

@@ -1,0 +1,75 @@
+// Kernel declarations and launch-argument structs of the B200 APSM library.
+#pragma once
+
+#include "apsm_common.cuh"
+
+namespace apsm {
+
+constexpr int kPackSamples = 64;     // complex samples per pack_rows_kernel block
+constexpr int kGramColsPerBlock = 8; // kernel columns per gram_columns_kernel block
+constexpr int kLookahead = 2;        // training steps fetched ahead by cp.async
+
+// First universe row stored in kernel column v (16-byte aligned).
+__host__ __device__ inline int column_base(int v, int cap)
+{
+    const int lo = v + 1 - cap;
+    return lo > 0 ? (lo & ~3) : 0;
+}
+
+struct TrainArgs {
+    const float* X;         // universe rows nU x Dp (old dictionary rows, then the new pilots)
+    const float* nrm;       // nU squared row norms
+    const float* y;         // users x y_stride targets
+    float* a;               // users x a_stride coefficients (in: old rows; out: visible rows)
+    float* w;               // users x D linear weights (in/out)
+    const float* K;         // nV x Lk kernel columns (gram_columns_kernel), column v starts at row column_base(v)
+    const TrainStep* steps; // n_steps
+    int n_steps;
+    int nU, D, Dp, cap, q2, Lk, v_first;
+    int A_ring, XW;         // power-of-two ring sizes (coefficients, window rows)
+    int NS, Lc;             // staged kernel columns per CTA and their length (floats)
+    int used_before;        // rows present before this call
+    int final_hi;           // visible end after the last step
+    size_t y_stride, a_stride;
+    int users;
+    ModelParams mp;
+    unsigned long long* prof; // phase timestamps (profiling builds only), kProfSteps x kProfMarks
+};
+
+constexpr int kProfSteps = 4096;
+constexpr int kProfMarks = 8;
+
+__global__ void pack_rows_kernel(const float2* __restrict__ rx, int num_ant, int n_total, const int* __restrict__ perm,
+                                 float* __restrict__ X, int Dp, int row0, float* __restrict__ nrm);
+
+__global__ void gather_targets_kernel(const float2* __restrict__ tx, int P, int users, const int* __restrict__ perm,
+                                      float* __restrict__ y, size_t y_stride, int row0);
+
+__global__ void gram_columns_kernel(const float* __restrict__ X, int Dp, int D, int nU, int v_first, int nV, int Lk,
+                                    int cap, ModelParams mp, float* __restrict__ K);
+
+// Persistent training sweep: one cluster of `cluster` CTAs per user.  Sets
+// *max_clusters to the number of clusters that fit the device; launches only
+// when that is >= 1.
+cudaError_t launch_train_exact(bool staged, int cluster, int threads, size_t smem, cudaStream_t stream,
+                               const TrainArgs& args, int* max_clusters);
+
+struct DetectArgs {
+    const float* Xs;   // n_samples x Dp data rows (Dedup columns of the received data)
+    int n_samples;     // 2S
+    int Dp, D;
+    const float* dict; // M x Dp dictionary rows
+    int M;
+    const float* a;    // users x a_stride
+    size_t a_stride;
+    const float* w;    // users x D
+    int users;
+    ModelParams mp;
+    float* out;        // users x out_stride soft outputs (real rows; complex64 interleaved per symbol)
+    size_t out_stride;
+};
+
+// Exact FP32 detection in the reference BALANCED kernel's evaluation order.
+void launch_detect_exact(const DetectArgs& args, cudaStream_t stream);
+
+} // namespace apsm
