@@ -107,6 +107,15 @@ apsm_status apsm_synchronize(apsm_detector* h);
 uint32_t apsm_rows(const apsm_detector* h);
 apsm_status apsm_get_state(apsm_detector* h, float* dict, float* a, float* w);
 
+/*
+ * GPU time (CUDA events, ms) of the last training sweep kernel and of the last
+ * detection kernel of this handle; -1 when that stage has not run.  Blocks
+ * until those kernels finished.  Replaces nothing in the reference (its
+ * train/detect return one event time each, apsm_train.cu:163-165,
+ * apsm_detect.cu:972-974); used for roofline accounting.
+ */
+apsm_status apsm_last_kernel_ms(apsm_detector* h, float* sweep_ms, float* detect_ms);
+
 /* Last error message of the handle ("" if none). */
 const char* apsm_last_error(const apsm_detector* h);
 

@@ -308,3 +308,9 @@ extern "C" apsm_status apsm_get_state(apsm_detector* h, float* dict, float* a, f
     if (!h) return APSM_ERR_INVALID_ARGUMENT;
     return h->get_state(dict, a, w);
 }
+
+extern "C" apsm_status apsm_last_kernel_ms(apsm_detector* h, float* sweep_ms, float* detect_ms)
+{
+    if (!h) return APSM_ERR_INVALID_ARGUMENT;
+    return h->stage_ms(sweep_ms, detect_ms);
+}

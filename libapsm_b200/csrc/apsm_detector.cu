@@ -45,6 +45,8 @@ apsm_detector::~apsm_detector()
     gram_workspace_free(gram);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (auto& e : stage_ev)
+        if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -93,23 +95,25 @@ apsm_status apsm_detector::init(const Config& c, uint32_t num_antennas, uint32_t
     APSM_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     APSM_CK(cudaEventCreate(&ev0));
     APSM_CK(cudaEventCreate(&ev1));
+    for (auto& e : stage_ev) APSM_CK(cudaEventCreate(&e));
     APSM_CK(dict_X.ensure(size_t(cap) * Dp));
     APSM_CK(dict_nrm.ensure(cap));
     APSM_CK(dict_y.ensure(size_t(U) * cap));
     APSM_CK(dict_a.ensure(size_t(U) * cap));
     APSM_CK(w.ensure(size_t(U) * D));
+    APSM_CK(train_err.ensure(1));
+    APSM_CK(cudaMemset(train_err.p, 0, sizeof(int)));
     cluster = env_int("APSM_TRAIN_CLUSTER", 16);
     return reset();
 }
 
 apsm_status apsm_detector::reset()
 {
-    // resetState (apsm_noma_detector.cu:89-93): fresh, zeroed training state
-    APSM_CK(cudaStreamSynchronize(stream));
+    // resetState (apsm_noma_detector.cu:89-93): fresh, zeroed training state.
+    // Stream-ordered: work already enqueued sees the old state, later work the new.
     used = 0;
     APSM_CK(cudaMemsetAsync(dict_a.p, 0, sizeof(float) * size_t(U) * cap, stream));
     APSM_CK(cudaMemsetAsync(w.p, 0, sizeof(float) * size_t(U) * D, stream));
-    APSM_CK(cudaStreamSynchronize(stream));
     return APSM_OK;
 }
 
@@ -226,40 +230,74 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         ta.a_stride = nU;
         ta.mp = mp;
 
-        // launch shape: the largest cluster whose CTAs can hold their kernel columns
+        ta.XP = int(Dp) + 4; // padded window-row pitch (conflict-free column reads)
+        ta.err = train_err.p;
+
+        // launch shape: the largest cluster (<= 16 CTAs) that holds its kernel
+        // columns in shared memory and of which every user gets one at once
         auto shape = [&](int C, bool staged, int* nwarps_out, int* ns_out) -> size_t {
             int nwarps = std::max({(int(q2) + C - 1) / C, (int(D) * kWGroups + 31) / 32, 4});
             int ns = staged ? ta.XW / C + 2 : 0;
             *nwarps_out = nwarps;
             *ns_out = ns;
-            return sizeof(float) * (size_t(ta.XW) * Dp + size_t(ns) * Lk + size_t(ta.A_ring) + kMaxFeatures + 2 * q2 +
-                                    size_t(nwarps) * 32 + 2 * size_t(ta.XW));
+            return sizeof(float) * (size_t(ta.XW) * ta.XP + size_t(ns) * Lk + size_t(ta.A_ring) + kMaxFeatures +
+                                    2 * q2 + size_t(nwarps) * 32 + 2 * size_t(ta.XW)) +
+                   32;
         };
         const size_t smem_limit = 227 * 1024;
-        int C = 16, nwarps = 0, ns = 0;
-        bool staged = true;
-        if (cluster > 0) C = std::min(16, cluster);
-        size_t smem = shape(C, true, &nwarps, &ns);
-        if (smem > smem_limit || nwarps > 32) {
-            staged = false;
-            smem = shape(C, false, &nwarps, &ns);
+        struct Choice {
+            int C = 0, nwarps = 0, ns = 0, clusters = 0;
+            bool staged = false;
+            size_t smem = 0;
+        } best;
+        const int cmax = cluster > 0 ? std::min(16, cluster) : 16;
+        for (int C = cmax; C >= 1; C /= 2) {
+            for (int st = 1; st >= 0; --st) {
+                int nw = 0, ns = 0;
+                size_t sm = shape(C, st == 1, &nw, &ns);
+                if (sm > smem_limit || nw > 32) continue;
+                int mc = 0;
+                if (query_train_clusters(st == 1, C, nw * 32, sm, int(U), &mc) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+                if (mc < 1) continue;
+                // prefer: all users concurrent, then staged columns, then larger clusters
+                auto score = [&](int clusters, bool staged, int c) {
+                    return (clusters >= int(U) ? 4 : 0) + (staged ? 2 : 0) + (c >= 8 ? 1 : 0);
+                };
+                if (best.C == 0 || score(mc, st == 1, C) > score(best.clusters, best.staged, best.C)) {
+                    best.C = C;
+                    best.nwarps = nw;
+                    best.ns = ns;
+                    best.clusters = mc;
+                    best.staged = st == 1;
+                    best.smem = sm;
+                }
+                break; // staged preferred at this cluster size
+            }
+            if (best.C != 0 && best.clusters >= int(U) && best.staged) break;
         }
-        if (smem > smem_limit || nwarps > 32) {
+        if (best.C == 0) {
             last_error = "training kernel does not fit one cluster (window " + std::to_string(q2) +
                          " rows, dictionary " + std::to_string(cap) + " rows)";
             return APSM_ERR_UNSUPPORTED;
         }
-        ta.NS = ns;
+        ta.NS = best.ns;
         ta.users = int(U);
         ta.prof = prof_buffer;
         int max_clusters = 0;
-        APSM_CK(launch_train_exact(staged, C, nwarps * 32, smem, s, ta, &max_clusters));
+        APSM_CK(cudaMemsetAsync(train_err.p, 0, sizeof(int), s));
+        APSM_CK(cudaEventRecord(stage_ev[0], s));
+        APSM_CK(launch_train_exact(best.staged, best.C, best.nwarps * 32, best.smem, s, ta, &max_clusters));
+        APSM_CK(cudaEventRecord(stage_ev[1], s));
+        stage_valid[0] = true;
         if (max_clusters < 1) {
-            last_error = "training cluster of " + std::to_string(C) + " CTAs cannot be scheduled";
+            last_error = "training cluster of " + std::to_string(best.C) + " CTAs cannot be scheduled";
             return APSM_ERR_UNSUPPORTED;
         }
-        last_train_cluster = C;
-        last_train_staged = staged;
+        last_train_cluster = best.C;
+        last_train_staged = best.staged;
     }
     APSM_CK(cudaEventRecord(ev1, s));
 
@@ -293,6 +331,8 @@ apsm_status apsm_detector::detect(const float2* d_rx, uint32_t S, float2* d_est,
         pack_rows_kernel<<<grid, 256, sm, s>>>(d_rx, int(N), int(S), nullptr, xs.p, int(Dp), 0, nullptr);
         APSM_CK(cudaGetLastError());
     }
+    APSM_CK(cudaEventRecord(stage_ev[2], s));
+    stage_valid[1] = true;
     if (cfg.detect_mode == DetectMode::Exact) {
         DetectArgs da;
         da.Xs = xs.p;
@@ -310,9 +350,13 @@ apsm_status apsm_detector::detect(const float2* d_rx, uint32_t S, float2* d_est,
         da.out_stride = ns;
         launch_detect_exact(da, s);
         APSM_CK(cudaGetLastError());
+        APSM_CK(cudaEventRecord(stage_ev[3], s));
         return APSM_OK;
     }
-    return detect_gram(this, S, reinterpret_cast<float*>(d_est), s);
+    apsm_status st = detect_gram(this, S, reinterpret_cast<float*>(d_est), s);
+    if (st != APSM_OK) return st;
+    APSM_CK(cudaEventRecord(stage_ev[3], s));
+    return APSM_OK;
 }
 
 apsm_status apsm_detector::train_host(const float2* rx, const float2* tx, uint32_t P, float* ms)
@@ -325,6 +369,8 @@ apsm_status apsm_detector::train_host(const float2* rx, const float2* tx, uint32
     apsm_status st = train(rx_stage.p, tx_stage.p, P, stream, &t);
     if (st != APSM_OK) return st;
     APSM_CK(cudaStreamSynchronize(stream));
+    st = check_train_error();
+    if (st != APSM_OK) return st;
     if (ms) *ms = t;
     return APSM_OK;
 }
@@ -354,5 +400,29 @@ apsm_status apsm_detector::get_state(float* dict, float* a_out, float* w_out)
         APSM_CK(cudaMemcpy2D(a_out, sizeof(float) * used, dict_a.p, sizeof(float) * cap, sizeof(float) * used, U,
                              cudaMemcpyDeviceToHost));
     if (w_out) APSM_CK(cudaMemcpy(w_out, w.p, sizeof(float) * size_t(U) * D, cudaMemcpyDeviceToHost));
+    return APSM_OK;
+}
+
+apsm_status apsm_detector::stage_ms(float* sweep_ms, float* detect_ms)
+{
+    float* out[2] = {sweep_ms, detect_ms};
+    for (int k = 0; k < 2; ++k) {
+        if (!out[k]) continue;
+        *out[k] = -1.f;
+        if (!stage_valid[k]) continue;
+        APSM_CK(cudaEventSynchronize(stage_ev[2 * k + 1]));
+        APSM_CK(cudaEventElapsedTime(out[k], stage_ev[2 * k], stage_ev[2 * k + 1]));
+    }
+    return APSM_OK;
+}
+
+apsm_status apsm_detector::check_train_error()
+{
+    int e = 0;
+    APSM_CK(cudaMemcpy(&e, train_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        last_error = "training sweep gave up waiting for its cluster (bounded wait expired)";
+        return APSM_ERR_CUDA;
+    }
     return APSM_OK;
 }

@@ -76,6 +76,9 @@ struct apsm_detector {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // stage events of the last train / detect call: [sweep start, sweep end, detect start, detect end]
+    cudaEvent_t stage_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool stage_valid[2] = {false, false};
     std::string last_error;
 
     // persistent model (dictionary rows oldest first, per-user targets and coefficients)
@@ -85,6 +88,7 @@ struct apsm_detector {
     // per-call scratch
     apsm::DevBuf<float> uX, unrm, uy, ua, K, xs;
     apsm::DevBuf<apsm::TrainStep> steps;
+    apsm::DevBuf<int> train_err; // set by the sweep when a bounded wait expired
     apsm::DevBuf<int> perm;
     apsm::DevBuf<float2> rx_stage, tx_stage, est_stage;
     apsm::GramWorkspace* gram = nullptr;
@@ -103,6 +107,8 @@ struct apsm_detector {
     apsm_status train_host(const float2* rx, const float2* tx, uint32_t P, float* ms);
     apsm_status detect_host(const float2* rx, uint32_t S, float2* est, float* ms);
     apsm_status get_state(float* dict, float* a, float* w_out);
+    apsm_status stage_ms(float* sweep_ms, float* detect_ms);
+    apsm_status check_train_error();
     apsm::ModelParams model_params() const;
     apsm_status cuda_fail(cudaError_t e, const char* what);
 };

@@ -28,12 +28,14 @@ struct TrainArgs {
     int nU, D, Dp, cap, q2, Lk, v_first;
     int A_ring, XW;         // power-of-two ring sizes (coefficients, window rows)
     int NS, Lc;             // staged kernel columns per CTA and their length (floats)
+    int XP;                 // shared-memory pitch of window rows (floats, Dp + 4)
     int used_before;        // rows present before this call
     int final_hi;           // visible end after the last step
     size_t y_stride, a_stride;
     int users;
     ModelParams mp;
     unsigned long long* prof; // phase timestamps (profiling builds only), kProfSteps x kProfMarks
+    int* err;                 // set to 1 when a bounded wait expired
 };
 
 constexpr int kProfSteps = 4096;
@@ -53,6 +55,8 @@ __global__ void gram_columns_kernel(const float* __restrict__ X, int Dp, int D, 
 // when that is >= 1.
 cudaError_t launch_train_exact(bool staged, int cluster, int threads, size_t smem, cudaStream_t stream,
                                const TrainArgs& args, int* max_clusters);
+// Clusters of this shape that fit the device at once.
+cudaError_t query_train_clusters(bool staged, int cluster, int threads, size_t smem, int users, int* max_clusters);
 
 struct DetectArgs {
     const float* Xs;   // n_samples x Dp data rows (Dedup columns of the received data)

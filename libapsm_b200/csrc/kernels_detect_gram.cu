@@ -1,13 +1,613 @@
-// Tensor-core Gram detection (placeholder until the tcgen05 kernel lands).
+// Tensor-core Gram detection on B200 (tcgen05 / TMEM / bulk async copies).
+//
+// The detection model (cpp/lib/apsm/apsm_detect.cu:690-876)
+//   f_u(x_s) = wL <w_u, x_s> + sum_b (a_ub wG) exp(ew ||d_b - x_s||^2)
+// is recast with ||d - x||^2 = ||x||^2 + ||d||^2 - 2 x.d: the cross terms of a
+// 128-sample tile against a 256-row dictionary chunk are one UMMA
+// (tcgen05.mma, M=128, N=256, FP32 accumulators in tensor memory), the norms
+// stay FP32, and the epilogue warps read the accumulator tile (tcgen05.ld),
+// form the squared distance, exponentiate on the SFU (ex2.approx) and
+// contract with every user's coefficients.  Operand precision:
+//   gram_bf16    x.d from BF16 operands (1 product)
+//   gram_bf16x3  compensated: x = xh + xl, d = dh + dl (BF16 each);
+//                x.d ~ xh.dh + xh.dl + xl.dh (3 products, ~2^-16 relative)
+//   gram_tf32    TF32 operands (1 product)
+//   gram_tf32x3  compensated TF32 split (3 products, ~FP32 accuracy)
+// The squared distance is clamped at 0 (cancellation for near-duplicate
+// points).  Each CTA owns one tile of data rows and a contiguous range of
+// dictionary chunks; partial sums per range are combined in a fixed order by
+// gram_finish_kernel, so results are deterministic.
+//
+// Roles (320 threads): warps 0-7 epilogue (warp w reads TMEM lanes
+// 32*(w%4).., columns of half w/4 of each chunk), warp 8 producer (bulk copies
+// of dictionary chunks into a 3-stage ring), warp 9 TMEM allocator and MMA
+// issuer.  Every mbarrier wait is bounded; on expiry the kernel records an
+// error, stops issuing work, still releases its tensor memory and returns.
 #include "apsm_gram.cuh"
+#include "apsm_kernels.cuh"
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
 
 namespace apsm {
-struct GramWorkspace {};
-void gram_workspace_free(GramWorkspace* g) { delete g; }
+
+enum GramMode : int { kBF16 = 0, kBF16x3 = 1, kTF32 = 2, kTF32x3 = 3 };
+
+constexpr int kTileM = 128;       // data rows per CTA tile (UMMA M)
+constexpr int kStages = 3;        // dictionary chunk ring
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = (kEpiWarps + 2) * 32;
+constexpr int kMaxUsers = 16;
+constexpr unsigned long long kWaitLimitNs = 2000000000ull; // bounded mbarrier waits (error instead of a hang)
+
+struct GramWorkspace {
+    DevBuf<uint8_t> a_ops, b_ops; // operand tiles in the UMMA canonical K-major layout
+    DevBuf<float> xn, dn, aw, part, lin_unused;
+    DevBuf<int> err;
+    int* h_err = nullptr;
+};
+
+void gram_workspace_free(GramWorkspace* g)
+{
+    if (!g) return;
+    if (g->h_err) cudaFreeHost(g->h_err);
+    delete g;
+}
+
+namespace {
+
+// ------------------------------------------------------------------ PTX --
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait (2 s): false (and *abort set) when the barrier did not complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (;;) {
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (*abort) return false;
+        if (global_ns() - t0 > kWaitLimitNs) break;
+    }
+    *abort = 1;
+    return false;
+}
+
+// Bounded wait used on the way out (also after an abort): in-flight async work
+// must land before the CTA exits or releases tensor memory.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity)
+{
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > kWaitLimitNs) return;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// UMMA shared-memory matrix descriptor, K-major, no swizzle ("interleaved"
+// canonical layout): 8-row x 16-byte core matrices; lbo = byte distance of the
+// two 16-byte K halves of one MMA K step, sbo = byte distance of 8-row groups.
+__device__ __forceinline__ uint64_t smem_desc(const void* base, uint32_t lbo, uint32_t sbo)
+{
+    uint64_t d = 0;
+    d |= uint64_t((smem_u32(base) >> 4) & 0x3FFFu);
+    d |= uint64_t((lbo >> 4) & 0x3FFFu) << 16;
+    d |= uint64_t((sbo >> 4) & 0x3FFFu) << 32;
+    d |= uint64_t(1) << 46; // descriptor version for tcgen05
+    return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: FP32 accumulate, A/B K-major, M x N.
+template <int MODE> __host__ __device__ constexpr uint32_t instr_desc(int M, int N)
+{
+    const uint32_t fmt = (MODE == kTF32 || MODE == kTF32x3) ? 2u : 1u; // TF32 : BF16
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+template <int MODE>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+    if constexpr (MODE == kTF32 || MODE == kTF32x3) {
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+                     "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+    } else {
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+                     "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+    }
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// 32 consecutive accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
+{
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                   "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float ex2(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+template <int MODE> struct OpTraits {
+    static constexpr bool kTF = (MODE == kTF32 || MODE == kTF32x3);
+    static constexpr bool kSplit = (MODE == kBF16x3 || MODE == kTF32x3);
+    static constexpr int kElem = kTF ? 4 : 2;     // bytes per operand element
+    static constexpr int kChunk = 16 / kElem;     // elements per 16-byte K chunk
+    static constexpr int kStepK = 2 * kChunk;     // K per UMMA instruction (32 bytes)
+};
+
+// ------------------------------------------------------ operand packing --
+
+// rows: n x Dp fp32.  Writes tiles of R rows: element (r, k) of tile t at byte
+// t*R*KE*elem + (k/kc)*(R*16) + (r/8)*128 + (r%8)*16 + (k%kc)*elem, where the
+// K extent KE = Kp (hi part) [+ Kp (lo part) for split modes]; rows >= n and
+// features >= D are zero.  Also the FP32 squared norms.
+template <int MODE>
+__global__ void gram_pack_kernel(const float* __restrict__ rows, int n, int Dp, int D, int Kp, int R, int n_tiles,
+                                 uint8_t* __restrict__ ops, float* __restrict__ norms)
+{
+    using T = OpTraits<MODE>;
+    const int KE = T::kSplit ? 2 * Kp : Kp;
+    const size_t total = size_t(n_tiles) * R * Kp;
+    for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < total; idx += size_t(gridDim.x) * blockDim.x) {
+        const int k = int(idx % Kp);
+        const size_t rr = idx / Kp;
+        const int r = int(rr % R), t = int(rr / R);
+        const int row = t * R + r;
+        const float x = (row < n && k < D) ? rows[size_t(row) * Dp + k] : 0.f;
+        float hi, lo;
+        if constexpr (T::kTF) {
+            uint32_t h;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+            hi = __uint_as_float(h);
+            lo = x - hi;
+        } else {
+            hi = __bfloat162float(__float2bfloat16_rn(x));
+            lo = x - hi;
+        }
+        uint8_t* tile = ops + size_t(t) * R * KE * T::kElem;
+        auto put = [&](int kk, float v) {
+            uint8_t* p = tile + size_t(kk / T::kChunk) * (R * 16) + (r / 8) * 128 + (r % 8) * 16 + (kk % T::kChunk) * T::kElem;
+            if constexpr (T::kTF) *reinterpret_cast<float*>(p) = v;
+            else *reinterpret_cast<__nv_bfloat16*>(p) = __float2bfloat16_rn(v);
+        };
+        put(k, hi);
+        if constexpr (T::kSplit) put(Kp + k, lo);
+    }
+    if (norms) {
+        for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+            float acc = 0.f;
+            for (int k = 0; k < D; ++k) {
+                const float v = rows[size_t(row) * Dp + k];
+                acc = fmaf(v, v, acc);
+            }
+            norms[row] = acc;
+        }
+    }
+}
+
+// aw[u][b] = a_u[b] * wG (the reference's coeff * gaussianKernelWeight), 0 past M.
+__global__ void gram_coeff_kernel(const float* __restrict__ a, size_t a_stride, int users, int M, int Mpad, float wG,
+                                  float* __restrict__ aw)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= users * Mpad) return;
+    const int u = i / Mpad, b = i % Mpad;
+    aw[i] = b < M ? __fmul_rn(a[size_t(u) * a_stride + b], wG) : 0.f;
+}
+
+struct GramArgs {
+    const uint8_t* a_ops; // data tiles (kTileM rows)
+    const uint8_t* b_ops; // dictionary chunks (N rows)
+    const float* xn;      // data norms
+    const float* dn;      // dictionary norms (Mpad)
+    const float* aw;      // users x Mpad
+    float* part;          // splits x users x n_samples partial sums
+    int* err;
+    int n_samples, Mpad, users, Kp, N;
+    int chunks_per_split, n_chunks;
+    float ewl2; // ew * log2(e)
+};
+
+template <int MODE, int NU>
+__global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
+{
+    using T = OpTraits<MODE>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int KE = T::kSplit ? 2 * g.Kp : g.Kp;
+    const uint32_t a_bytes = uint32_t(kTileM) * KE * T::kElem;
+    const uint32_t b_bytes = uint32_t(g.N) * KE * T::kElem;
+    const uint32_t x_bytes = uint32_t(g.N) * 4 * (1 + g.users); // dn + aw rows
+    uint8_t* sA = smem;
+    uint8_t* sB = sA + a_bytes;
+    float* sX = reinterpret_cast<float*>(sB + size_t(kStages) * b_bytes); // [stage][1 + users][N]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(sX) + size_t(kStages) * x_bytes);
+    uint64_t* full = bars;                 // [kStages]
+    uint64_t* empty = bars + kStages;      // [kStages]
+    uint64_t* tfull = bars + 2 * kStages;  // [2]
+    uint64_t* tempty = tfull + 2;          // [2]
+    uint64_t* afull = tempty + 2;          // [1]
+    uint64_t* done = afull + 1;            // [1] all MMAs of the CTA completed
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    float* red = reinterpret_cast<float*>(tmem_slot + 4); // [4 warps][32][users] second-half partials
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x, split = blockIdx.y;
+    const int c0 = split * g.chunks_per_split;
+    const int c1 = min(g.n_chunks, c0 + g.chunks_per_split);
+    const int nch = max(0, c1 - c0);
+    const int N = g.N;
+    const uint32_t ncols = uint32_t(2 * N);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1 + kEpiWarps);
+        }
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&tfull[s], 1);
+            mbar_init(&tempty[s], kEpiWarps);
+        }
+        mbar_init(afull, 1);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == kEpiWarps + 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == kEpiWarps) {
+        // ---------------- producer: data tile once, then dictionary chunks ----------------
+        if (lane == 0) {
+            mbar_expect_tx(afull, a_bytes);
+            bulk_g2s(sA, g.a_ops + size_t(tile) * a_bytes, a_bytes, afull);
+            int issued = 0;
+            for (int i = 0; i < nch; ++i) {
+                const int s = i % kStages;
+                if (i >= kStages && !mbar_wait(&empty[s], ((i / kStages) - 1) & 1, abort_flag)) break;
+                ++issued;
+                const int c = c0 + i;
+                mbar_expect_tx(&full[s], b_bytes + x_bytes);
+                bulk_g2s(sB + size_t(s) * b_bytes, g.b_ops + size_t(c) * b_bytes, b_bytes, &full[s]);
+                float* xs = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(sX) + size_t(s) * x_bytes);
+                bulk_g2s(xs, g.dn + size_t(c) * N, N * 4, &full[s]);
+                for (int u = 0; u < g.users; ++u)
+                    bulk_g2s(xs + (1 + u) * N, g.aw + size_t(u) * g.Mpad + size_t(c) * N, N * 4, &full[s]);
+            }
+            // no bulk copy may still be writing shared memory when the CTA exits
+            mbar_drain(afull, 0);
+            for (int i = max(0, issued - kStages); i < issued; ++i) mbar_drain(&full[i % kStages], (i / kStages) & 1);
+        }
+    } else if (warp == kEpiWarps + 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0 && mbar_wait(afull, 0, abort_flag)) {
+            const uint32_t idesc = instr_desc<MODE>(kTileM, N);
+            const uint32_t lbo_a = kTileM * 16, lbo_b = uint32_t(N) * 16;
+            const int ksteps = g.Kp / T::kStepK;
+            const int lo_off = g.Kp / T::kChunk; // K chunks to the lo half
+            for (int i = 0; i < nch; ++i) {
+                const int s = i % kStages, buf = i & 1;
+                if (!mbar_wait(&full[s], (i / kStages) & 1, abort_flag)) break;
+                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag)) break;
+                tc_fence_after();
+                const uint8_t* b = sB + size_t(s) * b_bytes;
+                const uint32_t d = tmem + uint32_t(buf * N);
+                uint32_t acc = 0;
+                for (int kk = 0; kk < ksteps; ++kk) {
+                    const uint64_t ah = smem_desc(sA + size_t(2 * kk) * lbo_a, lbo_a, 128);
+                    const uint64_t bh = smem_desc(b + size_t(2 * kk) * lbo_b, lbo_b, 128);
+                    umma<MODE>(d, ah, bh, idesc, acc);
+                    acc = 1;
+                    if constexpr (T::kSplit) {
+                        const uint64_t al = smem_desc(sA + size_t(lo_off + 2 * kk) * lbo_a, lbo_a, 128);
+                        const uint64_t bl = smem_desc(b + size_t(lo_off + 2 * kk) * lbo_b, lbo_b, 128);
+                        umma<MODE>(d, ah, bl, idesc, 1);
+                        umma<MODE>(d, al, bh, idesc, 1);
+                    }
+                }
+                umma_commit(&tfull[buf]); // accumulator ready for the epilogue
+                umma_commit(&empty[s]);   // operand stage free once these MMAs completed
+            }
+        }
+        if (lane == 0) {
+            // every MMA of this CTA has completed before tensor memory is released
+            umma_commit(done);
+            mbar_drain(done, 0);
+        }
+    } else {
+        // ---------------- epilogue: 8 warps ----------------
+        const int q = warp & 3, h = warp >> 2;
+        const int row = tile * kTileM + q * 32 + lane;
+        const float xn = row < g.n_samples ? g.xn[row] : 0.f;
+        float acc[NU];
+#pragma unroll
+        for (int u = 0; u < NU; ++u) acc[u] = 0.f;
+        const int half = N / 2;
+        for (int i = 0; i < nch; ++i) {
+            const int s = i % kStages, buf = i & 1;
+            // the stage's norms / coefficients (bulk copies) and the accumulator
+            if (!mbar_wait(&full[s], (i / kStages) & 1, abort_flag)) break;
+            if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag)) break;
+            tc_fence_after();
+            const float* xs = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(sX) + size_t(s) * x_bytes);
+            for (int cb = 0; cb < half; cb += 32) {
+                const int col = h * half + cb;
+                float gv[32];
+                tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * N + col), gv);
+#pragma unroll
+                for (int j = 0; j < 32; j += 4) {
+                    const float4 dn4 = *reinterpret_cast<const float4*>(xs + col + j);
+                    float kv[4];
+                    kv[0] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j + 0], xn + dn4.x), 0.f));
+                    kv[1] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j + 1], xn + dn4.y), 0.f));
+                    kv[2] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j + 2], xn + dn4.z), 0.f));
+                    kv[3] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j + 3], xn + dn4.w), 0.f));
+#pragma unroll
+                    for (int u = 0; u < NU; ++u) {
+                        if (u < g.users) {
+                            const float4 a4 = *reinterpret_cast<const float4*>(xs + (1 + u) * N + col + j);
+                            acc[u] = fmaf(a4.x, kv[0], acc[u]);
+                            acc[u] = fmaf(a4.y, kv[1], acc[u]);
+                            acc[u] = fmaf(a4.z, kv[2], acc[u]);
+                            acc[u] = fmaf(a4.w, kv[3], acc[u]);
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&tempty[buf]);
+                mbar_arrive(&empty[s]);
+            }
+        }
+        // combine the two column halves: warps 4-7 hand their sums to warps 0-3
+        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");
+        if (h == 1) {
+#pragma unroll
+            for (int u = 0; u < NU; ++u)
+                if (u < g.users) red[(q * 32 + lane) * g.users + u] = acc[u];
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");
+        if (h == 0 && row < g.n_samples) {
+#pragma unroll
+            for (int u = 0; u < NU; ++u)
+                if (u < g.users)
+                    g.part[(size_t(split) * g.users + u) * g.n_samples + row] =
+                        acc[u] + red[(q * 32 + lane) * g.users + u];
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == kEpiWarps + 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+    }
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(g.err, 1);
+}
+
+// out[u][s] = wL <w_u, x_s> + sum_split part[split][u][s] (fixed order).
+__global__ void gram_finish_kernel(const float* __restrict__ xs, int Dp, int D, const float* __restrict__ w, float wL,
+                                   const float* __restrict__ part, int splits, int users, int n_samples,
+                                   float* __restrict__ out, size_t out_stride)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= users * n_samples) return;
+    const int u = i / n_samples, s = i % n_samples;
+    float lin = 0.f;
+    for (int d = 0; d < D; ++d) lin = fmaf(w[size_t(u) * D + d], xs[size_t(s) * Dp + d], lin);
+    float gsum = 0.f;
+    for (int sp = 0; sp < splits; ++sp) gsum += part[(size_t(sp) * users + u) * n_samples + s];
+    out[size_t(u) * out_stride + s] = fmaf(wL, lin, gsum);
+}
+
+template <int MODE, int NU> void launch_gram(const GramArgs& ga, int n_tiles, int splits, size_t smem, cudaStream_t s,
+                                             cudaError_t* e)
+{
+    *e = cudaFuncSetAttribute(gram_detect_kernel<MODE, NU>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (*e != cudaSuccess) return;
+    gram_detect_kernel<MODE, NU><<<dim3(n_tiles, splits), kThreads, smem, s>>>(ga);
+    *e = cudaGetLastError();
+}
+
+template <int MODE>
+apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
+{
+    using T = OpTraits<MODE>;
+    GramWorkspace* gw = h->gram;
+    const int ns = int(2 * S);
+    const int M = int(h->used);
+    const int D = int(h->D), Dp = int(h->Dp), U = int(h->U);
+    if (U > kMaxUsers) {
+        h->last_error = "Gram detection supports at most " + std::to_string(kMaxUsers) + " users per detector";
+        return APSM_ERR_UNSUPPORTED;
+    }
+    const int Kp = int(round_up(uint32_t(D), uint32_t(T::kStepK)));
+    const int KE = T::kSplit ? 2 * Kp : Kp;
+    // dictionary chunk width: keep the data tile and 3 stages within shared memory
+    int N = 256;
+    auto smem_for = [&](int n) {
+        return size_t(kTileM) * KE * T::kElem + size_t(kStages) * (size_t(n) * KE * T::kElem + size_t(n) * 4 * (1 + U)) +
+               (2 * kStages + 6) * 8 + 16 + size_t(4 * 32) * U * 4;
+    };
+    while (N > 64 && smem_for(N) > 220 * 1024) N /= 2;
+    if (smem_for(N) > 220 * 1024) {
+        h->last_error = "Gram detection operands do not fit shared memory";
+        return APSM_ERR_UNSUPPORTED;
+    }
+    const int n_tiles = (ns + kTileM - 1) / kTileM;
+    const int n_chunks = std::max(1, (M + N - 1) / N);
+    const int Mpad = n_chunks * N;
+    int splits = std::max(1, std::min(n_chunks, (2 * 148 + n_tiles - 1) / n_tiles));
+    const int cps = (n_chunks + splits - 1) / splits;
+    splits = (n_chunks + cps - 1) / cps;
+
+    cudaError_t e;
+#define GR_CK(x)                                                   \
+    do {                                                           \
+        e = (x);                                                   \
+        if (e != cudaSuccess) return h->cuda_fail(e, #x);          \
+    } while (0)
+    GR_CK(gw->a_ops.ensure(size_t(n_tiles) * kTileM * KE * T::kElem));
+    GR_CK(gw->b_ops.ensure(size_t(n_chunks) * N * KE * T::kElem));
+    GR_CK(gw->xn.ensure(size_t(n_tiles) * kTileM));
+    GR_CK(gw->dn.ensure(Mpad));
+    GR_CK(gw->aw.ensure(size_t(U) * Mpad));
+    GR_CK(gw->part.ensure(size_t(splits) * U * ns));
+    GR_CK(gw->err.ensure(1));
+    GR_CK(cudaMemsetAsync(gw->err.p, 0, sizeof(int), s));
+    GR_CK(cudaMemsetAsync(gw->dn.p, 0, sizeof(float) * Mpad, s));
+
+    const int threads = 256;
+    gram_pack_kernel<MODE><<<std::min(4096, (n_tiles * kTileM * Kp + threads - 1) / threads), threads, 0, s>>>(
+        h->xs.p, ns, Dp, D, Kp, kTileM, n_tiles, gw->a_ops.p, gw->xn.p);
+    GR_CK(cudaGetLastError());
+    gram_pack_kernel<MODE><<<std::min(4096, (n_chunks * N * Kp + threads - 1) / threads), threads, 0, s>>>(
+        h->dict_X.p, M, Dp, D, Kp, N, n_chunks, gw->b_ops.p, gw->dn.p);
+    GR_CK(cudaGetLastError());
+    gram_coeff_kernel<<<(U * Mpad + 255) / 256, 256, 0, s>>>(h->dict_a.p, h->cap, U, M, Mpad, h->cfg.wG, gw->aw.p);
+    GR_CK(cudaGetLastError());
+
+    GramArgs ga;
+    ga.a_ops = gw->a_ops.p;
+    ga.b_ops = gw->b_ops.p;
+    ga.xn = gw->xn.p;
+    ga.dn = gw->dn.p;
+    ga.aw = gw->aw.p;
+    ga.part = gw->part.p;
+    ga.err = gw->err.p;
+    ga.n_samples = ns;
+    ga.Mpad = Mpad;
+    ga.users = U;
+    ga.Kp = Kp;
+    ga.N = N;
+    ga.chunks_per_split = cps;
+    ga.n_chunks = n_chunks;
+    ga.ewl2 = h->model_params().ew * 1.4426950408889634f;
+    // >= 120 KB keeps one CTA per SM, so the 2N tensor-memory columns of a CTA never wait for another's
+    const size_t smem = std::max<size_t>(smem_for(N) + 1024, 120 * 1024);
+    if (U <= 1) launch_gram<MODE, 1>(ga, n_tiles, splits, smem, s, &e);
+    else if (U <= 2) launch_gram<MODE, 2>(ga, n_tiles, splits, smem, s, &e);
+    else if (U <= 4) launch_gram<MODE, 4>(ga, n_tiles, splits, smem, s, &e);
+    else if (U <= 8) launch_gram<MODE, 8>(ga, n_tiles, splits, smem, s, &e);
+    else launch_gram<MODE, 16>(ga, n_tiles, splits, smem, s, &e);
+    if (e != cudaSuccess) return h->cuda_fail(e, "gram_detect_kernel launch");
+    gram_finish_kernel<<<(U * ns + 255) / 256, 256, 0, s>>>(h->xs.p, Dp, D, h->w.p, h->cfg.wL, gw->part.p, splits, U,
+                                                            ns, d_out, size_t(ns));
+    GR_CK(cudaGetLastError());
+    GR_CK(cudaMemcpyAsync(gw->h_err, gw->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+#undef GR_CK
+    return APSM_OK;
+}
+
+} // namespace
 } // namespace apsm
 
-apsm_status detect_gram(apsm_detector* h, uint32_t, float*, cudaStream_t)
+using namespace apsm;
+
+apsm_status detect_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
 {
-    h->last_error = "Gram detection is not available in this build";
-    return APSM_ERR_UNSUPPORTED;
+    if (!h->gram) {
+        h->gram = new GramWorkspace();
+        if (cudaMallocHost(&h->gram->h_err, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            h->last_error = "pinned allocation failed";
+            return APSM_ERR_OUT_OF_MEMORY;
+        }
+        *h->gram->h_err = 0;
+    }
+    if (*h->gram->h_err) {
+        h->last_error = "a previous Gram detection timed out waiting on the GPU";
+        return APSM_ERR_CUDA;
+    }
+    switch (h->cfg.detect_mode) {
+    case DetectMode::GramBF16: return run_gram<kBF16>(h, S, d_out, s);
+    case DetectMode::GramBF16x3: return run_gram<kBF16x3>(h, S, d_out, s);
+    case DetectMode::GramTF32: return run_gram<kTF32>(h, S, d_out, s);
+    case DetectMode::GramTF32x3: return run_gram<kTF32x3>(h, S, d_out, s);
+    default: break;
+    }
+    h->last_error = "not a Gram detection mode";
+    return APSM_ERR_INVALID_ARGUMENT;
 }

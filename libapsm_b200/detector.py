@@ -137,6 +137,12 @@ class NomaDetector:
         self._check(self._lib.apsm_detect_device(self._h, rx.data_ptr(), int(rx.shape[-1]), est.data_ptr(),
                                                  stream or None))
 
+    def last_kernel_ms(self) -> tuple[float, float]:
+        """GPU ms of the last training sweep kernel and the last detection kernel (-1 if not run)."""
+        a, b = ctypes.c_float(), ctypes.c_float()
+        self._check(self._lib.apsm_last_kernel_ms(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return float(a.value), float(b.value)
+
     def synchronize(self) -> None:
         self._check(self._lib.apsm_synchronize(self._h))
 
