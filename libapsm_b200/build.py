@@ -58,7 +58,8 @@ def build(ptxas_verbose: bool = False) -> Path:
     newest = max(o.stat().st_mtime for o in objs)
     if not LIB.exists() or LIB.stat().st_mtime < newest:
         tmp = LIB.with_suffix(".so.tmp")
-        cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", str(tmp)] + [str(o) for o in objs] + ["-lcudart"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", str(tmp)] + [str(o) for o in objs] + [
+            "-lcublas", "-lcudart"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

@@ -2,6 +2,7 @@
 #include "apsm_host.hpp"
 #include "apsm_kernels.cuh"
 #include "apsm_gram.cuh"
+#include "apsm_lls.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -43,6 +44,7 @@ apsm_detector::~apsm_detector()
 {
     if (stream) cudaStreamSynchronize(stream);
     gram_workspace_free(gram);
+    lls_workspace_free(lls);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     for (auto& e : stage_ev)
@@ -67,14 +69,7 @@ apsm_status apsm_detector::init(const Config& c, uint32_t num_antennas, uint32_t
     D = 2 * N;
     Dp = row_pitch(D);
     U = num_users;
-    if (cfg.otype != "APSM") {
-        last_error = "LLS detector is not available in this build";
-        return APSM_ERR_UNSUPPORTED;
-    }
-    if (cfg.lls_init) {
-        last_error = "llsInitialization is not available in this build";
-        return APSM_ERR_UNSUPPORTED;
-    }
+    is_lls = cfg.otype == "LLS";
     if (cfg.norm_constraint > 0.f) {
         last_error = "normConstraint > 0 is not available in this build";
         return APSM_ERR_UNSUPPORTED;
@@ -119,6 +114,32 @@ apsm_status apsm_detector::reset()
 
 apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_t P, cudaStream_t s, float* ms)
 {
+    if (is_lls || cfg.lls_init) {
+        // LlsNomaDetector::train (lls_detector.cu:136-161) on the unshuffled pilots;
+        // for llsInitialization (apsm_noma_detector.cu:98-99, 331-346) w = w_lls / wL
+        APSM_CK(uX.ensure(size_t(2 * P) * Dp));
+        APSM_CK(uy.ensure(size_t(U) * 2 * P));
+        dim3 grid((P + kPackSamples - 1) / kPackSamples);
+        pack_rows_kernel<<<grid, 256, sizeof(float2) * N * kPackSamples, s>>>(d_rx, int(N), int(P), nullptr, uX.p,
+                                                                            int(Dp), 0, nullptr);
+        APSM_CK(cudaGetLastError());
+        gather_targets_kernel<<<(int(P * U) + 255) / 256, 256, 0, s>>>(d_tx, int(P), int(U), nullptr, uy.p,
+                                                                      size_t(2 * P), 0);
+        APSM_CK(cudaGetLastError());
+        if (ms) APSM_CK(cudaEventRecord(ev0, s));
+        apsm_status st = lls_solve(this, uX.p, int(2 * P), uy.p, size_t(2 * P), 0, is_lls ? 1.f : cfg.wL, s);
+        if (st != APSM_OK) return st;
+        if (is_lls) {
+            used = 2 * P; // marks the detector as trained
+            if (ms) {
+                APSM_CK(cudaEventRecord(ev1, s));
+                APSM_CK(cudaEventSynchronize(ev1));
+                APSM_CK(cudaEventElapsedTime(ms, ev0, ev1));
+            }
+            return APSM_OK;
+        }
+        APSM_CK(cudaMemcpyAsync(w.p, lls_weights(this), sizeof(float) * size_t(U) * D, cudaMemcpyDeviceToDevice, s));
+    }
     if (variance_eff == 0.f) {
         // the reference computes the heuristic on the host from the pilots
         std::vector<float2> h_rx(size_t(N) * P);
@@ -333,6 +354,12 @@ apsm_status apsm_detector::detect(const float2* d_rx, uint32_t S, float2* d_est,
     }
     APSM_CK(cudaEventRecord(stage_ev[2], s));
     stage_valid[1] = true;
+    if (is_lls) {
+        apsm_status st = lls_detect(this, int(ns), reinterpret_cast<float*>(d_est), s);
+        if (st != APSM_OK) return st;
+        APSM_CK(cudaEventRecord(stage_ev[3], s));
+        return APSM_OK;
+    }
     if (cfg.detect_mode == DetectMode::Exact) {
         DetectArgs da;
         da.Xs = xs.p;

@@ -66,6 +66,7 @@ template <class T> struct DevBuf {
 };
 
 struct GramWorkspace; // tensor-core detection operands (kernels_detect_gram.cu)
+struct LlsWorkspace;  // least-squares solver state (kernels_lls.cu)
 
 } // namespace apsm
 
@@ -92,6 +93,8 @@ struct apsm_detector {
     apsm::DevBuf<int> perm;
     apsm::DevBuf<float2> rx_stage, tx_stage, est_stage;
     apsm::GramWorkspace* gram = nullptr;
+    apsm::LlsWorkspace* lls = nullptr; // least-squares detector / llsInitialization
+    bool is_lls = false;               // "otype": "LLS"
 
     // training-kernel launch shape: requested cluster size, and the last one used
     int cluster = 0;

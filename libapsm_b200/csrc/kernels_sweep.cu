@@ -255,6 +255,7 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
 #pragma unroll
                 for (int j = 0; j < 8; ++j) p = __fadd_rn(p, __fmul_rn(kv[j], av[j]));
             }
+            if (v == first) APSM_PROF_MARK(6);
             red[warp * 32 + lane] = p;
             __syncwarp();
             float c = 0.f;
@@ -277,6 +278,7 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
                 c = __fdiv_rn(c, float(st.wk));
                 c = __fdiv_rn(c, __fadd_rn(linearNorm, mp.wG));
             }
+            if (v == first) APSM_PROF_MARK(7);
             c = __shfl_sync(0xffffffffu, c, 0);
             if (lane < C) st_async_f32(cb + (v - start), bar, uint32_t(lane), c);
             __syncwarp();

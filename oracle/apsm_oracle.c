@@ -409,3 +409,11 @@ int apsm_oracle_set_state(apsm_oracle* o, uint32_t rows, const double* dict, con
 }
 
 void apsm_oracle_set_variance(apsm_oracle* o, float variance) { o->par.gaussian_variance = variance; }
+
+void apsm_oracle_set_w(apsm_oracle* o, const double* w)
+{
+    for (uint32_t d = 0; d < o->D; ++d) {
+        if (o->prec == APSM_ORACLE_F32) o->Wf[d] = (float)w[d];
+        else o->Wd[d] = w[d];
+    }
+}

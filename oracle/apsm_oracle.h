@@ -64,6 +64,9 @@ int apsm_oracle_set_state(apsm_oracle* o, uint32_t rows, const double* dict, con
 /* Replace the effective Gaussian variance (the reference's heuristic path sets it in train()). */
 void apsm_oracle_set_variance(apsm_oracle* o, float variance);
 
+/* Replace the linear weights (llsInitialization, apsm_noma_detector.cu:321-346). */
+void apsm_oracle_set_w(apsm_oracle* o, const double* w);
+
 /* trainingShuffle permutation (shuffle.cpp). */
 void apsm_oracle_shuffle_permutation(uint32_t P, int32_t* perm);
 

@@ -97,6 +97,7 @@ def _load_oracle() -> ctypes.CDLL:
         lib.apsm_oracle_set_state.restype = ctypes.c_int
         lib.apsm_oracle_set_variance.argtypes = [P, ctypes.c_float]
         lib.apsm_oracle_shuffle_permutation.argtypes = [ctypes.c_uint32, P]
+        lib.apsm_oracle_set_w.argtypes = [P, P]
         _oracle_lib = lib
     return _oracle_lib
 
@@ -128,6 +129,35 @@ def variance_heuristic(rx: np.ndarray) -> np.float32:
     return np.float32(v * v)
 
 
+def dedup_rows(rx: np.ndarray) -> np.ndarray:
+    """Real rows of the Dedup embedding (cuda_matrix_device.cuh:180-188):
+    row 2n = [Re y_n; Im y_n], row 2n+1 = [Im y_n; -Re y_n]."""
+    rx = np.asarray(rx)
+    N, n = rx.shape
+    out = np.empty((2 * n, 2 * N), dtype=np.float64)
+    out[0::2, :N] = rx.real.T
+    out[0::2, N:] = rx.imag.T
+    out[1::2, :N] = rx.imag.T
+    out[1::2, N:] = -rx.real.T
+    return out
+
+
+def lls_weights(rx: np.ndarray, tx: np.ndarray) -> np.ndarray:
+    """LLS detector training (lls_detector.cu:136-179) in FP64: least squares
+    of the Dedup system, targets (Re x_n, Im x_n) interleaved."""
+    A = dedup_rows(rx)
+    t = np.asarray(tx).reshape(-1)
+    y = np.empty(2 * t.size)
+    y[0::2], y[1::2] = t.real, t.imag
+    return np.linalg.lstsq(A, y, rcond=None)[0]
+
+
+def lls_detect(rx: np.ndarray, w: np.ndarray) -> np.ndarray:
+    """LLS detection (lls_detector.cu:181-218): est = A w as complex symbols."""
+    f = dedup_rows(rx) @ w
+    return (f[0::2] + 1j * f[1::2]).astype(np.complex64)
+
+
 class OracleDetector:
     """CPU restatement of one reference ApsmNomaDetector (single user)."""
 
@@ -135,6 +165,7 @@ class OracleDetector:
         self._lib = _load_oracle()
         self.params = reference_params(config, num_antennas)
         self.shuffle = bool(config.get("trainingShuffle", False))
+        self.lls_init = bool(config.get("llsInitialization", False))
         self.N = int(num_antennas)
         self._h = self._lib.apsm_oracle_create(ctypes.byref(self.params), self.N, int(precision))
         if not self._h:
@@ -152,6 +183,10 @@ class OracleDetector:
         rx = np.ascontiguousarray(rx, dtype=np.complex64)
         tx = np.ascontiguousarray(np.asarray(tx).reshape(-1), dtype=np.complex64)
         assert rx.shape == (self.N, tx.shape[0])
+        if self.lls_init:
+            # llsInitialization (apsm_noma_detector.cu:98-99, 321-346): w = w_lls / wL, unshuffled pilots
+            w = lls_weights(rx, tx).astype(np.float32) / np.float32(self.params.linear_weight)
+            self._lib.apsm_oracle_set_w(self._h, np.ascontiguousarray(w, dtype=np.float64).ctypes.data)
         if self.shuffle:
             perm = shuffle_permutation(tx.shape[0])
             rx = np.ascontiguousarray(rx[:, perm])

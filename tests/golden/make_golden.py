@@ -1,0 +1,118 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures of the parity tests (test infrastructure).
+
+The reference has no tests and stores no expected outputs, so the fixtures
+are produced by running the reference library itself — fraunhoferhhi/libapsm
+compiled from its sources for sm_100a by oracle/Makefile (oracle/_ref/
+libapsm_ref.so) — through its public API (NomaDetectorFactory::build ->
+train -> detect) on a B200.
+
+  python tests/golden/make_golden.py capture
+      (where the reference tree is mounted) extracts a small slice of the
+      reference's captured testbed data, cpp/data/offline, into
+      tests/golden/captured_qpsk_inputs.npz
+  python tests/golden/make_golden.py run --out DIR
+      (on a GPU box) runs the reference library on every case and writes
+      DIR/golden_<case>.npz: inputs, config and the reference's estimates.
+
+Synthetic cases use libapsm_b200.synth with fixed seeds; 2S is a multiple of
+32 in every case (the reference BALANCED detect mis-handles a partial last
+block, see tests/test_parity_gpu.py).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+
+REF_DATA = Path("/root/reference/cpp/data/offline")
+
+CASES = {
+    "qpsk_small": (dict(seed=101, K=2, N=4, P=64, S=64, modulation="QPSK"),
+                   {"otype": "APSM", "windowSize": 8, "gaussianKernelVariance": 0.5, "eB": 0.01}),
+    "qam16_defaults": (dict(seed=102, K=3, N=8, P=120, S=112, modulation="QAM16"), {"otype": "APSM"}),
+    "config0_like": (dict(seed=103, K=6, N=8, P=300, S=304, modulation="QPSK"),
+                     {"otype": "APSM", "windowSize": 80, "gaussianKernelVariance": 0.5, "eB": 0.01}),
+    "sfw_step1": (dict(seed=104, K=3, N=6, P=100, S=96, modulation="QAM16"),
+                  {"otype": "APSM", "windowSize": 15, "startWithFullWindow": True, "sampleStep": 1,
+                   "gaussianKernelVariance": 0.3, "eB": 0.005}),
+    "passes2": (dict(seed=105, K=3, N=6, P=100, S=96, modulation="QAM16"),
+                {"otype": "APSM", "windowSize": 10, "trainPasses": 2, "dictionarySize": 100}),
+    "shuffle_var0": (dict(seed=106, K=3, N=6, P=100, S=96, modulation="QAM16"),
+                     {"otype": "APSM", "windowSize": 10, "trainingShuffle": True, "gaussianKernelVariance": 0.0}),
+    "wG08_detect_oldfast": (dict(seed=107, K=4, N=16, P=200, S=208, modulation="QAM16"),
+                            {"otype": "APSM", "windowSize": 40, "gaussianKernelWeight": 0.8,
+                             "gaussianKernelVariance": 0.2, "eB": 0.02, "detectVersion": "oldfast"}),
+}
+CAPTURED_CFG = {"otype": "APSM", "windowSize": 80}  # the README example's algorithm config
+USER = 1
+
+
+def capture() -> None:
+    """Slice of the captured QPSK (time-domain) data: 8 equidistant antennas,
+    user 1, first 160 pilots and 192 data symbols, tx scaled by 1/sqrt(2)
+    (loadData with Modulation::getScale, binary_load.cpp:55-81)."""
+    from libapsm_b200 import binfile
+
+    rx = binfile.read(REF_DATA / "rx" / "time" / "rxData_QPSK_alltx_converted.bin")
+    tx = binfile.read(REF_DATA / "tx" / "NOMA_signals_qpsk_complex.bin")
+    ant = [i * 16 // 8 for i in range(8)]  # antennaPatternEquidistant(8), util.cpp:264-272
+    scale = np.float32(1.0 / np.sqrt(2.0))
+    rxt = binfile.complex_matrix(rx["rxSigTraining"])[ant, :160]
+    rxd = binfile.complex_matrix(rx["rxSigData"])[ant, :192]
+    txt = binfile.complex_matrix(tx["mod_training"], scale)[:, :160]
+    txd = binfile.complex_matrix(tx["mod_data"], scale)[:, :192]
+    np.savez_compressed(HERE / "captured_qpsk_inputs.npz", rx_train=rxt, rx_data=rxd, tx_train=txt, tx_data=txd,
+                        source="cpp/data/offline/rx/time/rxData_QPSK_alltx_converted.bin + "
+                               "cpp/data/offline/tx/NOMA_signals_qpsk_complex.bin")
+    print("wrote", HERE / "captured_qpsk_inputs.npz")
+
+
+def run(out: Path) -> None:
+    from libapsm_b200 import synth
+    from oracle import oracle as O
+
+    out.mkdir(parents=True, exist_ok=True)
+    todo = []
+    for name, (fr, cfg) in CASES.items():
+        f = synth.generate_frame(fr["seed"], K=fr["K"], N=fr["N"], P=fr["P"], S=fr["S"], modulation=fr["modulation"],
+                                 snr_db=20)
+        todo.append((name, cfg, f.rx_train, f.tx_train, f.rx_data, f.tx_data, fr["modulation"]))
+    cap = np.load(HERE / "captured_qpsk_inputs.npz")
+    todo.append(("captured_qpsk", CAPTURED_CFG, cap["rx_train"], cap["tx_train"], cap["rx_data"], cap["tx_data"],
+                 "QPSK"))
+    for name, cfg, rxt, txt, rxd, txd, mod in todo:
+        r = O.ReferenceDetector(cfg, rxt.shape[0])
+        tms = r.train(rxt, txt[USER])
+        est, dms = r.detect(rxd)
+        r2 = O.ReferenceDetector(cfg, rxt.shape[0])
+        r2.train(rxt, txt[USER])
+        est2, _ = r2.detect(rxd)
+        spread = float(np.max(np.abs(est - est2)))
+        np.savez_compressed(out / f"golden_{name}.npz", config=json.dumps(cfg), user=USER, modulation=mod,
+                            rx_train=rxt, tx_train=txt[USER], rx_data=rxd, tx_data=txd[USER], est_ref=est,
+                            ref_run_to_run=spread, ref_train_ms=tms, ref_detect_ms=dms)
+        print(f"{name}: ref train {tms:.3f} ms detect {dms:.3f} ms, run-to-run max |d| {spread:.2e}")
+    # LLS reference outputs on one case (the reference's cuBLAS least-squares detector)
+    name, cfg, rxt, txt, rxd, txd, mod = todo[2]
+    r = O.ReferenceDetector({"otype": "LLS"}, rxt.shape[0])
+    r.train(rxt, txt[USER])
+    est, _ = r.detect(rxd)
+    np.savez_compressed(out / "golden_lls_config0_like.npz", config=json.dumps({"otype": "LLS"}), user=USER,
+                        modulation=mod, rx_train=rxt, tx_train=txt[USER], rx_data=rxd, tx_data=txd[USER], est_ref=est)
+    print("lls: done")
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("mode", choices=["capture", "run"])
+    ap.add_argument("--out", default=str(HERE))
+    a = ap.parse_args()
+    capture() if a.mode == "capture" else run(Path(a.out))
