@@ -76,7 +76,8 @@ Config parse_config(const std::string& json_text)
         for (const auto& k : keys)
             if (!key_in(k, {"otype", "llsInitialization", "trainingShuffle", "gaussianKernelWeight",
                             "gaussianKernelVariance", "windowSize", "sampleStep", "trainPasses",
-                            "startWithFullWindow", "dictionarySize", "normConstraint", "eB", "detectVersion"}))
+                            "startWithFullWindow", "dictionarySize", "normConstraint", "eB", "detectVersion",
+                            "trainVersion"}))
                 throw std::invalid_argument("Invalid key: " + k);
         c.lls_init = bool_value(cfg, "llsInitialization", false);
         c.shuffle = bool_value(cfg, "trainingShuffle", false);
@@ -90,6 +91,10 @@ Config parse_config(const std::string& json_text)
         c.dict_size = count_value(cfg, "dictionarySize", 685, 1);
         c.norm_constraint = float(num_value(cfg, "normConstraint", 0.));
         c.eB = float(num_value(cfg, "eB", 0.001));
+        const std::string tv = str_value(cfg, "trainVersion", "exact");
+        if (tv == "exact") c.train_incremental = false;
+        else if (tv == "incremental") c.train_incremental = true;
+        else throw std::invalid_argument("Unknown train version: " + tv);
         c.detect_version = str_value(cfg, "detectVersion", "balanced");
         if (c.detect_version == "original" || c.detect_version == "oldfast" || c.detect_version == "shmem" ||
             c.detect_version == "balanced")

@@ -222,8 +222,9 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         APSM_CK(steps.ensure(h_steps.size()));
         APSM_CK(cudaMemcpyAsync(steps.p, h_steps.data(), sizeof(TrainStep) * h_steps.size(), cudaMemcpyHostToDevice, s));
         {
-            dim3 grid((Lk + 255) / 256, (nV + kGramColsPerBlock - 1) / kGramColsPerBlock);
-            gram_columns_kernel<<<grid, 256, 0, s>>>(uX.p, int(Dp), int(D), int(nU), v_first, nV, Lk, int(cap), mp, K.p);
+            dim3 grid((Lk + kGramRows - 1) / kGramRows, (nV + kGramColsPerBlock - 1) / kGramColsPerBlock);
+            gram_columns_kernel<<<grid, kGramRows, 0, s>>>(uX.p, int(Dp), int(D), int(nU), v_first, nV, Lk, int(cap),
+                                                           mp, K.p);
             APSM_CK(cudaGetLastError());
         }
         TrainArgs ta;
@@ -253,6 +254,61 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
 
         ta.XP = int(Dp) + 4; // padded window-row pitch (conflict-free column reads)
         ta.err = train_err.p;
+        ta.users = int(U);
+        ta.prof = prof_buffer;
+        ta.NS = 0;
+
+        if (cfg.train_incremental) {
+            // rows resident at once: window(t) and the rows entering at t+1 (and t+2 prefetched)
+            int xs = 1;
+            for (int t = 0; t < T; ++t) {
+                const int t2 = std::min(T - 1, t + 1);
+                xs = std::max(xs, h_steps[t2].hi - (h_steps[t].hi - h_steps[t].wk) + 1);
+            }
+            ta.XS = xs;
+            // cluster size: the largest <= 8 of which every user gets one at once
+            const int cmax = cluster > 0 ? std::min(16, cluster) : 8;
+            {
+                int bestC = 0;
+                size_t bestSmem = 0;
+                for (int C = cmax; C >= 1; C /= 2) {
+                    const int nso = (xs + C - 1) / C + 1;
+                    const int nsop = int(round_up(uint32_t(nso), 32u));
+                    const size_t smem = incremental_smem_bytes(ta.XS, ta.XP, nsop, ta.A_ring);
+                    if (smem > 227 * 1024) continue;
+                    int mc = 0;
+                    cudaError_t e = query_incremental_clusters(C, smem, int(U), &mc);
+                    if (e != cudaSuccess) {
+                        cudaGetLastError();
+                        continue;
+                    }
+                    if (mc < 1) continue;
+                    if (bestC == 0) {
+                        bestC = C;
+                        bestSmem = smem;
+                    }
+                    if (mc >= int(U)) {
+                        bestC = C;
+                        bestSmem = smem;
+                        break;
+                    }
+                }
+                if (bestC > 0) {
+                    ta.NSO = (xs + bestC - 1) / bestC + 1;
+                    ta.NSOp = int(round_up(uint32_t(ta.NSO), 32u));
+                    int mc = 0;
+                    APSM_CK(cudaMemsetAsync(train_err.p, 0, sizeof(int), s));
+                    APSM_CK(cudaEventRecord(stage_ev[0], s));
+                    APSM_CK(launch_train_incremental(bestC, bestSmem, s, ta, &mc));
+                    APSM_CK(cudaEventRecord(stage_ev[1], s));
+                    stage_valid[0] = true;
+                    last_train_cluster = bestC;
+                    last_train_staged = false;
+                    goto sweep_done;
+                }
+            }
+            // window too large for the incremental sweep's shared memory: the exact sweep below
+        }
 
         // launch shape: the largest cluster (<= 16 CTAs) that holds its kernel
         // columns in shared memory and of which every user gets one at once
@@ -320,6 +376,7 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         last_train_cluster = best.C;
         last_train_staged = best.staged;
     }
+sweep_done:
     APSM_CK(cudaEventRecord(ev1, s));
 
     // the dictionary after the sweep is the last min(final_hi, cap) universe rows

@@ -30,6 +30,7 @@ struct Config {
     float eB = 0.001f;
     std::string detect_version = "balanced";
     DetectMode detect_mode = DetectMode::Exact;
+    bool train_incremental = false; // "trainVersion": "incremental"
 };
 
 Config parse_config(const std::string& json_text);

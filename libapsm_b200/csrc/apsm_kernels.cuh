@@ -7,6 +7,7 @@ namespace apsm {
 
 constexpr int kPackSamples = 64;     // complex samples per pack_rows_kernel block
 constexpr int kGramColsPerBlock = 8; // kernel columns per gram_columns_kernel block
+constexpr int kGramRows = 128;       // column entries per gram_columns_kernel block (its thread count)
 constexpr int kLookahead = 2;        // training steps fetched ahead by cp.async
 
 // First universe row stored in kernel column v (16-byte aligned).
@@ -29,6 +30,8 @@ struct TrainArgs {
     int A_ring, XW;         // power-of-two ring sizes (coefficients, window rows)
     int NS, Lc;             // staged kernel columns per CTA and their length (floats)
     int XP;                 // shared-memory pitch of window rows (floats, Dp + 4)
+    int XS;                 // window slots of the incremental sweep (row r in slot r % XS)
+    int NSO, NSOp;          // incremental sweep: owned-column slots per CTA and their padded pitch
     int used_before;        // rows present before this call
     int final_hi;           // visible end after the last step
     size_t y_stride, a_stride;
@@ -57,6 +60,13 @@ cudaError_t launch_train_exact(bool staged, int cluster, int threads, size_t sme
                                const TrainArgs& args, int* max_clusters);
 // Clusters of this shape that fit the device at once.
 cudaError_t query_train_clusters(bool staged, int cluster, int threads, size_t smem, int users, int* max_clusters);
+
+// Incremental sweep (kernels_sweep_inc.cu): one cluster of `cluster` CTAs per user.
+int incremental_threads();
+cudaError_t query_incremental_clusters(int cluster, size_t smem, int users, int* max_clusters);
+size_t incremental_smem_bytes(int XS, int XP, int NSOp, int A_ring);
+cudaError_t launch_train_incremental(int cluster, size_t smem, cudaStream_t stream, const TrainArgs& args,
+                                     int* max_clusters);
 
 struct DetectArgs {
     const float* Xs;   // n_samples x Dp data rows (Dedup columns of the received data)

@@ -107,34 +107,55 @@ __global__ void gather_targets_kernel(const float2* __restrict__ tx, int P, int 
 // reference's: sequential fma of (d_u - x_v)^2, float product with the exp
 // weight, expf, product with the Gaussian weight (apsm_detect.cu:131-152,
 // apsm_train.cu:219).
-__global__ void __launch_bounds__(256) gram_columns_kernel(const float* __restrict__ X, int Dp, int D, int nU,
-                                                           int v_first, int nV, int Lk, int cap, ModelParams mp,
-                                                           float* __restrict__ K)
+// Block: kGramRows consecutive entries i of kGramColsPerBlock consecutive
+// columns.  The rows those entries touch (at most kGramRows + 12 of them, the
+// columns' bases differ by < 12) are staged through shared memory 32
+// features at a time; the squared distance keeps its sequential feature order
+// across the chunks.
+__global__ void __launch_bounds__(kGramRows) gram_columns_kernel(const float* __restrict__ X, int Dp, int D, int nU,
+                                                                 int v_first, int nV, int Lk, int cap, ModelParams mp,
+                                                                 float* __restrict__ K)
 {
+    constexpr int kSpan = kGramRows + 16;
     __shared__ float xv[kGramColsPerBlock][kMaxFeatures];
+    __shared__ float xu[kSpan][33];
     const int vb = v_first + blockIdx.y * kGramColsPerBlock;
+    const int ncols = min(kGramColsPerBlock, v_first + nV - vb);
+    const int i0 = blockIdx.x * kGramRows;
+    const int u_lo = column_base(vb, cap) + i0;
     for (int idx = threadIdx.x; idx < kGramColsPerBlock * D; idx += blockDim.x) {
-        int c = idx / D, d = idx % D;
-        int v = vb + c;
-        xv[c][d] = (v < v_first + nV) ? X[size_t(v) * Dp + d] : 0.f;
+        const int c = idx / D, d = idx % D;
+        xv[c][d] = c < ncols ? X[size_t(vb + c) * Dp + d] : 0.f;
     }
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= Lk) return;
-    for (int c = 0; c < kGramColsPerBlock; ++c) {
-        const int v = vb + c;
-        if (v >= v_first + nV) break;
-        const int u = column_base(v, cap) + i;
-        float val = 0.f;
-        if (u < nU) {
-            const float* xu = X + size_t(u) * Dp;
-            float acc = 0.f;
-            for (int d = 0; d < D; ++d) {
-                float diff = __ldg(xu + d) - xv[c][d];
-                acc = fmaf(diff, diff, acc);
-            }
-            val = __fmul_rn(mp.wG, expf(__fmul_rn(mp.ew, acc)));
+    const int i = i0 + threadIdx.x;
+    float acc[kGramColsPerBlock];
+#pragma unroll
+    for (int c = 0; c < kGramColsPerBlock; ++c) acc[c] = 0.f;
+    for (int d0 = 0; d0 < D; d0 += 32) {
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < kSpan * 32; idx += blockDim.x) {
+            const int r = idx >> 5, d = idx & 31;
+            const int u = u_lo + r;
+            xu[r][d] = (u < nU && d0 + d < D) ? X[size_t(u) * Dp + d0 + d] : 0.f;
         }
+        __syncthreads();
+        const int dn = min(32, D - d0);
+#pragma unroll
+        for (int c = 0; c < kGramColsPerBlock; ++c) {
+            const int r = column_base(vb + c, cap) + i - u_lo; // < kSpan
+            for (int d = 0; d < dn; ++d) {
+                const float diff = xu[r][d] - xv[c][d0 + d];
+                acc[c] = fmaf(diff, diff, acc[c]);
+            }
+        }
+    }
+    if (i >= Lk) return;
+#pragma unroll
+    for (int c = 0; c < kGramColsPerBlock; ++c) {
+        if (c >= ncols) break;
+        const int v = vb + c;
+        const int u = column_base(v, cap) + i;
+        const float val = u < nU ? __fmul_rn(mp.wG, expf(__fmul_rn(mp.ew, acc[c]))) : 0.f;
         K[size_t(v - v_first) * Lk + i] = val;
     }
 }

@@ -207,3 +207,44 @@ def test_product_matches_reference_all_users_config1(oracle_mod):
         ser_b = L.symbol_error_rate(est[u], f.tx_data[u], f.modulation)
         ser_r = L.symbol_error_rate(er[u], f.tx_data[u], f.modulation)
         assert abs(ser_b - ser_r) <= 2.0 / f.tx_data.shape[1]
+
+
+# ------------------------------------------------ incremental training sweep --
+# "trainVersion": "incremental" keeps each window row's Gaussian sum up to date
+# instead of re-summing it in the reference's order; the FP32 bar (1e-4
+# relative) applies.
+
+@pytest.mark.parametrize("name,cfg,frame", CASES, ids=[c[0] for c in CASES])
+def test_incremental_sweep_matches_oracle(oracle_mod, name, cfg, frame):
+    seed, K, N, P, S, mod = frame
+    f = synth.generate_frame(seed, K=K, N=N, P=P, S=S, modulation=mod, snr_db=20)
+    det, est = run_product(dict(cfg, trainVersion="incremental"), f)
+    o, eo = run_oracle(oracle_mod, cfg, f)
+    assert det.rows() == o.rows()
+    assert_soft_close(est, eo)
+    assert_hard_equal(est, eo, f.modulation)
+
+
+def test_incremental_sweep_second_train_and_users(oracle_mod):
+    f = synth.generate_frame(20, K=3, N=6, P=150, S=100, modulation="QAM16")
+    g = synth.generate_frame(21, K=3, N=6, P=70, S=10, modulation="QAM16")
+    for cfg in (BASE, dict(BASE, dictionarySize=100)):
+        det = L.NomaDetectorFactory.build(dict(cfg, trainVersion="incremental"), 6, num_users=3)
+        det.train(f.rx_train, f.tx_train)
+        det.train(g.rx_train, g.tx_train)
+        est, _ = det.detect(f.rx_data)
+        for u in range(3):
+            o = oracle_mod.OracleDetector(cfg, 6, oracle_mod.F32)
+            o.train(f.rx_train, f.tx_train[u])
+            o.train(g.rx_train, g.tx_train[u])
+            assert_soft_close(est[u], o.detect(f.rx_data))
+
+
+def test_incremental_sweep_config1_all_users(oracle_mod):
+    f = synth.config1_frame()
+    cfg = synth.CONFIG1_ALGORITHM
+    _, est = run_product(dict(cfg, trainVersion="incremental"), f, users=8)
+    for u in (0, 7):
+        _, eo = run_oracle(oracle_mod, cfg, f, u=u)
+        assert_soft_close(est[u], eo)
+        assert_hard_equal(est[u], eo, f.modulation)
