@@ -117,6 +117,8 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     torch.cuda.set_device(dev)
     frame = synth.config1_frame(seed=1 + rank)
     cfg = dict(synth.CONFIG1_ALGORITHM)
+    if args.detect_version:
+        cfg["detectVersion"] = args.detect_version
     U, N = frame.tx_train.shape[0], frame.rx_train.shape[0]
     P, S = frame.rx_train.shape[1], frame.rx_data.shape[1]
     det = L.NomaDetectorFactory.build(cfg, N, num_users=U)
@@ -126,7 +128,9 @@ def run_b200(args, rank: int, world: int) -> dict | None:
     rxd = torch.from_numpy(frame.rx_data).cuda()
     est = torch.empty((U, S), dtype=torch.complex64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    launches_per_step = 6  # pack pilots, gather targets, kernel columns, sweep, pack data, detect
+    # pack pilots, gather targets, kernel columns, sweep, pack data, detect
+    # (+ operand packing x2, coefficients, reduction for the tensor-core detect)
+    launches_per_step = 10 if cfg.get("detectVersion", "").startswith("gram") else 6
 
     def step():
         det.reset_state()
@@ -211,13 +215,16 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         "metric": METRIC, "value": symbols / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded NOMA frames; no public dataset)",
-        "config": dict(WORKLOAD, parallelism=f"replicas x{world}"),
+        "config": dict(WORKLOAD, parallelism=f"replicas x{world}", detect_version=cfg.get("detectVersion", "balanced")),
         "e2e": {"value": symbols / (e2e_ms / args.steps * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h_rx.numel() * 8 + h_tx.numel() * 8 + h_rxd.numel() * 8),
                 "d2h_bytes_per_step": int(h_est.numel() * 8), "ms_per_step": e2e_ms / args.steps},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "kernel": "train_exact_kernel (training sweep)", "achieved": achieved,
-                     "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs, "traffic": None,
+                     "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
+                     # dram read + write of one sweep launch on this workload, ncu
+                     # (profiles/train_sweep_kernel_config1_frame.md): the kernel columns
+                     "traffic": 9772544,
                      "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": sweep,
                      "note": "sweep is a chain of P dependent steps; latency-bound, see DESIGN.md",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
@@ -302,6 +309,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--detect-version", default=None,
+                    help="detectVersion of the algorithm config (default: the reference's 'balanced')")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
