@@ -119,6 +119,77 @@ apsm_status apsm_last_kernel_ms(apsm_detector* h, float* sweep_ms, float* detect
 /* Last error message of the handle ("" if none). */
 const char* apsm_last_error(const apsm_detector* h);
 
+/* ======================================================================
+ * Detector pool: many resident detectors (users x cells), batched jobs.
+ *
+ * The reference runs one ApsmNomaDetector per user, each with its own
+ * stream, host thread and calls (its CLI's -p mode, noma_detect.cpp:109-112;
+ * one train/detect per detector, noma_detector.cuh:65-75).  A pool holds the
+ * device state of many detectors of one algorithm config (each with its own
+ * antenna count) and runs a batch of their train/detect calls in a handful
+ * of launches: every training job of the batch in one persistent sweep
+ * launch, every detection job in one launch per antenna class.  Per detector
+ * the semantics are those of NomaDetector::train / detect; results equal the
+ * single-detector path within the FP32 tolerance (1e-4 relative).
+ *
+ * Restrictions: otype "APSM" without llsInitialization or normConstraint,
+ * gaussianKernelVariance > 0, even sampleStep <= 8, dictionarySize >=
+ * windowSize + sampleStep / 2, N <= 64 antennas.
+ * ==================================================================== */
+typedef struct apsm_pool apsm_pool;
+
+typedef enum { APSM_JOB_TRAIN = 0, APSM_JOB_DETECT = 1 } apsm_job_kind;
+
+typedef struct {
+    uint32_t detector; /* id from apsm_pool_add */
+    uint32_t kind;     /* apsm_job_kind */
+    uint32_t length;   /* pilots P (train) or data symbols S (detect) */
+    uint32_t reserved; /* 0 */
+    const float* rx;   /* N x length complex64, antenna-major (NomaDetector's rxSig[N][length]) */
+    const float* tx;   /* train: length complex64 pilots of this detector's user; detect: NULL */
+    float* est;        /* detect: length complex64 soft estimates (output); train: NULL */
+} apsm_job;
+
+/* A pool for one algorithm config.  hbm_budget_bytes bounds the device memory
+ * of resident detector state plus batch scratch (0: no bound).  lanes >= 1
+ * independent streams, each with its own scratch, so batches can overlap. */
+apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm_budget_bytes, uint32_t lanes,
+                             apsm_pool** out, char* err, size_t errlen);
+void apsm_pool_destroy(apsm_pool* p);
+
+/* Resident detector with num_antennas antennas (fresh state, like resetState);
+ * APSM_ERR_OUT_OF_MEMORY if its state does not fit the budget. */
+apsm_status apsm_pool_add(apsm_pool* p, uint32_t num_antennas, uint32_t* detector);
+apsm_status apsm_pool_remove(apsm_pool* p, uint32_t detector);
+apsm_status apsm_pool_reset(apsm_pool* p, uint32_t detector);
+
+/* Runs a batch on a lane: all training jobs first (in one sweep launch; a
+ * detector may be trained at most once per batch), then all detection jobs,
+ * which see this batch's training.  device_buffers != 0: rx/tx/est are device
+ * pointers and the call returns once the work is enqueued on the lane's
+ * stream (apsm_pool_wait / apsm_pool_query); otherwise host buffers, staged
+ * through the lane and the call returns when the estimates are written.  A
+ * detector must not be in batches on two lanes at once. */
+apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs, int device_buffers);
+apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane);
+/* 1 when the lane is idle, 0 while its last batch runs, < 0 on error. */
+int apsm_pool_query(apsm_pool* p, uint32_t lane);
+void* apsm_pool_stream(apsm_pool* p, uint32_t lane);
+
+/* Device scratch bytes the job needs in a batch (admission by HBM budget),
+ * the pool's budget and the bytes currently held (resident + scratch). */
+uint64_t apsm_pool_job_bytes(const apsm_pool* p, const apsm_job* job);
+uint64_t apsm_pool_budget(const apsm_pool* p);
+uint64_t apsm_pool_bytes_in_use(const apsm_pool* p);
+
+/* GPU time (ms, CUDA events) of the lane's last batch: training (kernel
+ * columns + sweep) and detection stages; blocks until the batch finished. */
+apsm_status apsm_pool_last_ms(apsm_pool* p, uint32_t lane, float* train_ms, float* detect_ms);
+
+/* Snapshot of a detector: rows in use, a (rows), w (2N); pointers may be NULL. */
+apsm_status apsm_pool_get_state(apsm_pool* p, uint32_t detector, uint32_t* rows, float* a, float* w);
+const char* apsm_pool_last_error(const apsm_pool* p);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,23 @@ SIGNATURES = [
     ("apsm_get_state", ctypes.c_int, [_P, _P, _P, _P]),
     ("apsm_last_kernel_ms", ctypes.c_int, [_P, _F, _F]),
     ("apsm_last_error", ctypes.c_char_p, [_P]),
+    # detector pool (batched many-detector form)
+    ("apsm_pool_create", ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, _U32, ctypes.POINTER(_P), ctypes.c_char_p,
+                                        ctypes.c_size_t]),
+    ("apsm_pool_destroy", None, [_P]),
+    ("apsm_pool_add", ctypes.c_int, [_P, _U32, ctypes.POINTER(_U32)]),
+    ("apsm_pool_remove", ctypes.c_int, [_P, _U32]),
+    ("apsm_pool_reset", ctypes.c_int, [_P, _U32]),
+    ("apsm_pool_run", ctypes.c_int, [_P, _U32, _P, _U32, ctypes.c_int]),
+    ("apsm_pool_wait", ctypes.c_int, [_P, _U32]),
+    ("apsm_pool_query", ctypes.c_int, [_P, _U32]),
+    ("apsm_pool_stream", _P, [_P, _U32]),
+    ("apsm_pool_job_bytes", ctypes.c_uint64, [_P, _P]),
+    ("apsm_pool_budget", ctypes.c_uint64, [_P]),
+    ("apsm_pool_bytes_in_use", ctypes.c_uint64, [_P]),
+    ("apsm_pool_last_ms", ctypes.c_int, [_P, _U32, _F, _F]),
+    ("apsm_pool_get_state", ctypes.c_int, [_P, _U32, ctypes.POINTER(_U32), _P, _P]),
+    ("apsm_pool_last_error", ctypes.c_char_p, [_P]),
 ]
 
 _lib = None

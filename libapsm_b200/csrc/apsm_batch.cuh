@@ -1,0 +1,113 @@
+// Batched (many-detector) APSM kernels: descriptors and declarations.
+//
+// The batched form works on complex samples ("pairs"): universe pair b is the
+// complex received vector y_b (N antennas) behind the reference's two Dedup
+// rows 2b = [Re y_b; Im y_b] and 2b+1 = [Im y_b; -Re y_b]
+// (cpp/lib/cuda/cuda_matrix_device.cuh:180-188, :288-296).  For two pairs
+// b, n with r + i m = y_b^H y_n and squared norms n_b, n_n the four Gaussian
+// kernel values of their rows take three distinct values:
+//   K(2b, 2n)   = K(2b+1, 2n+1) = wG exp(ew (n_b + n_n - 2 r))   "A"
+//   K(2b, 2n+1)                 = wG exp(ew (n_b + n_n - 2 m))   "Bp"
+//   K(2b+1, 2n)                 = wG exp(ew (n_b + n_n + 2 m))   "Bm"
+// and the linear kernel <x_2b, x_2n> = <x_2b+1, x_2n+1> = r,
+// <x_2b, x_2n+1> = m, <x_2b+1, x_2n> = -m.
+#pragma once
+
+#include "apsm_common.cuh"
+
+namespace apsm {
+
+// Settings shared by every job of a batch (one algorithm config).
+struct BatchCommon {
+    float wL, wG, eB;
+    int qP;   // window length in pairs (windowSize)
+    int sp;   // pairs entering per step (sampleStep / 2)
+    int LB;   // band length of a column: qP + sp
+    int XSP;  // pair slots of the sweep's window ring: qP + 2 sp
+    int XSPp; // pitch (floats) of the window kernel planes, multiple of 4, >= XSP
+    int Np;   // largest complex row pitch of the jobs (float2 units)
+};
+
+// One training job: a detector's universe (dictionary pairs already present,
+// then the new pilots) swept by one CTA.
+struct BatchTrainJob {
+    const float2* Y;     // nP x Np universe samples (pair b = complex y_b)
+    const float* nrm;    // nP squared norms
+    const float* y;      // 2 nP targets (row form: Re x, Im x)
+    float* a;            // 2 nP coefficients (row form); in: old rows, out: visible rows
+    float* w;            // 2N linear weights (in/out)
+    const float4* Kc;    // kernel columns (A, Bp, Bm, 0), pairs n in [n_first, nP)
+    const float4* band;  // (nP - n_first) x LB window kernel values (A + wL r, Bp + wL m, Bm - wL m, 0)
+    const TrainStep* steps;
+    int n_steps;
+    int nP, N, Np, capP; // universe pairs, antennas, row pitch (float2), dictionary capacity in pairs
+    int n_first;         // first pair with a kernel column
+    int used_beforeP;    // pairs present before this call
+    long long kc_base;   // column_prefix(n_first)
+    float ew;            // -0.5 / (variance * N^2)
+    int err;             // unused by the kernels (host bookkeeping)
+};
+
+// Column n holds pairs [col_begin(n), col_end(n)).
+__host__ __device__ inline int col_begin(int n, int capP) { return n + 1 - capP > 0 ? n + 1 - capP : 0; }
+__host__ __device__ inline int col_end(int n, int qP, int nP) { return n + qP < nP ? n + qP : nP; }
+
+// Sum of the column lengths of pairs [0, n) (closed form of the clamped ramps).
+__host__ __device__ inline long long column_prefix(long long n, long long qP, long long nP, long long capP)
+{
+    long long k = nP - qP;
+    if (k < 0) k = 0;
+    if (k > n) k = n;
+    const long long s1 = k * qP + k * (k - 1) / 2 + (n - k) * nP;
+    const long long j = n - capP > 0 ? n - capP : 0;
+    return s1 - j * (j + 1) / 2;
+}
+
+// One detection job: S data samples of one detector against its dictionary.
+struct BatchDetectJob {
+    const float2* Ys;   // S x Np data samples
+    const float* nrm_s; // S squared norms
+    const float2* Yd;   // Mp x Np dictionary samples
+    const float* nrm_d; // Mp norms
+    const float* a;     // 2 Mp coefficients (row form)
+    const float* w;     // 2N linear weights
+    float2* out;        // S soft estimates (Re = f(row 2s), Im = f(row 2s+1))
+    int S, Mp, N, Np;
+    float ew;
+};
+
+// Packing of complex samples: antenna-major rx (N x L complex) -> L x Np pairs + norms.
+struct BatchPackJob {
+    const float2* rx;   // N x L
+    const float2* tx;   // L targets or null
+    const int* perm;    // sample order or null
+    float2* Y;          // destination pairs
+    float* nrm;         // destination norms
+    float* y;           // destination targets (2 per sample) or null
+    float* a;           // coefficients to zero (2 per sample) or null
+    int L, N, Np;
+};
+
+// Copy of a detector's resident dictionary into (or out of) a universe.
+struct BatchCopyJob {
+    const float2* Ysrc; const float* nsrc; const float* ysrc; const float* asrc;
+    float2* Ydst; float* ndst; float* ydst; float* adst;
+    int pairs, Np;
+};
+
+// max_n: largest antenna count of the jobs (sizes the kernel's shared memory)
+cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s);
+cudaError_t launch_batch_copy(const BatchCopyJob* d_jobs, int n_jobs, int max_pairs, int max_np, cudaStream_t s);
+cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, int n_jobs, int max_cols, int max_n, BatchCommon cm,
+                              cudaStream_t s);
+size_t batch_sweep_smem(const BatchCommon& cm);
+int batch_sweep_threads();
+cudaError_t batch_sweep_occupancy(const BatchCommon& cm, int* ctas_per_sm);
+cudaError_t launch_batch_sweep(const BatchTrainJob* d_jobs, int n_jobs, BatchCommon cm, int grid, int* d_counter,
+                               int* d_err, cudaStream_t s);
+// Jobs of one antenna class (N <= nmax, nmax in {4, 8, 16, 32, 64}).
+cudaError_t launch_batch_detect(const BatchDetectJob* d_jobs, int n_jobs, int max_tiles, int nmax, float wL, float wG,
+                                cudaStream_t s);
+int batch_detect_tile(); // samples per block of launch_batch_detect
+
+} // namespace apsm

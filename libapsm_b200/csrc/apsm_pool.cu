@@ -1,0 +1,715 @@
+// Detector pool: resident state of many detectors and batched train/detect
+// (the apsm_pool_* entry points of include/apsm_b200.h).
+//
+// A batch is laid out in one scratch buffer of its lane: the job descriptors
+// (filled in a pinned host buffer, one copy), the staged host inputs, each
+// training job's universe (its dictionary pairs, then the new pilots), kernel
+// columns and bands, and each detection job's packed samples.  Launch order
+// on the lane's stream: dictionary -> universe copies, packing, kernel
+// columns, the persistent sweep, universe tail -> dictionary copies, then the
+// detection launches (one per antenna class).
+#include "apsm_batch.cuh"
+#include "apsm_host.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace apsm;
+
+namespace {
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct PoolDet {
+    bool live = false;
+    uint32_t N = 0, Np = 0, cap = 0, capP = 0;
+    uint32_t used = 0; // rows (2 per complex entry)
+    float ew = 0.f;
+    void* mem = nullptr;
+    size_t bytes = 0;
+    float2* Y = nullptr; // capP x Np dictionary pairs, oldest first
+    float* nrm = nullptr;
+    float* y = nullptr; // cap targets
+    float* a = nullptr; // cap coefficients
+    float* w = nullptr; // 2N
+};
+
+struct Lane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr}; // train start/end, detect start/end
+    cudaEvent_t done = nullptr;                                // end of the last batch
+    cudaEvent_t desc_copied = nullptr;                         // the pinned descriptors were consumed
+    bool have_train = false, have_detect = false;
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+int detect_class(uint32_t N)
+{
+    for (int c : {4, 8, 16, 32, 64})
+        if (int(N) <= c) return c;
+    return 0;
+}
+
+} // namespace
+
+struct apsm_pool {
+    Config cfg;
+    BatchCommon cm{};
+    uint64_t budget = 0;
+    uint64_t resident = 0;
+    std::vector<PoolDet> dets;
+    std::vector<Lane> lanes;
+    int device = 0, sms = 0, sweep_ctas = 1;
+    std::string last_error;
+    std::mutex mu;
+    std::map<uint32_t, std::vector<int>> perms;
+
+    ~apsm_pool();
+    apsm_status fail(apsm_status st, const std::string& msg)
+    {
+        last_error = msg;
+        return st;
+    }
+    apsm_status cuda_fail(cudaError_t e, const char* what)
+    {
+        cudaGetLastError();
+        last_error = std::string(what) + ": " + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? APSM_ERR_OUT_OF_MEMORY : APSM_ERR_CUDA;
+    }
+    uint64_t in_use() const
+    {
+        uint64_t s = resident;
+        for (const auto& l : lanes) s += l.scratch_bytes;
+        return s;
+    }
+    size_t train_bytes(const PoolDet& d, uint32_t P, bool host) const;
+    size_t detect_bytes(const PoolDet& d, uint32_t S, bool host) const;
+    apsm_status run(uint32_t lane, const apsm_job* jobs, uint32_t n, bool device_buffers);
+};
+
+#define POOL_CK(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) return p->cuda_fail(e_, #call);                         \
+    } while (0)
+
+apsm_pool::~apsm_pool()
+{
+    for (auto& l : lanes) {
+        if (l.stream) cudaStreamSynchronize(l.stream);
+        if (l.scratch) cudaFree(l.scratch);
+        if (l.pinned) cudaFreeHost(l.pinned);
+        for (auto& e : l.ev)
+            if (e) cudaEventDestroy(e);
+        if (l.done) cudaEventDestroy(l.done);
+        if (l.desc_copied) cudaEventDestroy(l.desc_copied);
+        if (l.stream) cudaStreamDestroy(l.stream);
+    }
+    for (auto& d : dets)
+        if (d.mem) cudaFree(d.mem);
+}
+
+namespace {
+
+// Bytes of a detector's resident state and its sub-buffer offsets.
+size_t resident_layout(uint32_t N, uint32_t capP, size_t off[5])
+{
+    const uint32_t Np = round_up(N, 2);
+    size_t o = 0;
+    off[0] = o; o = align_up(o + sizeof(float2) * size_t(capP) * Np, 256);
+    off[1] = o; o = align_up(o + sizeof(float) * capP, 256);
+    off[2] = o; o = align_up(o + sizeof(float) * 2 * capP, 256);
+    off[3] = o; o = align_up(o + sizeof(float) * 2 * capP, 256);
+    off[4] = o; o = align_up(o + sizeof(float) * 2 * N, 256);
+    return o;
+}
+
+struct TrainPlan {
+    uint32_t job = 0; // index in the caller's list
+    PoolDet* det = nullptr;
+    std::vector<TrainStep> steps;
+    int final_hi = 0;
+    uint32_t P = 0, usedP = 0, nP = 0, n_first = 0;
+    long long kc_base = 0, n_kc = 0;
+    size_t off_rx = 0, off_tx = 0, off_Y = 0, off_nrm = 0, off_y = 0, off_a = 0, off_kc = 0, off_band = 0;
+    size_t off_steps = 0;
+    uint32_t usedP_new = 0, lo_new = 0;
+    const int* perm_dev = nullptr;
+    size_t perm_off = 0;
+};
+
+struct DetectPlan {
+    uint32_t job = 0;
+    PoolDet* det = nullptr;
+    uint32_t S = 0, Mp = 0;
+    int cls = 0;
+    size_t off_rx = 0, off_Y = 0, off_nrm = 0, off_est = 0;
+};
+
+} // namespace
+
+size_t apsm_pool::train_bytes(const PoolDet& d, uint32_t P, bool host) const
+{
+    const size_t usedP = d.used / 2, nP = usedP + P;
+    const size_t q = size_t(cm.qP);
+    size_t b = 0;
+    if (host) b += align_up(sizeof(float2) * d.N * P, 256) + align_up(sizeof(float2) * P, 256);
+    b += align_up(sizeof(float2) * nP * d.Np, 256) + align_up(sizeof(float) * nP, 256) +
+         2 * align_up(sizeof(float) * 2 * nP, 256);
+    // kernel columns: at most min(capP, nP) + q entries per pair of the first window onwards
+    const size_t first = usedP > q ? usedP - q : 0;
+    const size_t cols = nP - first;
+    const size_t len = std::min<size_t>(d.capP, nP) + q;
+    b += align_up(sizeof(float4) * cols * len, 256) + align_up(sizeof(float4) * cols * cm.LB, 256);
+    b += align_up(sizeof(TrainStep) * (size_t(cfg.passes) * (P + q + 2) + 4), 256) + align_up(sizeof(int) * P, 256);
+    b += 4 * sizeof(BatchTrainJob) + 4 * sizeof(BatchPackJob) + 4 * sizeof(BatchCopyJob);
+    return b;
+}
+
+size_t apsm_pool::detect_bytes(const PoolDet& d, uint32_t S, bool host) const
+{
+    size_t b = align_up(sizeof(float2) * size_t(S) * d.Np, 256) + align_up(sizeof(float) * S, 256);
+    if (host) b += align_up(sizeof(float2) * size_t(d.N) * S, 256) + align_up(sizeof(float2) * S, 256);
+    return b + sizeof(BatchDetectJob) + sizeof(BatchPackJob);
+}
+
+apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, bool device_buffers)
+{
+    apsm_pool* p = this;
+    Lane& L = lanes[lane_id];
+    const bool host = !device_buffers;
+    const uint32_t cap = 2 * cfg.dict_size;
+
+    // ---------- validate ----------
+    std::vector<char> trained(dets.size(), 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        const apsm_job& j = jobs[i];
+        if (j.detector >= dets.size() || !dets[j.detector].live)
+            return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": unknown detector");
+        if (j.kind != APSM_JOB_TRAIN && j.kind != APSM_JOB_DETECT)
+            return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": unknown kind");
+        if (j.length == 0) continue;
+        if (!j.rx) return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null rx");
+        if (j.kind == APSM_JOB_TRAIN) {
+            if (!j.tx) return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null tx");
+            if (trained[j.detector])
+                return fail(APSM_ERR_INVALID_ARGUMENT, "detector " + std::to_string(j.detector) +
+                                                           " is trained twice in one batch");
+            trained[j.detector] = 1;
+        } else if (!j.est) {
+            return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null est");
+        }
+    }
+
+    // ---------- plan (sizes and offsets) ----------
+    std::vector<TrainPlan> tp;
+    std::vector<DetectPlan> dp;
+    for (uint32_t i = 0; i < n; ++i)
+        if (jobs[i].kind == APSM_JOB_TRAIN && jobs[i].length > 0) {
+            TrainPlan t;
+            t.job = i;
+            t.det = &dets[jobs[i].detector];
+            t.P = jobs[i].length;
+            t.steps = build_schedule(cfg, t.det->used, t.P, cap, &t.final_hi);
+            t.usedP = t.det->used / 2;
+            t.nP = t.usedP + t.P;
+            t.n_first = t.steps.empty() ? t.nP : uint32_t(t.steps[0].hi - t.steps[0].wk) / 2;
+            t.kc_base = column_prefix(t.n_first, cm.qP, t.nP, t.det->capP);
+            t.n_kc = column_prefix(t.nP, cm.qP, t.nP, t.det->capP) - t.kc_base;
+            const uint32_t fhP = uint32_t(t.final_hi) / 2;
+            t.usedP_new = std::min(fhP, t.det->capP);
+            t.lo_new = fhP - t.usedP_new;
+            tp.push_back(std::move(t));
+        }
+    // longest sweeps first (the persistent kernel takes jobs in this order)
+    std::stable_sort(tp.begin(), tp.end(),
+                     [](const TrainPlan& x, const TrainPlan& y) { return x.steps.size() > y.steps.size(); });
+    // dictionary sizes after this batch's training, for the detection jobs
+    std::vector<uint32_t> used_after(dets.size());
+    for (size_t d = 0; d < dets.size(); ++d) used_after[d] = dets[d].used;
+    for (const auto& t : tp) used_after[jobs[t.job].detector] = 2 * t.usedP_new;
+    for (uint32_t i = 0; i < n; ++i)
+        if (jobs[i].kind == APSM_JOB_DETECT && jobs[i].length > 0) {
+            DetectPlan d;
+            d.job = i;
+            d.det = &dets[jobs[i].detector];
+            d.S = jobs[i].length;
+            d.Mp = used_after[jobs[i].detector] / 2;
+            d.cls = detect_class(d.det->N);
+            dp.push_back(d);
+        }
+    std::stable_sort(dp.begin(), dp.end(), [](const DetectPlan& x, const DetectPlan& y) { return x.cls < y.cls; });
+
+    const size_t nT = tp.size(), nD = dp.size();
+    size_t nCopyIn = 0;
+    for (const auto& t : tp) nCopyIn += t.usedP > 0;
+    const size_t nPack = nT + nD;
+    // descriptor region
+    size_t o = 0;
+    const size_t off_tj = o; o = align_up(o + sizeof(BatchTrainJob) * nT, 256);
+    const size_t off_dj = o; o = align_up(o + sizeof(BatchDetectJob) * nD, 256);
+    const size_t off_pj = o; o = align_up(o + sizeof(BatchPackJob) * nPack, 256);
+    const size_t off_ci = o; o = align_up(o + sizeof(BatchCopyJob) * nCopyIn, 256);
+    const size_t off_co = o; o = align_up(o + sizeof(BatchCopyJob) * nT, 256);
+    for (auto& t : tp) {
+        t.off_steps = o;
+        o = align_up(o + sizeof(TrainStep) * t.steps.size(), 16);
+    }
+    std::map<uint32_t, size_t> perm_off;
+    if (cfg.shuffle)
+        for (auto& t : tp) {
+            if (!perm_off.count(t.P)) {
+                perm_off[t.P] = o;
+                o = align_up(o + sizeof(int) * t.P, 16);
+                if (!perms.count(t.P)) perms[t.P] = shuffle_permutation(t.P);
+            }
+            t.perm_off = perm_off[t.P];
+        }
+    o = align_up(o, 256);
+    const size_t desc_bytes = o;
+    const size_t off_counter = o; o = align_up(o + 256, 256);
+    for (auto& t : tp) {
+        const PoolDet& d = *t.det;
+        if (host) {
+            t.off_rx = o; o = align_up(o + sizeof(float2) * size_t(d.N) * t.P, 256);
+            t.off_tx = o; o = align_up(o + sizeof(float2) * t.P, 256);
+        }
+        t.off_Y = o; o = align_up(o + sizeof(float2) * size_t(t.nP) * d.Np, 256);
+        t.off_nrm = o; o = align_up(o + sizeof(float) * t.nP, 256);
+        t.off_y = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
+        t.off_a = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
+        t.off_kc = o; o = align_up(o + sizeof(float4) * size_t(std::max<long long>(t.n_kc, 1)), 256);
+        t.off_band = o; o = align_up(o + sizeof(float4) * size_t(t.nP - t.n_first + 1) * cm.LB, 256);
+    }
+    for (auto& d : dp) {
+        if (host) {
+            d.off_rx = o; o = align_up(o + sizeof(float2) * size_t(d.det->N) * d.S, 256);
+            d.off_est = o; o = align_up(o + sizeof(float2) * d.S, 256);
+        }
+        d.off_Y = o; o = align_up(o + sizeof(float2) * size_t(d.S) * d.det->Np, 256);
+        d.off_nrm = o; o = align_up(o + sizeof(float) * d.S, 256);
+    }
+    const size_t scratch_need = o;
+
+    // ---------- memory ----------
+    if (scratch_need > L.scratch_bytes) {
+        const uint64_t others = in_use() - L.scratch_bytes;
+        if (budget && others + scratch_need > budget)
+            return fail(APSM_ERR_OUT_OF_MEMORY, "batch needs " + std::to_string(scratch_need) +
+                                                    " scratch bytes; the HBM budget leaves " +
+                                                    std::to_string(budget > others ? budget - others : 0));
+        POOL_CK(cudaStreamSynchronize(L.stream));
+        if (L.scratch) POOL_CK(cudaFree(L.scratch));
+        L.scratch = nullptr;
+        L.scratch_bytes = 0;
+        POOL_CK(cudaMalloc(&L.scratch, scratch_need));
+        L.scratch_bytes = scratch_need;
+    }
+    if (desc_bytes > L.pinned_bytes) {
+        POOL_CK(cudaEventSynchronize(L.desc_copied));
+        if (L.pinned) POOL_CK(cudaFreeHost(L.pinned));
+        L.pinned = nullptr;
+        L.pinned_bytes = 0;
+        POOL_CK(cudaMallocHost(&L.pinned, std::max<size_t>(desc_bytes, 1 << 16)));
+        L.pinned_bytes = std::max<size_t>(desc_bytes, 1 << 16);
+    }
+    POOL_CK(cudaEventSynchronize(L.desc_copied)); // the previous batch's descriptors were consumed
+    char* dev = static_cast<char*>(L.scratch);
+    char* hst = static_cast<char*>(L.pinned);
+    auto D = [&](size_t off) { return dev + off; };
+
+    // ---------- descriptors ----------
+    auto* h_tj = reinterpret_cast<BatchTrainJob*>(hst + off_tj);
+    auto* h_dj = reinterpret_cast<BatchDetectJob*>(hst + off_dj);
+    auto* h_pj = reinterpret_cast<BatchPackJob*>(hst + off_pj);
+    auto* h_ci = reinterpret_cast<BatchCopyJob*>(hst + off_ci);
+    auto* h_co = reinterpret_cast<BatchCopyJob*>(hst + off_co);
+    size_t ipack = 0, icopy = 0;
+    int max_len = 0, max_np = 1, max_cols = 0, max_n = 1, max_pairs_in = 0, max_pairs_out = 0;
+    for (size_t k = 0; k < nT; ++k) {
+        TrainPlan& t = tp[k];
+        PoolDet& d = *t.det;
+        const apsm_job& j = jobs[t.job];
+        std::memcpy(hst + t.off_steps, t.steps.data(), sizeof(TrainStep) * t.steps.size());
+        const float2* rx = host ? reinterpret_cast<const float2*>(D(t.off_rx)) : reinterpret_cast<const float2*>(j.rx);
+        const float2* tx = host ? reinterpret_cast<const float2*>(D(t.off_tx)) : reinterpret_cast<const float2*>(j.tx);
+        auto* Y = reinterpret_cast<float2*>(D(t.off_Y));
+        auto* nrm = reinterpret_cast<float*>(D(t.off_nrm));
+        auto* yv = reinterpret_cast<float*>(D(t.off_y));
+        auto* av = reinterpret_cast<float*>(D(t.off_a));
+        if (t.usedP > 0) {
+            h_ci[icopy++] = BatchCopyJob{d.Y, d.nrm, d.y, d.a, Y, nrm, yv, av, int(t.usedP), int(d.Np)};
+            max_pairs_in = std::max(max_pairs_in, int(t.usedP));
+        }
+        const int* perm = cfg.shuffle ? reinterpret_cast<const int*>(D(t.perm_off)) : nullptr;
+        h_pj[ipack++] = BatchPackJob{rx, tx, perm, Y + size_t(t.usedP) * d.Np, nrm + t.usedP, yv + 2 * t.usedP,
+                                     av + 2 * t.usedP, int(t.P), int(d.N), int(d.Np)};
+        max_len = std::max(max_len, int(t.P));
+        max_np = std::max(max_np, int(d.Np));
+        max_n = std::max(max_n, int(d.N));
+        BatchTrainJob tj{};
+        tj.Y = Y;
+        tj.nrm = nrm;
+        tj.y = yv;
+        tj.a = av;
+        tj.w = d.w;
+        tj.Kc = reinterpret_cast<const float4*>(D(t.off_kc));
+        tj.band = reinterpret_cast<const float4*>(D(t.off_band));
+        tj.steps = reinterpret_cast<const TrainStep*>(D(t.off_steps));
+        tj.n_steps = int(t.steps.size());
+        tj.nP = int(t.nP);
+        tj.N = int(d.N);
+        tj.Np = int(d.Np);
+        tj.capP = int(d.capP);
+        tj.n_first = int(t.n_first);
+        tj.used_beforeP = int(t.usedP);
+        tj.kc_base = t.kc_base;
+        tj.ew = d.ew;
+        h_tj[k] = tj;
+        max_cols = std::max(max_cols, int(t.nP - t.n_first));
+        h_co[k] = BatchCopyJob{Y + size_t(t.lo_new) * d.Np, nrm + t.lo_new, yv + 2 * t.lo_new, av + 2 * t.lo_new,
+                               d.Y, d.nrm, d.y, d.a, int(t.usedP_new), int(d.Np)};
+        max_pairs_out = std::max(max_pairs_out, int(t.usedP_new));
+    }
+    for (auto& kv : perm_off) std::memcpy(hst + kv.second, perms[kv.first].data(), sizeof(int) * kv.first);
+    const size_t pack_train = ipack;
+    for (size_t k = 0; k < nD; ++k) {
+        DetectPlan& q = dp[k];
+        PoolDet& d = *q.det;
+        const apsm_job& j = jobs[q.job];
+        const float2* rx = host ? reinterpret_cast<const float2*>(D(q.off_rx)) : reinterpret_cast<const float2*>(j.rx);
+        auto* Ys = reinterpret_cast<float2*>(D(q.off_Y));
+        auto* ns = reinterpret_cast<float*>(D(q.off_nrm));
+        h_pj[ipack++] = BatchPackJob{rx, nullptr, nullptr, Ys, ns, nullptr, nullptr, int(q.S), int(d.N), int(d.Np)};
+        max_len = std::max(max_len, int(q.S));
+        max_np = std::max(max_np, int(d.Np));
+        max_n = std::max(max_n, int(d.N));
+        float2* out = host ? reinterpret_cast<float2*>(D(q.off_est)) : reinterpret_cast<float2*>(j.est);
+        h_dj[k] = BatchDetectJob{Ys, ns, d.Y, d.nrm, d.a, d.w, out, int(q.S), int(q.Mp), int(d.N), int(d.Np), d.ew};
+    }
+    (void)pack_train;
+
+    // ---------- enqueue ----------
+    cudaStream_t s = L.stream;
+    if (host) {
+        for (const auto& t : tp) {
+            const apsm_job& j = jobs[t.job];
+            POOL_CK(cudaMemcpyAsync(D(t.off_rx), j.rx, sizeof(float2) * size_t(t.det->N) * t.P, cudaMemcpyHostToDevice, s));
+            POOL_CK(cudaMemcpyAsync(D(t.off_tx), j.tx, sizeof(float2) * t.P, cudaMemcpyHostToDevice, s));
+        }
+        for (const auto& q : dp)
+            POOL_CK(cudaMemcpyAsync(D(q.off_rx), jobs[q.job].rx, sizeof(float2) * size_t(q.det->N) * q.S,
+                                    cudaMemcpyHostToDevice, s));
+    }
+    POOL_CK(cudaMemcpyAsync(dev, hst, desc_bytes, cudaMemcpyHostToDevice, s));
+    POOL_CK(cudaEventRecord(L.desc_copied, s));
+    L.have_train = nT > 0;
+    L.have_detect = nD > 0;
+    if (nT > 0) {
+        POOL_CK(cudaEventRecord(L.ev[0], s));
+        POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_ci)), int(nCopyIn), max_pairs_in, max_np, s));
+    }
+    if (nPack > 0) POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)), int(nPack), max_len, max_n, s));
+    if (nT > 0) {
+        const auto* d_tj = reinterpret_cast<const BatchTrainJob*>(D(off_tj));
+        POOL_CK(launch_batch_kcol(d_tj, int(nT), max_cols, max_n, cm, s));
+        int* counter = reinterpret_cast<int*>(D(off_counter));
+        POOL_CK(cudaMemsetAsync(counter, 0, sizeof(int), s));
+        const int grid = int(std::min<size_t>(nT, size_t(sweep_ctas) * sms));
+        POOL_CK(launch_batch_sweep(d_tj, int(nT), cm, grid, counter, nullptr, s));
+        POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_co)), int(nT), max_pairs_out, max_np, s));
+        POOL_CK(cudaEventRecord(L.ev[1], s));
+        for (const auto& t : tp) t.det->used = 2 * t.usedP_new;
+    }
+    if (nD > 0) {
+        POOL_CK(cudaEventRecord(L.ev[2], s));
+        const auto* d_dj = reinterpret_cast<const BatchDetectJob*>(D(off_dj));
+        size_t k0 = 0;
+        while (k0 < nD) {
+            size_t k1 = k0;
+            int tiles = 0;
+            while (k1 < nD && dp[k1].cls == dp[k0].cls) {
+                tiles = std::max(tiles, int((dp[k1].S + batch_detect_tile() - 1) / batch_detect_tile()));
+                ++k1;
+            }
+            POOL_CK(launch_batch_detect(d_dj + k0, int(k1 - k0), tiles, dp[k0].cls, cfg.wL, cfg.wG, s));
+            k0 = k1;
+        }
+        POOL_CK(cudaEventRecord(L.ev[3], s));
+        if (host)
+            for (const auto& q : dp)
+                POOL_CK(cudaMemcpyAsync(jobs[q.job].est, D(q.off_est), sizeof(float2) * q.S, cudaMemcpyDeviceToHost, s));
+    }
+    POOL_CK(cudaEventRecord(L.done, s));
+    if (host) POOL_CK(cudaStreamSynchronize(s));
+    return APSM_OK;
+}
+
+// ==================================================================== ABI ==
+
+namespace {
+void copy_err(char* err, size_t errlen, const std::string& msg)
+{
+    if (err && errlen) {
+        std::strncpy(err, msg.c_str(), errlen - 1);
+        err[errlen - 1] = 0;
+    }
+}
+} // namespace
+
+extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm_budget_bytes, uint32_t lanes,
+                                        apsm_pool** out, char* err, size_t errlen)
+{
+    if (!algorithm_json || !out) {
+        copy_err(err, errlen, "null argument");
+        return APSM_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    if (lanes == 0 || lanes > 64) {
+        copy_err(err, errlen, "lanes must be in [1, 64]");
+        return APSM_ERR_INVALID_ARGUMENT;
+    }
+    Config cfg;
+    try {
+        cfg = parse_config(algorithm_json);
+    } catch (const std::exception& e) {
+        copy_err(err, errlen, e.what());
+        return APSM_ERR_INVALID_CONFIG;
+    }
+    std::string why;
+    if (cfg.otype != "APSM") why = "the detector pool runs APSM detectors only";
+    else if (cfg.lls_init) why = "llsInitialization is not available in the detector pool";
+    else if (cfg.norm_constraint > 0.f) why = "normConstraint > 0 is not available in this build";
+    else if (!(cfg.variance > 0.f)) why = "the detector pool needs gaussianKernelVariance > 0";
+    else if (cfg.step % 2 != 0 || cfg.step == 0 || cfg.step > 8) why = "the detector pool needs an even sampleStep <= 8";
+    else if (cfg.dict_size < cfg.window + cfg.step / 2) why = "the detector pool needs dictionarySize >= windowSize + sampleStep / 2";
+    else if (cfg.window == 0) why = "windowSize must be >= 1";
+    if (!why.empty()) {
+        copy_err(err, errlen, why);
+        return APSM_ERR_UNSUPPORTED;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        copy_err(err, errlen, "no CUDA device available");
+        return APSM_ERR_NO_DEVICE;
+    }
+    auto* p = new apsm_pool();
+    p->cfg = cfg;
+    p->budget = hbm_budget_bytes;
+    BatchCommon& cm = p->cm;
+    cm.wL = cfg.wL;
+    cm.wG = cfg.wG;
+    cm.eB = cfg.eB;
+    cm.qP = int(cfg.window);
+    cm.sp = int(cfg.step / 2);
+    cm.LB = cm.qP + cm.sp;
+    cm.XSP = cm.qP + 2 * cm.sp;
+    cm.XSPp = int(round_up(uint32_t(cm.XSP) + 1, 4));
+    cm.Np = 32; // sweep shared memory sized for N <= 32; larger N re-sizes at add
+    auto failp = [&](const std::string& m, apsm_status st) {
+        copy_err(err, errlen, m);
+        delete p;
+        return st;
+    };
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&p->device) != cudaSuccess || cudaGetDeviceProperties(&prop, p->device) != cudaSuccess)
+        return failp("cudaGetDeviceProperties failed", APSM_ERR_CUDA);
+    if (prop.major < 10) return failp("an sm_100 (Blackwell) device is required", APSM_ERR_NO_DEVICE);
+    p->sms = prop.multiProcessorCount;
+    p->lanes.resize(lanes);
+    for (auto& l : p->lanes) {
+        if (cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) != cudaSuccess)
+            return failp("cudaStreamCreate failed", APSM_ERR_CUDA);
+        for (auto& e : l.ev)
+            if (cudaEventCreate(&e) != cudaSuccess) return failp("cudaEventCreate failed", APSM_ERR_CUDA);
+        if (cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&l.desc_copied, cudaEventDisableTiming) != cudaSuccess)
+            return failp("cudaEventCreate failed", APSM_ERR_CUDA);
+        cudaEventRecord(l.done, l.stream);
+        cudaEventRecord(l.desc_copied, l.stream);
+    }
+    if (batch_sweep_occupancy(cm, &p->sweep_ctas) != cudaSuccess || p->sweep_ctas < 1)
+        return failp("the training sweep does not fit an SM", APSM_ERR_UNSUPPORTED);
+    *out = p;
+    return APSM_OK;
+}
+
+extern "C" void apsm_pool_destroy(apsm_pool* p) { delete p; }
+
+extern "C" const char* apsm_pool_last_error(const apsm_pool* p) { return p ? p->last_error.c_str() : "null handle"; }
+
+extern "C" apsm_status apsm_pool_add(apsm_pool* p, uint32_t num_antennas, uint32_t* detector)
+{
+    if (!p || !detector) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    if (num_antennas == 0) return p->fail(APSM_ERR_INVALID_ARGUMENT, "num_antennas must be >= 1");
+    if (num_antennas > uint32_t(kMaxFeatures / 2))
+        return p->fail(APSM_ERR_UNSUPPORTED, "num_antennas must be <= " + std::to_string(kMaxFeatures / 2));
+    PoolDet d;
+    d.N = num_antennas;
+    d.Np = round_up(num_antennas, 2);
+    d.capP = p->cfg.dict_size;
+    d.cap = 2 * d.capP;
+    d.ew = -0.5f / (p->cfg.variance * float(num_antennas * num_antennas));
+    size_t off[5];
+    d.bytes = resident_layout(d.N, d.capP, off);
+    if (p->budget && p->in_use() + d.bytes > p->budget)
+        return p->fail(APSM_ERR_OUT_OF_MEMORY, "detector state of " + std::to_string(d.bytes) +
+                                                   " bytes exceeds the pool's HBM budget");
+    if (int(d.Np) > p->cm.Np) {
+        BatchCommon cm2 = p->cm;
+        cm2.Np = int(d.Np);
+        int ctas = 0;
+        if (batch_sweep_occupancy(cm2, &ctas) != cudaSuccess || ctas < 1)
+            return p->fail(APSM_ERR_UNSUPPORTED, "the training sweep does not fit an SM for this antenna count");
+        for (auto& l : p->lanes) cudaStreamSynchronize(l.stream);
+        p->cm = cm2;
+        p->sweep_ctas = ctas;
+    }
+    cudaError_t e = cudaMalloc(&d.mem, d.bytes);
+    if (e != cudaSuccess) return p->cuda_fail(e, "cudaMalloc(detector state)");
+    char* m = static_cast<char*>(d.mem);
+    d.Y = reinterpret_cast<float2*>(m + off[0]);
+    d.nrm = reinterpret_cast<float*>(m + off[1]);
+    d.y = reinterpret_cast<float*>(m + off[2]);
+    d.a = reinterpret_cast<float*>(m + off[3]);
+    d.w = reinterpret_cast<float*>(m + off[4]);
+    e = cudaMemset(d.mem, 0, d.bytes);
+    if (e != cudaSuccess) {
+        cudaFree(d.mem);
+        return p->cuda_fail(e, "cudaMemset(detector state)");
+    }
+    d.live = true;
+    p->resident += d.bytes;
+    for (size_t i = 0; i < p->dets.size(); ++i)
+        if (!p->dets[i].live && !p->dets[i].mem) {
+            p->dets[i] = d;
+            *detector = uint32_t(i);
+            return APSM_OK;
+        }
+    p->dets.push_back(d);
+    *detector = uint32_t(p->dets.size() - 1);
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_pool_remove(apsm_pool* p, uint32_t detector)
+{
+    if (!p) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    if (detector >= p->dets.size() || !p->dets[detector].live)
+        return p->fail(APSM_ERR_INVALID_ARGUMENT, "unknown detector");
+    for (auto& l : p->lanes) cudaStreamSynchronize(l.stream);
+    PoolDet& d = p->dets[detector];
+    cudaFree(d.mem);
+    p->resident -= d.bytes;
+    d = PoolDet();
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_pool_reset(apsm_pool* p, uint32_t detector)
+{
+    if (!p) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    if (detector >= p->dets.size() || !p->dets[detector].live)
+        return p->fail(APSM_ERR_INVALID_ARGUMENT, "unknown detector");
+    PoolDet& d = p->dets[detector];
+    for (auto& l : p->lanes) cudaStreamSynchronize(l.stream);
+    cudaError_t e = cudaMemset(d.mem, 0, d.bytes);
+    if (e != cudaSuccess) return p->cuda_fail(e, "cudaMemset(detector state)");
+    d.used = 0;
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs,
+                                     int device_buffers)
+{
+    if (!p) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    if (lane >= p->lanes.size()) return p->fail(APSM_ERR_INVALID_ARGUMENT, "lane out of range");
+    if (n_jobs > 0 && !jobs) return p->fail(APSM_ERR_INVALID_ARGUMENT, "null job list");
+    return p->run(lane, jobs, n_jobs, device_buffers != 0);
+}
+
+extern "C" apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane)
+{
+    if (!p || lane >= p->lanes.size()) return APSM_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaEventSynchronize(p->lanes[lane].done);
+    if (e != cudaSuccess) return p->cuda_fail(e, "cudaEventSynchronize");
+    return APSM_OK;
+}
+
+extern "C" int apsm_pool_query(apsm_pool* p, uint32_t lane)
+{
+    if (!p || lane >= p->lanes.size()) return -int(APSM_ERR_INVALID_ARGUMENT);
+    cudaError_t e = cudaEventQuery(p->lanes[lane].done);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) {
+        cudaGetLastError();
+        return 0;
+    }
+    p->cuda_fail(e, "cudaEventQuery");
+    return -int(APSM_ERR_CUDA);
+}
+
+extern "C" void* apsm_pool_stream(apsm_pool* p, uint32_t lane)
+{
+    if (!p || lane >= p->lanes.size()) return nullptr;
+    return (void*)p->lanes[lane].stream;
+}
+
+extern "C" uint64_t apsm_pool_job_bytes(const apsm_pool* p, const apsm_job* job)
+{
+    if (!p || !job || job->detector >= p->dets.size() || !p->dets[job->detector].live) return 0;
+    const PoolDet& d = p->dets[job->detector];
+    return job->kind == APSM_JOB_TRAIN ? p->train_bytes(d, job->length, true) : p->detect_bytes(d, job->length, true);
+}
+
+extern "C" uint64_t apsm_pool_budget(const apsm_pool* p) { return p ? p->budget : 0; }
+
+extern "C" uint64_t apsm_pool_bytes_in_use(const apsm_pool* p) { return p ? p->in_use() : 0; }
+
+extern "C" apsm_status apsm_pool_last_ms(apsm_pool* p, uint32_t lane, float* train_ms, float* detect_ms)
+{
+    if (!p || lane >= p->lanes.size()) return APSM_ERR_INVALID_ARGUMENT;
+    Lane& L = p->lanes[lane];
+    cudaError_t e = cudaEventSynchronize(L.done);
+    if (e != cudaSuccess) return p->cuda_fail(e, "cudaEventSynchronize");
+    if (train_ms) {
+        *train_ms = -1.f;
+        if (L.have_train && cudaEventElapsedTime(train_ms, L.ev[0], L.ev[1]) != cudaSuccess) *train_ms = -1.f;
+    }
+    if (detect_ms) {
+        *detect_ms = -1.f;
+        if (L.have_detect && cudaEventElapsedTime(detect_ms, L.ev[2], L.ev[3]) != cudaSuccess) *detect_ms = -1.f;
+    }
+    cudaGetLastError();
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_pool_get_state(apsm_pool* p, uint32_t detector, uint32_t* rows, float* a, float* w)
+{
+    if (!p) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    if (detector >= p->dets.size() || !p->dets[detector].live)
+        return p->fail(APSM_ERR_INVALID_ARGUMENT, "unknown detector");
+    for (auto& l : p->lanes) cudaStreamSynchronize(l.stream);
+    const PoolDet& d = p->dets[detector];
+    if (rows) *rows = d.used;
+    if (a && d.used) {
+        cudaError_t e = cudaMemcpy(a, d.a, sizeof(float) * d.used, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return p->cuda_fail(e, "cudaMemcpy(a)");
+    }
+    if (w) {
+        cudaError_t e = cudaMemcpy(w, d.w, sizeof(float) * 2 * d.N, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return p->cuda_fail(e, "cudaMemcpy(w)");
+    }
+    return APSM_OK;
+}

@@ -1,0 +1,91 @@
+// Batched packing and dictionary copies (one launch for all jobs of a batch).
+//
+// Packing follows CudaHostMatrix(stream, ComplexSampleMatrix)
+// (cpp/lib/cuda/cuda_matrix_host.cu:105-149) but keeps complex samples: pair
+// i of the destination is the complex vector (rx[0][p(i)], ..., rx[N-1][p(i)])
+// with p the training shuffle (noma_detector.cu:59-74) or the identity.  The
+// squared norm is the sequential fma chain over the Dedup row [Re y; Im y],
+// the order the single-detector kernels use.
+#include "apsm_batch.cuh"
+
+#include <algorithm>
+
+namespace apsm {
+
+namespace {
+
+constexpr int kPackChunk = 64;
+
+__global__ void __launch_bounds__(256) batch_pack_kernel(const BatchPackJob* __restrict__ jobs, int smem_n)
+{
+    const BatchPackJob jb = jobs[blockIdx.y];
+    const int i0 = blockIdx.x * kPackChunk;
+    if (i0 >= jb.L || jb.N > smem_n) return; // shared memory is sized for smem_n antennas
+    const int n = min(kPackChunk, jb.L - i0);
+    extern __shared__ float2 sm[]; // [kPackChunk][N + 1]
+    const int N = jb.N, Np = jb.Np, pitch = N + 1;
+    for (int idx = threadIdx.x; idx < N * kPackChunk; idx += blockDim.x) {
+        const int k = idx / kPackChunk, i = idx % kPackChunk;
+        if (i < n) {
+            const int src = jb.perm ? jb.perm[i0 + i] : i0 + i;
+            sm[i * pitch + k] = jb.rx[size_t(k) * jb.L + src];
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < n * Np; idx += blockDim.x) {
+        const int i = idx / Np, k = idx % Np;
+        jb.Y[size_t(i0 + i) * Np + k] = k < N ? sm[i * pitch + k] : make_float2(0.f, 0.f);
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        float s = 0.f;
+        for (int k = 0; k < N; ++k) s = fmaf(sm[i * pitch + k].x, sm[i * pitch + k].x, s);
+        for (int k = 0; k < N; ++k) s = fmaf(sm[i * pitch + k].y, sm[i * pitch + k].y, s);
+        jb.nrm[i0 + i] = s;
+        if (jb.y) {
+            const int src = jb.perm ? jb.perm[i0 + i] : i0 + i;
+            const float2 t = jb.tx[src];
+            jb.y[2 * (i0 + i)] = t.x;
+            jb.y[2 * (i0 + i) + 1] = t.y;
+        }
+        if (jb.a) {
+            jb.a[2 * (i0 + i)] = 0.f;
+            jb.a[2 * (i0 + i) + 1] = 0.f;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) batch_copy_kernel(const BatchCopyJob* __restrict__ jobs)
+{
+    const BatchCopyJob jb = jobs[blockIdx.y];
+    const size_t nY = size_t(jb.pairs) * jb.Np;
+    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nY; i += stride) jb.Ydst[i] = jb.Ysrc[i];
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < size_t(jb.pairs); i += stride) {
+        jb.ndst[i] = jb.nsrc[i];
+        jb.ydst[2 * i] = jb.ysrc[2 * i];
+        jb.ydst[2 * i + 1] = jb.ysrc[2 * i + 1];
+        jb.adst[2 * i] = jb.asrc[2 * i];
+        jb.adst[2 * i + 1] = jb.asrc[2 * i + 1];
+    }
+}
+
+} // namespace
+
+cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s)
+{
+    if (n_jobs <= 0 || max_len <= 0) return cudaSuccess;
+    dim3 grid((max_len + kPackChunk - 1) / kPackChunk, n_jobs);
+    batch_pack_kernel<<<grid, 256, sizeof(float2) * kPackChunk * (max_n + 1), s>>>(d_jobs, max_n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_copy(const BatchCopyJob* d_jobs, int n_jobs, int max_pairs, int max_np, cudaStream_t s)
+{
+    if (n_jobs <= 0 || max_pairs <= 0) return cudaSuccess;
+    const long long work = (long long)max_pairs * max_np;
+    const int gx = int(std::min<long long>(256, (work + 1023) / 1024));
+    batch_copy_kernel<<<dim3(std::max(1, gx), n_jobs), 256, 0, s>>>(d_jobs);
+    return cudaGetLastError();
+}
+
+} // namespace apsm

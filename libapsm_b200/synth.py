@@ -74,3 +74,54 @@ def config1_frame(seed: int = 1) -> Frame:
 CONFIG0_ALGORITHM = {"otype": "APSM", "windowSize": 80, "gaussianKernelVariance": 0.5, "eB": 0.01}
 CONFIG1_ALGORITHM = {"otype": "APSM", "windowSize": 80, "gaussianKernelVariance": 0.5, "eB": 0.01,
                      "dictionarySize": 1000}
+
+
+# Batched workload: many independent detectors (users x cells).  Keys a
+# configuration does not set keep the reference's defaults
+# (apsm_parameters.cuh:68-86): gaussianKernelVariance 0.05, eB 0.001.
+CONFIG2_ALGORITHM = {"otype": "APSM", "windowSize": 80, "dictionarySize": 2000}
+
+
+@dataclass
+class DetectorFrame:
+    """One detector's frame: the cell's received pilots/data and its user's symbols."""
+
+    rx_train: np.ndarray  # (N, P) complex64
+    tx_train: np.ndarray  # (P,) complex64
+    rx_data: np.ndarray   # (N, S) complex64
+    tx_data: np.ndarray   # (S,) complex64
+    modulation: Modulation
+    snr_db: float
+
+    @property
+    def N(self) -> int:
+        return self.rx_train.shape[0]
+
+    @property
+    def P(self) -> int:
+        return self.rx_train.shape[1]
+
+    @property
+    def S(self) -> int:
+        return self.rx_data.shape[1]
+
+
+def config2_detectors(n: int = 512, seed: int = 2, users_per_cell: int = 4,
+                      pilots: tuple[int, int] = (200, 2000), data: tuple[int, int] = (1000, 16000)) -> list[DetectorFrame]:
+    """n detectors: antennas uniform over {4, 8, 16, 32}, pilots uniform over
+    [200, 2000], data symbols over [1000, 16000], SNR over [10, 25] dB, QPSK or
+    16QAM with probability 1/2, Rapp PA p=2 at 3 dB back-off; detector i's
+    frame is drawn with seed 1000 * seed + i (its cell has users_per_cell
+    users, the detector detects user 0)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        N = int(rng.choice([4, 8, 16, 32]))
+        P = int(rng.integers(pilots[0], pilots[1] + 1))
+        S = int(rng.integers(data[0], data[1] + 1))
+        snr = float(rng.uniform(10.0, 25.0))
+        mod = "QPSK" if rng.random() < 0.5 else "QAM16"
+        f = generate_frame(1000 * seed + i, K=users_per_cell, N=N, P=P, S=S, modulation=mod, snr_db=snr, rapp_p=2.0)
+        out.append(DetectorFrame(f.rx_train, np.ascontiguousarray(f.tx_train[0]), f.rx_data,
+                                 np.ascontiguousarray(f.tx_data[0]), f.modulation, snr))
+    return out

@@ -1,0 +1,176 @@
+"""Detector pool (batched many-detector form) on the GPU.
+
+Each pool detector must behave like its own NomaDetector (reference
+cpp/lib/noma/noma_detector.cuh:65-75: train then detect, state kept between
+calls): its soft outputs are compared with the FP32 oracle (the restatement of
+apsm_train.cu / apsm_detect.cu) run detector by detector on the same inputs,
+at the FP32-form tolerance 1e-4 relative to the largest soft output; the
+hard decisions are compared away from decision boundaries.  The batch must
+not change a detector's result: a job alone and in a mixed batch give
+bit-identical outputs (one CTA per training job, one thread per sample).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+def _rel(a, b):
+    scale = max(np.max(np.abs(b)), 1e-30)
+    return float(np.max(np.abs(a - b)) / scale)
+
+
+def _frame(seed, N, P, S, mod="QPSK"):
+    from libapsm_b200 import synth
+
+    f = synth.generate_frame(seed, K=2, N=N, P=P, S=S, modulation=mod, snr_db=20.0)
+    return f.rx_train, f.tx_train[0], f.rx_data
+
+
+def _oracle_run(oracle_mod, cfg, N, trains, rx_data):
+    o = oracle_mod.OracleDetector(cfg, N, oracle_mod.F32)
+    for rx, tx in trains:
+        o.train(rx, tx)
+    return o.detect(rx_data)
+
+
+CFG = {"otype": "APSM", "windowSize": 20, "gaussianKernelVariance": 0.5, "eB": 0.01, "dictionarySize": 400}
+
+
+@pytest.mark.parametrize("cfg", [
+    CFG,
+    dict(CFG, windowSize=80, dictionarySize=2000),
+    dict(CFG, trainPasses=2),
+    dict(CFG, startWithFullWindow=True),
+    dict(CFG, trainingShuffle=True),
+    dict(CFG, sampleStep=4),
+    dict(CFG, gaussianKernelWeight=0.8, eB=0.001),
+], ids=["w20", "w80", "passes2", "sfw", "shuffle", "step4", "wG08"])
+def test_pool_matches_oracle_per_detector(native_lib, oracle_mod, cfg):
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    pool = DetectorPool(cfg)
+    specs = [(3, 120, 200), (4, 300, 96), (8, 60, 50), (16, 250, 300), (2, 31, 17), (32, 150, 128)]
+    dets, jobs, frames = [], [], []
+    for i, (N, P, S) in enumerate(specs):
+        d = pool.add(N)
+        rx, tx, rxd = _frame(100 + i, N, P, S)
+        dets.append(d)
+        frames.append((N, rx, tx, rxd))
+        jobs.append(PoolJob(d, rx, tx))
+    for d, (N, rx, tx, rxd) in zip(dets, frames):
+        jobs.append(PoolJob(d, rxd))
+    outs = pool.run(jobs)
+    for k, (N, rx, tx, rxd) in enumerate(frames):
+        est = outs[len(specs) + k]
+        ref = _oracle_run(oracle_mod, cfg, N, [(rx, tx)], rxd)
+        assert _rel(est, ref) < TOL, (k, N, _rel(est, ref))
+
+
+def test_pool_train_append_and_eviction(native_lib, oracle_mod):
+    """Pilots appended to the resident dictionary over several batches; the
+    dictionary (200 entries) fills and evicts its oldest entries."""
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    cfg = dict(CFG, dictionarySize=200)
+    pool = DetectorPool(cfg)
+    N = 6
+    d0, d1 = pool.add(N), pool.add(N)
+    rx, tx, rxd = _frame(7, N, 330, 160)
+    chunks = [(0, 90), (90, 150), (150, 230), (230, 330)]
+    trains = []
+    for lo, hi in chunks:
+        trains.append((rx[:, lo:hi], tx[lo:hi]))
+        pool.run([PoolJob(d0, rx[:, lo:hi], tx[lo:hi]), PoolJob(d1, rx[:, lo:hi], tx[lo:hi])])
+        est0, est1 = pool.run([PoolJob(d0, rxd), PoolJob(d1, rxd)])
+        ref = _oracle_run(oracle_mod, cfg, N, trains, rxd)
+        assert _rel(est0, ref) < TOL, (hi, _rel(est0, ref))
+        assert np.array_equal(est0, est1)
+    rows, a, w = pool.get_state(d0)
+    assert rows == 2 * 200
+
+
+def test_pool_alone_equals_in_mix(native_lib):
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    cfg = dict(CFG, windowSize=80, dictionarySize=2000)
+    N, P, S = 8, 400, 256
+    rx, tx, rxd = _frame(11, N, P, S)
+    alone = DetectorPool(cfg)
+    d = alone.add(N)
+    alone.run([PoolJob(d, rx, tx)])
+    (ref,) = alone.run([PoolJob(d, rxd)])
+
+    mix = DetectorPool(cfg)
+    others = []
+    for i, (n2, p2, s2) in enumerate([(4, 900, 300), (16, 200, 1000), (32, 700, 64)]):
+        others.append((mix.add(n2),) + _frame(50 + i, n2, p2, s2))
+    dm = mix.add(N)
+    jobs = [PoolJob(o[0], o[1], o[2]) for o in others] + [PoolJob(dm, rx, tx)]
+    jobs += [PoolJob(o[0], o[3]) for o in others] + [PoolJob(dm, rxd)]
+    outs = mix.run(jobs)
+    assert np.array_equal(outs[-1], ref)
+
+
+def test_pool_untrained_detect_is_zero_and_reset(native_lib):
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    pool = DetectorPool(CFG)
+    d = pool.add(4)
+    rx, tx, rxd = _frame(3, 4, 50, 40)
+    (est,) = pool.run([PoolJob(d, rxd)])
+    assert np.all(est == 0)
+    pool.run([PoolJob(d, rx, tx)])
+    (e1,) = pool.run([PoolJob(d, rxd)])
+    assert np.any(e1 != 0)
+    pool.reset(d)
+    (e2,) = pool.run([PoolJob(d, rxd)])
+    assert np.all(e2 == 0)
+    pool.run([PoolJob(d, rx, tx)])
+    (e3,) = pool.run([PoolJob(d, rxd)])
+    assert np.array_equal(e1, e3)
+
+
+def test_pool_device_buffers_and_lanes(native_lib):
+    import torch
+
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    pool = DetectorPool(CFG, lanes=2)
+    specs = [(4, 200, 100), (8, 150, 333)]
+    dets = [pool.add(n) for n, _, _ in specs]
+    frames = [_frame(20 + i, *s) for i, s in enumerate(specs)]
+    host = DetectorPool(CFG)
+    hd = [host.add(n) for n, _, _ in specs]
+    refs = host.run([PoolJob(d, f[0], f[1]) for d, f in zip(hd, frames)] + [PoolJob(d, f[2]) for d, f in zip(hd, frames)])
+    ests = []
+    for lane, (d, f) in enumerate(zip(dets, frames)):
+        rx, tx, rxd = (torch.from_numpy(x).cuda() for x in f)
+        est = torch.empty(rxd.shape[1], dtype=torch.complex64, device="cuda")
+        torch.cuda.synchronize()
+        pool.run_device([PoolJob(d, rx, tx), PoolJob(d, rxd, est=est)], lane=lane)
+        ests.append((est, rx, tx, rxd))
+    for lane in range(2):
+        pool.wait(lane)
+    for k in range(2):
+        assert np.array_equal(ests[k][0].cpu().numpy(), refs[2 + k])
+    t_ms, d_ms = pool.last_ms(0)
+    assert t_ms > 0 and d_ms > 0
+
+
+def test_pool_budget_admission(native_lib):
+    from libapsm_b200 import ApsmError, DetectorPool, PoolJob
+
+    pool = DetectorPool(CFG, hbm_budget=600_000)
+    d = pool.add(4)
+    with pytest.raises(ApsmError, match="OUT_OF_MEMORY"):
+        for _ in range(100):
+            pool.add(32)
+    rx, tx, rxd = _frame(5, 4, 2000, 10)
+    job = PoolJob(d, rx, tx)
+    assert pool.job_bytes(job) > 0
+    with pytest.raises(ApsmError, match="OUT_OF_MEMORY"):
+        pool.run([job])
+    assert pool.bytes_in_use <= pool.budget
