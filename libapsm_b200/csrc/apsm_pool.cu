@@ -12,6 +12,7 @@
 #include "apsm_host.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -48,6 +49,7 @@ struct Lane {
     size_t scratch_bytes = 0;
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    int* err = nullptr; // error flag of the last batch (in the scratch)
 };
 
 int detect_class(uint32_t N)
@@ -92,6 +94,7 @@ struct apsm_pool {
     size_t train_bytes(const PoolDet& d, uint32_t P, bool host) const;
     size_t detect_bytes(const PoolDet& d, uint32_t S, bool host) const;
     apsm_status run(uint32_t lane, const apsm_job* jobs, uint32_t n, bool device_buffers);
+    apsm_status check_lane(uint32_t lane);
 };
 
 #define POOL_CK(call)                                                                  \
@@ -149,9 +152,19 @@ struct DetectPlan {
     uint32_t job = 0;
     PoolDet* det = nullptr;
     uint32_t S = 0, Mp = 0;
-    int cls = 0;
+    int cls = 0;       // CUDA-core class (max antennas) or tensor-core class (max Kp)
+    bool gram = false; // tensor-core (tcgen05) form
+    int Kp = 0, tiles = 0, chunks = 0;
     size_t off_rx = 0, off_Y = 0, off_nrm = 0, off_est = 0;
+    size_t off_aops = 0, off_bops = 0, off_bx = 0, off_lin = 0;
 };
+
+int gram_class(int Kp)
+{
+    for (int c : {8, 16, 32, 64})
+        if (Kp <= c) return c;
+    return 0;
+}
 
 } // namespace
 
@@ -242,10 +255,26 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
             d.det = &dets[jobs[i].detector];
             d.S = jobs[i].length;
             d.Mp = used_after[jobs[i].detector] / 2;
-            d.cls = detect_class(d.det->N);
+            d.gram = cfg.detect_mode == DetectMode::GramTF32x3 && d.det->N <= 32;
+            if (d.gram) {
+                d.Kp = int(round_up(2 * d.det->N, 8));
+                d.cls = gram_class(d.Kp);
+                d.tiles = int((d.S + batch_gram_tile() - 1) / batch_gram_tile());
+                d.chunks = int((d.Mp + batch_gram_chunk_pairs() - 1) / batch_gram_chunk_pairs());
+            } else {
+                d.cls = detect_class(d.det->N);
+            }
             dp.push_back(d);
         }
-    std::stable_sort(dp.begin(), dp.end(), [](const DetectPlan& x, const DetectPlan& y) { return x.cls < y.cls; });
+    std::stable_sort(dp.begin(), dp.end(), [](const DetectPlan& x, const DetectPlan& y) {
+        return x.gram != y.gram ? x.gram < y.gram : x.cls < y.cls;
+    });
+    size_t nG = 0, nGcls = 0;
+    for (size_t k = 0; k < dp.size(); ++k)
+        if (dp[k].gram) {
+            ++nG;
+            if (k == 0 || !dp[k - 1].gram || dp[k - 1].cls != dp[k].cls) ++nGcls;
+        }
 
     const size_t nT = tp.size(), nD = dp.size();
     size_t nCopyIn = 0;
@@ -258,6 +287,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
     const size_t off_pj = o; o = align_up(o + sizeof(BatchPackJob) * nPack, 256);
     const size_t off_ci = o; o = align_up(o + sizeof(BatchCopyJob) * nCopyIn, 256);
     const size_t off_co = o; o = align_up(o + sizeof(BatchCopyJob) * nT, 256);
+    const size_t off_gj = o; o = align_up(o + sizeof(BatchGramJob) * nG, 256);
+    const size_t off_gp = o; o = align_up(o + sizeof(int) * (nG + nGcls), 256);
     for (auto& t : tp) {
         t.off_steps = o;
         o = align_up(o + sizeof(TrainStep) * t.steps.size(), 16);
@@ -274,7 +305,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         }
     o = align_up(o, 256);
     const size_t desc_bytes = o;
-    const size_t off_counter = o; o = align_up(o + 256, 256);
+    const size_t off_counter = o; o = align_up(o + 256, 256); // sweep job counter, error flag
     for (auto& t : tp) {
         const PoolDet& d = *t.det;
         if (host) {
@@ -295,6 +326,12 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         }
         d.off_Y = o; o = align_up(o + sizeof(float2) * size_t(d.S) * d.det->Np, 256);
         d.off_nrm = o; o = align_up(o + sizeof(float) * d.S, 256);
+        if (d.gram) {
+            d.off_aops = o; o = align_up(o + batch_gram_a_bytes(d.Kp) * d.tiles, 256);
+            d.off_bops = o; o = align_up(o + batch_gram_b_bytes(d.Kp) * std::max(d.chunks, 1), 256);
+            d.off_bx = o; o = align_up(o + sizeof(float) * batch_gram_bx_floats() * std::max(d.chunks, 1), 256);
+            d.off_lin = o; o = align_up(o + sizeof(float2) * d.S, 256);
+        }
     }
     const size_t scratch_need = o;
 
@@ -393,6 +430,49 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         max_n = std::max(max_n, int(d.N));
         float2* out = host ? reinterpret_cast<float2*>(D(q.off_est)) : reinterpret_cast<float2*>(j.est);
         h_dj[k] = BatchDetectJob{Ys, ns, d.Y, d.nrm, d.a, d.w, out, int(q.S), int(q.Mp), int(d.N), int(d.Np), d.ew};
+        if (q.gram) {
+            BatchGramJob g{};
+            g.Ys = Ys;
+            g.nrm_s = ns;
+            g.w = d.w;
+            g.lin = reinterpret_cast<float2*>(D(q.off_lin));
+            g.a_ops = reinterpret_cast<uint8_t*>(D(q.off_aops));
+            g.Yd = d.Y;
+            g.nrm_d = d.nrm;
+            g.a = d.a;
+            g.b_ops = reinterpret_cast<uint8_t*>(D(q.off_bops));
+            g.bx = reinterpret_cast<float*>(D(q.off_bx));
+            g.out = out;
+            g.S = int(q.S);
+            g.N = int(d.N);
+            g.Np = int(d.Np);
+            g.Kp = q.Kp;
+            g.Mp = int(q.Mp);
+            g.n_chunks = q.chunks;
+            g.ew2 = d.ew * 1.4426950408889634f;
+            reinterpret_cast<BatchGramJob*>(hst + off_gj)[k - (nD - nG)] = g;
+        }
+    }
+    // tile prefixes of the tensor-core classes (one segment per class)
+    std::vector<std::array<int, 6>> gseg; // k0, k1, prefix offset, total tiles, max tiles, max chunks
+    {
+        int* pre = reinterpret_cast<int*>(hst + off_gp);
+        size_t k = nD - nG, po = 0;
+        while (k < nD) {
+            size_t k1 = k;
+            int acc = 0, mt = 0, mc = 0;
+            while (k1 < nD && dp[k1].cls == dp[k].cls) {
+                pre[po + (k1 - k)] = acc;
+                acc += dp[k1].tiles;
+                mt = std::max(mt, dp[k1].tiles);
+                mc = std::max(mc, dp[k1].chunks);
+                ++k1;
+            }
+            pre[po + (k1 - k)] = acc;
+            gseg.push_back({int(k), int(k1), int(po), acc, mt, mc});
+            po += k1 - k + 1;
+            k = k1;
+        }
     }
     (void)pack_train;
 
@@ -412,6 +492,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
     POOL_CK(cudaEventRecord(L.desc_copied, s));
     L.have_train = nT > 0;
     L.have_detect = nD > 0;
+    int* d_counter = reinterpret_cast<int*>(D(off_counter));
+    int* d_err = d_counter + 4;
+    POOL_CK(cudaMemsetAsync(d_counter, 0, 32, s));
+    L.err = d_err;
     if (nT > 0) {
         POOL_CK(cudaEventRecord(L.ev[0], s));
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_ci)), int(nCopyIn), max_pairs_in, max_np, s));
@@ -420,10 +504,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
     if (nT > 0) {
         const auto* d_tj = reinterpret_cast<const BatchTrainJob*>(D(off_tj));
         POOL_CK(launch_batch_kcol(d_tj, int(nT), max_cols, max_n, cm, s));
-        int* counter = reinterpret_cast<int*>(D(off_counter));
-        POOL_CK(cudaMemsetAsync(counter, 0, sizeof(int), s));
         const int grid = int(std::min<size_t>(nT, size_t(sweep_ctas) * sms));
-        POOL_CK(launch_batch_sweep(d_tj, int(nT), cm, grid, counter, nullptr, s));
+        POOL_CK(launch_batch_sweep(d_tj, int(nT), cm, grid, d_counter, d_err, s));
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_co)), int(nT), max_pairs_out, max_np, s));
         POOL_CK(cudaEventRecord(L.ev[1], s));
         for (const auto& t : tp) t.det->used = 2 * t.usedP_new;
@@ -432,15 +514,23 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         POOL_CK(cudaEventRecord(L.ev[2], s));
         const auto* d_dj = reinterpret_cast<const BatchDetectJob*>(D(off_dj));
         size_t k0 = 0;
-        while (k0 < nD) {
+        const size_t nC = nD - nG; // CUDA-core jobs come first
+        while (k0 < nC) {
             size_t k1 = k0;
             int tiles = 0;
-            while (k1 < nD && dp[k1].cls == dp[k0].cls) {
+            while (k1 < nC && dp[k1].cls == dp[k0].cls) {
                 tiles = std::max(tiles, int((dp[k1].S + batch_detect_tile() - 1) / batch_detect_tile()));
                 ++k1;
             }
             POOL_CK(launch_batch_detect(d_dj + k0, int(k1 - k0), tiles, dp[k0].cls, cfg.wL, cfg.wG, s));
             k0 = k1;
+        }
+        const auto* d_gj = reinterpret_cast<const BatchGramJob*>(D(off_gj));
+        const int* d_gp = reinterpret_cast<const int*>(D(off_gp));
+        for (const auto& g : gseg) {
+            const size_t base = size_t(g[0]) - nC;
+            POOL_CK(launch_batch_gram(d_gj + base, g[1] - g[0], g[4], g[5], d_gp + g[2], g[3], dp[g[0]].cls, cfg.wL,
+                                      cfg.wG, d_err, s));
         }
         POOL_CK(cudaEventRecord(L.ev[3], s));
         if (host)
@@ -448,7 +538,21 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
                 POOL_CK(cudaMemcpyAsync(jobs[q.job].est, D(q.off_est), sizeof(float2) * q.S, cudaMemcpyDeviceToHost, s));
     }
     POOL_CK(cudaEventRecord(L.done, s));
-    if (host) POOL_CK(cudaStreamSynchronize(s));
+    if (host) {
+        POOL_CK(cudaStreamSynchronize(s));
+        return check_lane(lane_id);
+    }
+    return APSM_OK;
+}
+
+apsm_status apsm_pool::check_lane(uint32_t lane_id)
+{
+    apsm_pool* p = this;
+    Lane& L = lanes[lane_id];
+    if (!L.err) return APSM_OK;
+    int h = 0;
+    POOL_CK(cudaMemcpy(&h, L.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) return fail(APSM_ERR_CUDA, "a bounded wait in a tensor-core kernel expired (results of the batch are invalid)");
     return APSM_OK;
 }
 
@@ -491,6 +595,8 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
     else if (cfg.step % 2 != 0 || cfg.step == 0 || cfg.step > 8) why = "the detector pool needs an even sampleStep <= 8";
     else if (cfg.dict_size < cfg.window + cfg.step / 2) why = "the detector pool needs dictionarySize >= windowSize + sampleStep / 2";
     else if (cfg.window == 0) why = "windowSize must be >= 1";
+    else if (cfg.detect_mode != DetectMode::Exact && cfg.detect_mode != DetectMode::GramTF32x3)
+        why = "the detector pool implements detectVersion gram_tf32x3 (tensor cores) and the FP32 CUDA-core form";
     if (!why.empty()) {
         copy_err(err, errlen, why);
         return APSM_ERR_UNSUPPORTED;
@@ -643,7 +749,7 @@ extern "C" apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane)
     if (!p || lane >= p->lanes.size()) return APSM_ERR_INVALID_ARGUMENT;
     cudaError_t e = cudaEventSynchronize(p->lanes[lane].done);
     if (e != cudaSuccess) return p->cuda_fail(e, "cudaEventSynchronize");
-    return APSM_OK;
+    return p->check_lane(lane);
 }
 
 extern "C" int apsm_pool_query(apsm_pool* p, uint32_t lane)

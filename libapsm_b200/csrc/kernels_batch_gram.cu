@@ -1,0 +1,333 @@
+// Batched tensor-core detection in pair form (tcgen05, TF32 operands split
+// hi + lo, three UMMAs per K step: FP32-accurate Gram products).
+//
+// For data sample s and dictionary pair b (complex y_b) the detector needs
+// r = Re(y_b^H x_s) and m = Im(y_b^H x_s) (kernel values of the four row
+// combinations, see apsm_batch.cuh).  With A = the samples' rows [Re x; Im x]
+// and B = two rows per dictionary pair, [Re y; Im y] and [-Im y; Re y], the
+// product A B^T holds r and m in adjacent columns.  One CTA takes a tile of
+// 128 samples of one job against every chunk of 64 dictionary pairs
+// (UMMA M=128, N=128, FP32 accumulators in tensor memory, double-buffered);
+// the epilogue forms the three distances with FP32 norms, exponentiates on
+// the SFU and accumulates a_2b K(2b, .) + a_2b+1 K(2b+1, .) for the two soft
+// outputs of the sample (reference model cpp/lib/apsm/apsm_detect.cu:690-876).
+//
+// Roles (320 threads): warps 0-7 epilogue (warp w: TMEM lanes 32*(w%4)..,
+// column half w/4), warp 8 producer (bulk async copies of the sample tile and
+// the dictionary chunks), warp 9 TMEM allocator and MMA issuer.  Every
+// mbarrier wait is bounded; on expiry the CTA records an error, still waits
+// for its own copies and MMAs, releases tensor memory and returns.
+#include "apsm_batch.cuh"
+#include "apsm_tc.cuh"
+
+#include <algorithm>
+
+namespace apsm {
+
+namespace {
+
+using namespace tc;
+
+constexpr int kTileM = 128;      // samples per tile (UMMA M)
+constexpr int kChunkPairs = 64;  // dictionary pairs per chunk
+constexpr int kChunkN = 128;     // accumulator columns per chunk (UMMA N)
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = (kEpiWarps + 2) * 32;
+constexpr int kBx = 2 * kChunkPairs + kChunkPairs; // per chunk: a*wG (128, column order) then pair norms (64)
+
+__device__ __forceinline__ uint32_t tf32_bits(float x)
+{
+    uint32_t h;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+    return h;
+}
+
+// canonical K-major, no-swizzle byte offset of element (r, k) in a tile of R rows (4-byte elements)
+__device__ __forceinline__ size_t canon_off(int r, int k, int R)
+{
+    return size_t(k >> 2) * (R * 16) + (r >> 3) * 128 + (r & 7) * 16 + (k & 3) * 4;
+}
+
+// A operand tiles (hi then lo halves along K), the samples' linear terms wL <w, x>.
+__global__ void __launch_bounds__(256) batch_gram_pack_a_kernel(const BatchGramJob* __restrict__ jobs, float wL)
+{
+    const BatchGramJob& jb = jobs[blockIdx.y];
+    const int t = blockIdx.x;
+    if (t * kTileM >= jb.S) return;
+    const int N = jb.N, Np = jb.Np, Kp = jb.Kp, KE = 2 * Kp;
+    uint8_t* tile = jb.a_ops + size_t(t) * kTileM * KE * 4;
+    for (int idx = threadIdx.x; idx < kTileM * Kp; idx += blockDim.x) {
+        const int r = idx / Kp, k = idx % Kp;
+        const int s = t * kTileM + r;
+        float x = 0.f;
+        if (s < jb.S && k < 2 * N) {
+            const float2 v = jb.Ys[size_t(s) * Np + (k < N ? k : k - N)];
+            x = k < N ? v.x : v.y;
+        }
+        const float hi = __uint_as_float(tf32_bits(x));
+        *reinterpret_cast<float*>(tile + canon_off(r, k, kTileM)) = hi;
+        *reinterpret_cast<float*>(tile + canon_off(r, Kp + k, kTileM)) = x - hi;
+    }
+    for (int r = threadIdx.x; r < kTileM; r += blockDim.x) {
+        const int s = t * kTileM + r;
+        if (s >= jb.S) continue;
+        float l0 = 0.f, l1 = 0.f;
+        for (int k = 0; k < N; ++k) {
+            const float2 v = jb.Ys[size_t(s) * Np + k];
+            const float w0 = jb.w[k], w1 = jb.w[N + k];
+            l0 = fmaf(w0, v.x, fmaf(w1, v.y, l0));
+            l1 = fmaf(w0, v.y, fmaf(-w1, v.x, l1));
+        }
+        jb.lin[s] = make_float2(wL * l0, wL * l1);
+    }
+}
+
+// B operand chunks of the job's dictionary (two rows per pair) and per chunk
+// the coefficients a*wG and the pair norms.
+__global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJob* __restrict__ jobs, float wG)
+{
+    const BatchGramJob& jb = jobs[blockIdx.y];
+    const int c = blockIdx.x;
+    if (c >= jb.n_chunks) return;
+    const int N = jb.N, Np = jb.Np, Kp = jb.Kp, KE = 2 * Kp;
+    uint8_t* chunk = jb.b_ops + size_t(c) * kChunkN * KE * 4;
+    for (int idx = threadIdx.x; idx < kChunkN * Kp; idx += blockDim.x) {
+        const int r = idx / Kp, k = idx % Kp;
+        const int b = c * kChunkPairs + (r >> 1);
+        float x = 0.f;
+        if (b < jb.Mp && k < 2 * N) {
+            const float2 v = jb.Yd[size_t(b) * Np + (k < N ? k : k - N)];
+            // row 2j: [Re y; Im y]; row 2j+1: [-Im y; Re y]
+            x = (r & 1) == 0 ? (k < N ? v.x : v.y) : (k < N ? -v.y : v.x);
+        }
+        const float hi = __uint_as_float(tf32_bits(x));
+        *reinterpret_cast<float*>(chunk + canon_off(r, k, kChunkN)) = hi;
+        *reinterpret_cast<float*>(chunk + canon_off(r, Kp + k, kChunkN)) = x - hi;
+    }
+    float* bx = jb.bx + size_t(c) * kBx;
+    for (int i = threadIdx.x; i < kBx; i += blockDim.x) {
+        float v = 0.f;
+        if (i < 2 * kChunkPairs) {
+            const int b = c * kChunkPairs + (i >> 1);
+            v = b < jb.Mp ? jb.a[2 * b + (i & 1)] * wG : 0.f;
+        } else {
+            const int b = c * kChunkPairs + (i - 2 * kChunkPairs);
+            v = b < jb.Mp ? jb.nrm_d[b] : 0.f;
+        }
+        bx[i] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    batch_gram_kernel(const BatchGramJob* __restrict__ jobs, int n_jobs, const int* __restrict__ tile_prefix, int KEmax,
+                      int stages, int* err)
+{
+    // job of this CTA: tile_prefix[j] <= blockIdx.x < tile_prefix[j + 1]
+    int lo = 0, hi = n_jobs;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (tile_prefix[mid] <= int(blockIdx.x)) lo = mid;
+        else hi = mid;
+    }
+    const BatchGramJob& jb = jobs[lo];
+    const int tile = int(blockIdx.x) - tile_prefix[lo];
+    const int KE = 2 * jb.Kp;
+    const int nch = jb.n_chunks;
+
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const uint32_t a_bytes = uint32_t(kTileM) * KE * 4;
+    const uint32_t b_bytes = uint32_t(kChunkN) * KE * 4;
+    const uint32_t b_stride = uint32_t(kChunkN) * KEmax * 4;
+    uint8_t* sA = smem;
+    uint8_t* sB = sA + size_t(kTileM) * KEmax * 4;
+    float* sX = reinterpret_cast<float*>(sB + size_t(stages) * b_stride); // [stages][kBx]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sX + size_t(stages) * kBx);
+    uint64_t* full = bars;                // [stages]
+    uint64_t* empty = bars + stages;      // [stages]
+    uint64_t* tfull = bars + 2 * stages;  // [2]
+    uint64_t* tempty = tfull + 2;         // [2]
+    uint64_t* afull = tempty + 2;         // [1]
+    uint64_t* done = afull + 1;           // [1]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    float2* red = reinterpret_cast<float2*>(tmem_slot + 4); // [kTileM]
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr uint32_t kCols = 2 * kChunkN;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1 + kEpiWarps);
+        }
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&tfull[s], 1);
+            mbar_init(&tempty[s], kEpiWarps);
+        }
+        mbar_init(afull, 1);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == kEpiWarps + 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == kEpiWarps) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            mbar_expect_tx(afull, a_bytes);
+            bulk_g2s(sA, jb.a_ops + size_t(tile) * a_bytes, a_bytes, afull);
+            int issued = 0;
+            for (int i = 0; i < nch; ++i) {
+                const int s = i % stages;
+                if (i >= stages && !mbar_wait(&empty[s], ((i / stages) - 1) & 1, abort_flag)) break;
+                ++issued;
+                mbar_expect_tx(&full[s], b_bytes + kBx * 4);
+                bulk_g2s(sB + size_t(s) * b_stride, jb.b_ops + size_t(i) * b_bytes, b_bytes, &full[s]);
+                bulk_g2s(sX + size_t(s) * kBx, jb.bx + size_t(i) * kBx, kBx * 4, &full[s]);
+            }
+            mbar_drain(afull, 0);
+            for (int i = max(0, issued - stages); i < issued; ++i) mbar_drain(&full[i % stages], (i / stages) & 1);
+        }
+    } else if (warp == kEpiWarps + 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0 && nch > 0 && mbar_wait(afull, 0, abort_flag)) {
+            const uint32_t idesc = instr_desc<kTF32x3>(kTileM, kChunkN);
+            const uint32_t lbo_a = kTileM * 16, lbo_b = kChunkN * 16;
+            const int ksteps = jb.Kp / 8; // 8 TF32 elements (32 bytes) per UMMA K step
+            const int lo_off = jb.Kp / 4; // 16-byte K chunks to the lo half
+            for (int i = 0; i < nch; ++i) {
+                const int s = i % stages, buf = i & 1;
+                if (!mbar_wait(&full[s], (i / stages) & 1, abort_flag)) break;
+                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag)) break;
+                tc_fence_after();
+                const uint8_t* b = sB + size_t(s) * b_stride;
+                const uint32_t d = tmem + uint32_t(buf * kChunkN);
+                for (int kk = 0; kk < ksteps; ++kk) {
+                    const uint64_t ah = smem_desc(sA + size_t(2 * kk) * lbo_a, lbo_a, 128);
+                    const uint64_t bh = smem_desc(b + size_t(2 * kk) * lbo_b, lbo_b, 128);
+                    const uint64_t al = smem_desc(sA + size_t(lo_off + 2 * kk) * lbo_a, lbo_a, 128);
+                    const uint64_t bl = smem_desc(b + size_t(lo_off + 2 * kk) * lbo_b, lbo_b, 128);
+                    umma<kTF32x3>(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
+                    umma<kTF32x3>(d, ah, bl, idesc, 1u);
+                    umma<kTF32x3>(d, al, bh, idesc, 1u);
+                }
+                umma_commit(&tfull[buf]);
+                umma_commit(&empty[s]);
+            }
+        }
+        if (lane == 0) {
+            umma_commit(done);
+            mbar_drain(done, 0);
+        }
+    } else {
+        // ---------------- epilogue ----------------
+        const int q = warp & 3, h = warp >> 2;
+        const int row = tile * kTileM + q * 32 + lane;
+        const float xn = row < jb.S ? jb.nrm_s[row] : 0.f;
+        const float ew2 = jb.ew2;
+        float f0 = 0.f, f1 = 0.f;
+        for (int i = 0; i < nch; ++i) {
+            const int s = i % stages, buf = i & 1;
+            if (!mbar_wait(&full[s], (i / stages) & 1, abort_flag)) break;
+            if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag)) break;
+            tc_fence_after();
+            const float* xs = sX + size_t(s) * kBx;
+#pragma unroll 1
+            for (int cb = 0; cb < kChunkN / 2; cb += 32) {
+                const int col = h * (kChunkN / 2) + cb; // 32 columns = 16 pairs
+                float gv[32];
+                tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * kChunkN + col), gv);
+#pragma unroll
+                for (int j = 0; j < 16; j += 2) {
+                    const int pj = (col >> 1) + j; // pair index within the chunk
+                    const float4 aw = *reinterpret_cast<const float4*>(xs + 2 * pj); // pairs pj, pj+1
+                    const float2 nb = *reinterpret_cast<const float2*>(xs + 2 * kChunkPairs + pj);
+                    {
+                        const float sum = xn + nb.x, re = gv[2 * j], im = gv[2 * j + 1];
+                        const float kA = ex2(ew2 * fmaxf(fmaf(-2.f, re, sum), 0.f));
+                        const float kP = ex2(ew2 * fmaxf(fmaf(-2.f, im, sum), 0.f));
+                        const float kM = ex2(ew2 * fmaxf(fmaf(2.f, im, sum), 0.f));
+                        f0 = fmaf(aw.x, kA, fmaf(aw.y, kM, f0));
+                        f1 = fmaf(aw.x, kP, fmaf(aw.y, kA, f1));
+                    }
+                    {
+                        const float sum = xn + nb.y, re = gv[2 * j + 2], im = gv[2 * j + 3];
+                        const float kA = ex2(ew2 * fmaxf(fmaf(-2.f, re, sum), 0.f));
+                        const float kP = ex2(ew2 * fmaxf(fmaf(-2.f, im, sum), 0.f));
+                        const float kM = ex2(ew2 * fmaxf(fmaf(2.f, im, sum), 0.f));
+                        f0 = fmaf(aw.z, kA, fmaf(aw.w, kM, f0));
+                        f1 = fmaf(aw.z, kP, fmaf(aw.w, kA, f1));
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&tempty[buf]);
+                mbar_arrive(&empty[s]);
+            }
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");
+        if (h == 1) red[q * 32 + lane] = make_float2(f0, f1);
+        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");
+        if (h == 0 && row < jb.S) {
+            const float2 o = red[q * 32 + lane];
+            const float2 l = jb.lin[row];
+            jb.out[row] = make_float2(l.x + (f0 + o.x), l.y + (f1 + o.y));
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == kEpiWarps + 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+    }
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(err, 1);
+}
+
+size_t gram_smem(int KEmax, int stages)
+{
+    return size_t(kTileM) * KEmax * 4 + size_t(stages) * kChunkN * KEmax * 4 + size_t(stages) * kBx * 4 +
+           sizeof(uint64_t) * (2 * stages + 6) + 16 + sizeof(float2) * kTileM + 1024;
+}
+
+} // namespace
+
+int batch_gram_tile() { return kTileM; }
+int batch_gram_chunk_pairs() { return kChunkPairs; }
+size_t batch_gram_a_bytes(int Kp) { return size_t(kTileM) * 2 * Kp * 4; }
+size_t batch_gram_b_bytes(int Kp) { return size_t(kChunkN) * 2 * Kp * 4; }
+size_t batch_gram_bx_floats() { return kBx; }
+
+cudaError_t launch_batch_gram(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
+                              const int* d_tile_prefix, int total_tiles, int Kp, float wL, float wG, int* d_err,
+                              cudaStream_t s)
+{
+    if (n_jobs <= 0) return cudaSuccess;
+    if (Kp % 8 != 0 || Kp > 64) return cudaErrorInvalidValue;
+    if (max_tiles > 0) batch_gram_pack_a_kernel<<<dim3(max_tiles, n_jobs), 256, 0, s>>>(d_jobs, wL);
+    if (max_chunks > 0) batch_gram_pack_b_kernel<<<dim3(max_chunks, n_jobs), 256, 0, s>>>(d_jobs, wG);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || total_tiles <= 0) return e;
+    const int KE = 2 * Kp;
+    // two pipeline stages when that lets two CTAs share an SM, else three if they fit
+    int stages = (2 * gram_smem(KE, 3) > 227 * 1024) ? 2 : 3;
+    // every CTA holds 256 TMEM columns: at most two CTAs per SM (512 columns), so
+    // shared memory is padded to more than a third of the SM's
+    const size_t smem = std::max<size_t>(gram_smem(KE, stages), 80 * 1024);
+    e = cudaFuncSetAttribute(batch_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    batch_gram_kernel<<<total_tiles, kThreads, smem, s>>>(d_jobs, n_jobs, d_tile_prefix, KE, stages, d_err);
+    return cudaGetLastError();
+}
+
+} // namespace apsm

@@ -47,7 +47,10 @@ CFG = {"otype": "APSM", "windowSize": 20, "gaussianKernelVariance": 0.5, "eB": 0
     dict(CFG, trainingShuffle=True),
     dict(CFG, sampleStep=4),
     dict(CFG, gaussianKernelWeight=0.8, eB=0.001),
-], ids=["w20", "w80", "passes2", "sfw", "shuffle", "step4", "wG08"])
+    dict(CFG, detectVersion="gram_tf32x3"),
+    dict(CFG, windowSize=80, dictionarySize=2000, detectVersion="gram_tf32x3", gaussianKernelVariance=0.05,
+         eB=0.001),
+], ids=["w20", "w80", "passes2", "sfw", "shuffle", "step4", "wG08", "gram_tf32x3", "gram_tf32x3_narrow"])
 def test_pool_matches_oracle_per_detector(native_lib, oracle_mod, cfg):
     from libapsm_b200 import DetectorPool, PoolJob
 
@@ -92,10 +95,11 @@ def test_pool_train_append_and_eviction(native_lib, oracle_mod):
     assert rows == 2 * 200
 
 
-def test_pool_alone_equals_in_mix(native_lib):
+@pytest.mark.parametrize("dv", ["balanced", "gram_tf32x3"])
+def test_pool_alone_equals_in_mix(native_lib, dv):
     from libapsm_b200 import DetectorPool, PoolJob
 
-    cfg = dict(CFG, windowSize=80, dictionarySize=2000)
+    cfg = dict(CFG, windowSize=80, dictionarySize=2000, detectVersion=dv)
     N, P, S = 8, 400, 256
     rx, tx, rxd = _frame(11, N, P, S)
     alone = DetectorPool(cfg)
