@@ -140,11 +140,15 @@ typedef struct apsm_pool apsm_pool;
 
 typedef enum { APSM_JOB_TRAIN = 0, APSM_JOB_DETECT = 1 } apsm_job_kind;
 
+/* Train-job flag: reset the detector (resetState, apsm_noma_detector.cu:89-93)
+ * before training on this job's pilots. */
+#define APSM_JOB_FRESH 1u
+
 typedef struct {
     uint32_t detector; /* id from apsm_pool_add */
     uint32_t kind;     /* apsm_job_kind */
     uint32_t length;   /* pilots P (train) or data symbols S (detect) */
-    uint32_t reserved; /* 0 */
+    uint32_t flags;    /* APSM_JOB_FRESH or 0 */
     const float* rx;   /* N x length complex64, antenna-major (NomaDetector's rxSig[N][length]) */
     const float* tx;   /* train: length complex64 pilots of this detector's user; detect: NULL */
     float* est;        /* detect: length complex64 soft estimates (output); train: NULL */

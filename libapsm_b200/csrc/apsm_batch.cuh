@@ -22,8 +22,8 @@ struct BatchCommon {
     float wL, wG, eB;
     int qP;   // window length in pairs (windowSize)
     int sp;   // pairs entering per step (sampleStep / 2)
-    int LB;   // band length of a column: qP + sp
-    int XSP;  // pair slots of the sweep's window ring: qP + 2 sp
+    int LB;   // pairs of a column that enter the window kernel: qP + sp
+    int XSP;  // pair slots of the sweep's window ring: qP + 3 sp
     int XSPp; // pitch (floats) of the window kernel planes, multiple of 4, >= XSP
     int Np;   // largest complex row pitch of the jobs (float2 units)
 };
@@ -36,8 +36,7 @@ struct BatchTrainJob {
     const float* y;      // 2 nP targets (row form: Re x, Im x)
     float* a;            // 2 nP coefficients (row form); in: old rows, out: visible rows
     float* w;            // 2N linear weights (in/out)
-    const float4* Kc;    // kernel columns (A, Bp, Bm, 0), pairs n in [n_first, nP)
-    const float4* band;  // (nP - n_first) x LB window kernel values (A + wL r, Bp + wL m, Bm - wL m, 0)
+    const float4* Kc;    // combined kernel columns (A + wL r, Bp + wL m, Bm - wL m, 0), pairs n in [n_first, nP)
     const TrainStep* steps;
     int n_steps;
     int nP, N, Np, capP; // universe pairs, antennas, row pitch (float2), dictionary capacity in pairs
@@ -45,7 +44,7 @@ struct BatchTrainJob {
     int used_beforeP;    // pairs present before this call
     long long kc_base;   // column_prefix(n_first)
     float ew;            // -0.5 / (variance * N^2)
-    int err;             // unused by the kernels (host bookkeeping)
+    int fresh;           // start from a fresh state (w = 0; the universe holds only the new pilots)
 };
 
 // Column n holds pairs [col_begin(n), col_end(n)).

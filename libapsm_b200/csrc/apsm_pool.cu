@@ -4,7 +4,7 @@
 // A batch is laid out in one scratch buffer of its lane: the job descriptors
 // (filled in a pinned host buffer, one copy), the staged host inputs, each
 // training job's universe (its dictionary pairs, then the new pilots), kernel
-// columns and bands, and each detection job's packed samples.  Launch order
+// columns, and each detection job's packed samples.  Launch order
 // on the lane's stream: dictionary -> universe copies, packing, kernel
 // columns, the persistent sweep, universe tail -> dictionary copies, then the
 // detection launches (one per antenna class).
@@ -141,11 +141,12 @@ struct TrainPlan {
     int final_hi = 0;
     uint32_t P = 0, usedP = 0, nP = 0, n_first = 0;
     long long kc_base = 0, n_kc = 0;
-    size_t off_rx = 0, off_tx = 0, off_Y = 0, off_nrm = 0, off_y = 0, off_a = 0, off_kc = 0, off_band = 0;
+    size_t off_rx = 0, off_tx = 0, off_Y = 0, off_nrm = 0, off_y = 0, off_a = 0, off_kc = 0;
     size_t off_steps = 0;
     uint32_t usedP_new = 0, lo_new = 0;
     const int* perm_dev = nullptr;
     size_t perm_off = 0;
+    bool fresh = false;
 };
 
 struct DetectPlan {
@@ -180,7 +181,7 @@ size_t apsm_pool::train_bytes(const PoolDet& d, uint32_t P, bool host) const
     const size_t first = usedP > q ? usedP - q : 0;
     const size_t cols = nP - first;
     const size_t len = std::min<size_t>(d.capP, nP) + q;
-    b += align_up(sizeof(float4) * cols * len, 256) + align_up(sizeof(float4) * cols * cm.LB, 256);
+    b += align_up(sizeof(float4) * cols * len, 256);
     b += align_up(sizeof(TrainStep) * (size_t(cfg.passes) * (P + q + 2) + 4), 256) + align_up(sizeof(int) * P, 256);
     b += 4 * sizeof(BatchTrainJob) + 4 * sizeof(BatchPackJob) + 4 * sizeof(BatchCopyJob);
     return b;
@@ -208,7 +209,15 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
             return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": unknown detector");
         if (j.kind != APSM_JOB_TRAIN && j.kind != APSM_JOB_DETECT)
             return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": unknown kind");
-        if (j.length == 0) continue;
+        if (j.length == 0) {
+            if (j.kind == APSM_JOB_TRAIN && (j.flags & APSM_JOB_FRESH)) {
+                if (trained[j.detector])
+                    return fail(APSM_ERR_INVALID_ARGUMENT, "detector " + std::to_string(j.detector) +
+                                                               " is trained twice in one batch");
+                trained[j.detector] = 1;
+            }
+            continue;
+        }
         if (!j.rx) return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null rx");
         if (j.kind == APSM_JOB_TRAIN) {
             if (!j.tx) return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null tx");
@@ -230,8 +239,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
             t.job = i;
             t.det = &dets[jobs[i].detector];
             t.P = jobs[i].length;
-            t.steps = build_schedule(cfg, t.det->used, t.P, cap, &t.final_hi);
-            t.usedP = t.det->used / 2;
+            t.fresh = (jobs[i].flags & APSM_JOB_FRESH) != 0;
+            const uint32_t used0 = t.fresh ? 0u : t.det->used;
+            t.steps = build_schedule(cfg, used0, t.P, cap, &t.final_hi);
+            t.usedP = used0 / 2;
             t.nP = t.usedP + t.P;
             t.n_first = t.steps.empty() ? t.nP : uint32_t(t.steps[0].hi - t.steps[0].wk) / 2;
             t.kc_base = column_prefix(t.n_first, cm.qP, t.nP, t.det->capP);
@@ -247,6 +258,12 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
     // dictionary sizes after this batch's training, for the detection jobs
     std::vector<uint32_t> used_after(dets.size());
     for (size_t d = 0; d < dets.size(); ++d) used_after[d] = dets[d].used;
+    std::vector<PoolDet*> resets;
+    for (uint32_t i = 0; i < n; ++i)
+        if (jobs[i].kind == APSM_JOB_TRAIN && jobs[i].length == 0 && (jobs[i].flags & APSM_JOB_FRESH)) {
+            resets.push_back(&dets[jobs[i].detector]);
+            used_after[jobs[i].detector] = 0;
+        }
     for (const auto& t : tp) used_after[jobs[t.job].detector] = 2 * t.usedP_new;
     for (uint32_t i = 0; i < n; ++i)
         if (jobs[i].kind == APSM_JOB_DETECT && jobs[i].length > 0) {
@@ -317,7 +334,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         t.off_y = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
         t.off_a = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
         t.off_kc = o; o = align_up(o + sizeof(float4) * size_t(std::max<long long>(t.n_kc, 1)), 256);
-        t.off_band = o; o = align_up(o + sizeof(float4) * size_t(t.nP - t.n_first + 1) * cm.LB, 256);
     }
     for (auto& d : dp) {
         if (host) {
@@ -398,7 +414,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         tj.a = av;
         tj.w = d.w;
         tj.Kc = reinterpret_cast<const float4*>(D(t.off_kc));
-        tj.band = reinterpret_cast<const float4*>(D(t.off_band));
         tj.steps = reinterpret_cast<const TrainStep*>(D(t.off_steps));
         tj.n_steps = int(t.steps.size());
         tj.nP = int(t.nP);
@@ -409,6 +424,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         tj.used_beforeP = int(t.usedP);
         tj.kc_base = t.kc_base;
         tj.ew = d.ew;
+        tj.fresh = t.fresh ? 1 : 0;
         h_tj[k] = tj;
         max_cols = std::max(max_cols, int(t.nP - t.n_first));
         h_co[k] = BatchCopyJob{Y + size_t(t.lo_new) * d.Np, nrm + t.lo_new, yv + 2 * t.lo_new, av + 2 * t.lo_new,
@@ -492,6 +508,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
     POOL_CK(cudaEventRecord(L.desc_copied, s));
     L.have_train = nT > 0;
     L.have_detect = nD > 0;
+    for (PoolDet* d : resets) {
+        POOL_CK(cudaMemsetAsync(d->w, 0, sizeof(float) * 2 * d->N, s));
+        d->used = 0;
+    }
     int* d_counter = reinterpret_cast<int*>(D(off_counter));
     int* d_err = d_counter + 4;
     POOL_CK(cudaMemsetAsync(d_counter, 0, 32, s));
@@ -617,7 +637,7 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
     cm.qP = int(cfg.window);
     cm.sp = int(cfg.step / 2);
     cm.LB = cm.qP + cm.sp;
-    cm.XSP = cm.qP + 2 * cm.sp;
+    cm.XSP = cm.qP + 3 * cm.sp;
     cm.XSPp = int(round_up(uint32_t(cm.XSP) + 1, 4));
     cm.Np = 32; // sweep shared memory sized for N <= 32; larger N re-sizes at add
     auto failp = [&](const std::string& m, apsm_status st) {

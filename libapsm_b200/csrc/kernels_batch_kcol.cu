@@ -1,13 +1,13 @@
 // Kernel columns of the batched training sweep, all jobs in one launch.
 //
-// For every pair n that enters a window during the sweep, column n holds the
-// three distinct Gaussian kernel values (A, Bp, Bm) against every pair b the
-// sweep may combine with n: b in [max(0, n + 1 - capP), min(n + qP, nP)).
-// The band of n additionally holds the window kernel values with the linear
-// kernel folded in, Kt = K + wL <x, x'>, for b in [n - LB + 1, n]; the sweep
-// keeps its window predictions current with them.  Same quantities as the
-// reference's per-evaluation distance loop (cpp/lib/apsm/apsm_detect.cu:131-152)
-// and linear kernel (:103-129), formed from y_b^H y_n and the row norms.
+// For every pair n that enters a window during the sweep, column n holds,
+// against every pair b the sweep may combine with n (b in
+// [max(0, n + 1 - capP), min(n + qP, nP))), the three distinct values of the
+// combined kernel Kt = K + wL <x, x'> (Gaussian plus weighted linear kernel):
+// (A + wL r, Bp + wL m, Bm - wL m) with r + i m = y_b^H y_n.  Same
+// quantities as the reference's per-evaluation distance loop
+// (cpp/lib/apsm/apsm_detect.cu:131-152) and linear kernel (:103-129), formed
+// from y_b^H y_n and the row norms.
 #include "apsm_batch.cuh"
 
 namespace apsm {
@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(kColRows)
     batch_kcol_kernel(const BatchTrainJob* __restrict__ jobs, BatchCommon cm, int smem_n)
 {
     const BatchTrainJob& jb = jobs[blockIdx.y];
-    const int nP = jb.nP, N = jb.N, Np = jb.Np, capP = jb.capP, qP = cm.qP, LB = cm.LB;
+    const int nP = jb.nP, N = jb.N, Np = jb.Np, capP = jb.capP, qP = cm.qP;
     const int n0 = jb.n_first + blockIdx.x * kColGroup;
     if (n0 >= nP || N > smem_n) return; // shared memory is sized for smem_n antennas
     const int nc = min(kColGroup, nP - n0);
@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(kColRows)
 #pragma unroll
     for (int c = 0; c < kColGroup; ++c) nn[c] = c < nc ? jb.nrm[n0 + c] : 0.f;
 
-    const int b_lo = col_begin(n0, capP);
+    const int b_lo = col_begin(n0, capP); // columns of the group start no earlier
     const int b_hi = col_end(n0 + nc - 1, qP, nP);
     for (int b0 = b_lo; b0 < b_hi; b0 += kColRows) {
         __syncthreads();
@@ -72,22 +72,13 @@ __global__ void __launch_bounds__(kColRows)
         for (int c = 0; c < kColGroup; ++c) {
             if (c >= nc) break;
             const int n = n0 + c;
-            const bool in_col = b >= col_begin(n, capP) && b < col_end(n, qP, nP);
-            const bool in_band = b <= n && b > n - LB;
-            if (!in_col && !in_band) continue;
+            if (b < col_begin(n, capP) || b >= col_end(n, qP, nP)) continue;
             const float s = nb + nn[c];
             const float A = wG * expf(ew * fmaxf(fmaf(-2.f, re[c], s), 0.f));
             const float Bp = wG * expf(ew * fmaxf(fmaf(-2.f, im[c], s), 0.f));
             const float Bm = wG * expf(ew * fmaxf(fmaf(2.f, im[c], s), 0.f));
-            if (in_col) {
-                const long long off = column_prefix(n, qP, nP, capP) - jb.kc_base + (b - col_begin(n, capP));
-                const_cast<float4*>(jb.Kc)[off] = make_float4(A, Bp, Bm, 0.f);
-            }
-            if (in_band) {
-                const size_t off = size_t(n - jb.n_first) * LB + (b - (n - LB + 1));
-                const_cast<float4*>(jb.band)[off] =
-                    make_float4(fmaf(wL, re[c], A), fmaf(wL, im[c], Bp), fmaf(-wL, im[c], Bm), 0.f);
-            }
+            const long long off = column_prefix(n, qP, nP, capP) - jb.kc_base + (b - col_begin(n, capP));
+            const_cast<float4*>(jb.Kc)[off] = make_float4(fmaf(wL, re[c], A), fmaf(wL, im[c], Bp), fmaf(-wL, im[c], Bm), 0.f);
         }
     }
 }

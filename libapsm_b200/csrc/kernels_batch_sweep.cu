@@ -10,20 +10,25 @@
 // then a_j += c_j and w += sum_j c_j x_j, all from the pre-step values.
 //
 // Incremental, pair-form evaluation (the floating-point order differs from
-// the reference; results agree to ~1e-6 relative, the FP32 bar is 1e-4):
-//   * every window row keeps its whole prediction f_j; after a step it adds
-//     sum_i c_i Kt(i, j) with the window kernel Kt = K + wL <x_i, x_j>, which
-//     accounts for the change of both a and w;
-//   * a pair entering the window starts from wL <x_n, w> + sum_b a_b K(b, n),
-//     formed one step ahead from kernel-column values that were prefetched
-//     into registers one step before that (rows that already left the window
-//     have final coefficients and are read with the prefetch; rows still in
-//     the ring come from shared memory);
-//   * when the dictionary is full, the evicted pairs' terms leave the sums.
-// The window (samples, targets, norms, coefficients, predictions) and its
-// kernel, as three planes A / Bp / Bm indexed [row slot][column slot], live in
-// shared memory; pair p occupies slot p mod XSP.  Two block barriers per step.
-// The kernel has no inter-block waits.
+// the reference, and the two divisions of the projection are products with
+// reciprocals; results agree to ~1e-6 relative, the FP32 bar is 1e-4).  With
+// the combined kernel Kt = K + wL <x, x'> and the residual weights
+// r = w - sum_{b visible} a_b x_b (zero for a fresh detector),
+//     f_j = wL <x_j, r> + sum_{b visible} a_b Kt(b, j),
+// and a step changes only window coefficients, so r stays fixed until a
+// dictionary entry is evicted (then r += a_b x_b and the entry's K term leaves
+// the sums).  Therefore:
+//   * every window row keeps its whole prediction; after a step it adds
+//     sum_i c_i Kt(i, j) (the window kernel lives in shared memory as three
+//     planes A / Bp / Bm indexed [row slot][column slot]; pair p occupies
+//     slot p mod XSP);
+//   * a pair entering at step t+1 starts from wL <x_n, r> + sum_b a_b Kt(b, n),
+//     formed in three stages: its kernel-column values and the coefficients
+//     of the pairs that left the window are loaded at step t-2, the part over
+//     those final coefficients is summed at step t-1, and the part over the
+//     pairs still in the window ring (shared memory) is added at step t;
+//   * w = r + sum_b a_b x_b is formed once at the end.
+// Two block barriers per step; the kernel has no inter-block waits.
 #include "apsm_batch.cuh"
 
 namespace apsm {
@@ -32,24 +37,33 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kPf = 8;        // prefetched column entries per thread: columns up to kThreads * kPf pairs
-constexpr int kParts = 4;     // row-slot parts of the window update
+constexpr int kPf = 8;        // frozen column entries per thread: up to kThreads * kPf pairs per column
+constexpr int kParts = 6;     // row-slot parts of the window update
 constexpr int kMaxEnter = 4;  // pairs entering per step (sampleStep <= 8)
 
 struct PairStep {
     int hiP, sP, nAP, loP, wk;
 };
 
-__device__ __forceinline__ PairStep pair_step(const TrainStep& s, int capP)
+__device__ __forceinline__ PairStep pair_step(const int4& s, int capP)
 {
+    // s = TrainStep {hi, wk, n_active, reveal_lo}
     PairStep p;
-    p.hiP = s.hi >> 1;
-    p.sP = (s.hi - s.wk) >> 1;
-    p.nAP = s.n_active >> 1;
+    p.hiP = s.x >> 1;
+    p.sP = (s.x - s.y) >> 1;
+    p.nAP = s.z >> 1;
     p.loP = max(0, p.hiP - capP);
-    p.wk = s.wk;
+    p.wk = s.y;
     return p;
 }
+
+// A pair entering the window, as staged by the pipeline: frozen part
+// [lo, F) (final coefficients), window part [F, top) (ring coefficients).
+struct Entry {
+    int n;    // pair, -1 when no pair enters at that step
+    int lo, F, top;
+    int slow; // served by direct loads when consumed
+};
 
 __device__ __forceinline__ float hyperslab(float e, float eB)
 {
@@ -59,7 +73,7 @@ __device__ __forceinline__ float hyperslab(float e, float eB)
     return 0.f;
 }
 
-// a_{2b} K(2b, .) + a_{2b+1} K(2b+1, .) for the two rows of the column's pair
+// a_{2b} Kt(2b, .) + a_{2b+1} Kt(2b+1, .) for the two rows of the column's pair
 __device__ __forceinline__ void acc_pair(float2 ab, float4 kv, float& g0, float& g1)
 {
     g0 = fmaf(ab.x, kv.x, fmaf(ab.y, kv.z, g0));
@@ -82,12 +96,12 @@ __global__ void __launch_bounds__(kThreads, 2)
 {
     extern __shared__ __align__(16) float smem[];
     __shared__ int job_s;
+    __shared__ BatchTrainJob js;
     const int XSP = cm.XSP, XSPp = cm.XSPp, LB = cm.LB, qP = cm.qP;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const float wL = cm.wL, wG = cm.wG, eB = cm.eB;
     const int Lp = (XSP + kParts - 1) / kParts; // row slots per part
     const int ncp = (XSP + 1) / 2;              // column-slot pairs
-    const int halfP = (XSP + 1) / 2;            // row slots per half of the w update
 
     float* KA = smem;                                        // [XSP][XSPp]
     float* KP = KA + XSP * XSPp;                             // [XSP][XSPp]
@@ -97,39 +111,33 @@ __global__ void __launch_bounds__(kThreads, 2)
     float* yw = hw + 2 * XSPp;                               // targets
     float* aw = yw + 2 * XSPp;                               // coefficients
     float* cs = aw + 2 * XSPp;                               // corrections of the step (0 when inactive)
-    float* nw = cs + 2 * XSPp;                               // [XSPp] norms by pair slot
-    float* red = nw + XSPp;                                  // [kParts][2 XSPp] window-update partials
-    float* w_s = red + kParts * 2 * XSPp;                    // [kMaxFeatures]
-    float* wred = w_s + kMaxFeatures;                        // [2][kMaxFeatures] w-update partials
-    float* wp = wred + 2 * kMaxFeatures;                     // [kMaxEnter][kWarps][2] entering partial sums
+    float* rd = cs + 2 * XSPp;                               // [XSPp] 1 / (wL |x|^2 + wG) by pair slot
+    float* red = rd + XSPp;                                  // [kParts][2 XSPp] window-update partials
+    float* r_s = red + kParts * 2 * XSPp;                    // [kMaxFeatures] residual weights r
+    float* dr = r_s + kMaxFeatures;                          // [kMaxFeatures] r increment of an eviction
+    float* wp = dr + kMaxFeatures;                           // [kMaxEnter][kWarps][2] entering partial sums
 
     for (;;) {
         __syncthreads();
-        if (tid == 0) job_s = atomicAdd(counter, 1);
+        if (tid == 0) {
+            job_s = atomicAdd(counter, 1);
+            if (job_s < n_jobs) js = jobs[job_s];
+        }
         __syncthreads();
-        const int jid = job_s;
-        if (jid >= n_jobs) break;
-        const BatchTrainJob& jb = jobs[jid];
-        const int N = jb.N, Np = jb.Np, capP = jb.capP, nP = jb.nP, n_steps = jb.n_steps;
+        if (job_s >= n_jobs) break;
+        const int N = js.N, Np = js.Np, capP = js.capP, nP = js.nP, n_steps = js.n_steps;
         const int D = 2 * N;
-        const float2* __restrict__ Y = jb.Y;
-        float* __restrict__ ag = jb.a;
-        const long long kc_base = jb.kc_base;
+        const float ew = js.ew;
+        const float2* __restrict__ Y = js.Y;
+        float* __restrict__ ag = js.a;
+        const int4* __restrict__ steps = reinterpret_cast<const int4*>(js.steps);
 
         auto col_ptr = [&](int n) -> const float4* {
-            return jb.Kc + (column_prefix(n, qP, nP, capP) - kc_base) - col_begin(n, capP);
+            return js.Kc + (column_prefix(n, qP, nP, capP) - js.kc_base) - col_begin(n, capP);
         };
-        auto band_ptr = [&](int n) -> const float4* { // indexed by pair b in [n - LB + 1, n]
-            return jb.band + size_t(n - jb.n_first) * LB - (n - LB + 1);
-        };
-        auto slot_of = [&](int p) { return p % XSP; };
-        auto pair_in = [&](int q, int lo) { // pair in slot q among the XSP pairs starting at lo
-            int d = q - lo % XSP;
-            if (d < 0) d += XSP;
-            return lo + d;
-        };
-        auto fill_band = [&](int n, int b, float4 kt) { // window kernel block (b, n) and its transpose
-            const int sb = slot_of(b), qn = slot_of(n);
+        auto wrap_slot = [&](int s) { return s >= XSP ? s - XSP : (s < 0 ? s + XSP : s); };
+        // window kernel block (b, n) and its transpose, slots sb / qn
+        auto fill_band = [&](int sb, int qn, float4 kt) {
             KA[sb * XSPp + qn] = kt.x;
             KP[sb * XSPp + qn] = kt.y;
             KM[sb * XSPp + qn] = kt.z;
@@ -137,255 +145,315 @@ __global__ void __launch_bounds__(kThreads, 2)
             KP[qn * XSPp + sb] = kt.z;
             KM[qn * XSPp + sb] = kt.y;
         };
-        // linear-term contribution of feature d (< D) of pair value v = y_n[d mod N] with weight wd
+        // diagonal block of pair n with squared norm nv: r = nv, m = 0
+        auto fill_diag = [&](int qn, float nv) {
+            const float b = wG * expf(ew * (2.f * nv));
+            KA[qn * XSPp + qn] = fmaf(wL, nv, wG);
+            KP[qn * XSPp + qn] = b;
+            KM[qn * XSPp + qn] = b;
+        };
+        // linear-term contribution of feature d (< D) with weight wd of pair value v = y_n[d mod N]
         auto lin_feature = [&](int d, float wd, float2 v, float& g0, float& g1) {
+            const float lw = wL * wd;
             if (d < N) {
-                g0 = fmaf(wL * wd, v.x, g0);
-                g1 = fmaf(wL * wd, v.y, g1);
+                g0 = fmaf(lw, v.x, g0);
+                g1 = fmaf(lw, v.y, g1);
             } else {
-                g0 = fmaf(wL * wd, v.y, g0);
-                g1 = fmaf(-wL * wd, v.x, g1);
+                g0 = fmaf(lw, v.y, g0);
+                g1 = fmaf(-lw, v.x, g1);
             }
+        };
+        // sum_b (a_2b x_2b + a_2b+1 x_2b+1)[d] over pairs [b0, b1) (global state)
+        auto ax_sum = [&](int d, int b0, int b1) {
+            const int k = d < N ? d : d - N;
+            float acc = 0.f;
+            for (int b = b0; b < b1; ++b) {
+                const float2 ab = *reinterpret_cast<const float2*>(ag + 2 * b);
+                const float2 v = Y[size_t(b) * Np + k];
+                acc = d < N ? fmaf(ab.x, v.x, fmaf(ab.y, v.y, acc)) : fmaf(ab.x, v.y, fmaf(-ab.y, v.x, acc));
+            }
+            return acc;
         };
 
         // ---- job state ----
         for (int i = tid; i < 3 * XSP * XSPp; i += kThreads) KA[i] = 0.f;
         for (int i = tid; i < XSP * Np; i += kThreads) Yw[i] = make_float2(0.f, 0.f);
         for (int i = tid; i < 2 * XSPp; i += kThreads) hw[i] = yw[i] = aw[i] = cs[i] = 0.f;
-        for (int i = tid; i < XSPp; i += kThreads) nw[i] = 0.f;
+        for (int i = tid; i < XSPp; i += kThreads) rd[i] = 0.f;
         for (int i = tid; i < kParts * 2 * XSPp; i += kThreads) red[i] = 0.f;
-        for (int i = tid; i < kMaxFeatures; i += kThreads) {
-            w_s[i] = i < D ? jb.w[i] : 0.f;
-            wred[i] = wred[kMaxFeatures + i] = 0.f;
+        PairStep pc = pair_step(n_steps > 0 ? steps[0] : make_int4(0, 0, 0, 0), capP);
+        for (int d = tid; d < kMaxFeatures; d += kThreads) {
+            float r = 0.f;
+            if (d < D && !js.fresh) r = js.w[d] - (n_steps > 0 ? ax_sum(d, pc.loP, js.used_beforeP) : 0.f);
+            r_s[d] = r;
         }
-        if (n_steps <= 0) continue;
+        if (n_steps <= 0) continue; // w unchanged
         __syncthreads();
 
-        PairStep pc = pair_step(jb.steps[0], capP);
+        int4 st_n = steps[n_steps > 1 ? 1 : 0];
+        int4 st_nn = steps[n_steps > 2 ? 2 : 0];
+        int4 st_3 = steps[n_steps > 3 ? 3 : 0];
 
         // ---- prologue: the pairs of the first window enter with direct loads ----
         {
-            const int e_lo = pc.sP, e_hi = pc.hiP, top = jb.used_beforeP;
+            const int e_lo = pc.sP, e_hi = pc.hiP, top = js.used_beforeP;
             for (int j = e_lo + warp; j < e_hi; j += kWarps) {
-                const int q = slot_of(j);
+                const int q = j % XSP;
                 for (int k = lane; k < Np; k += 32) Yw[q * Np + k] = Y[size_t(j) * Np + k];
                 float g0 = 0.f, g1 = 0.f;
                 const float4* col = col_ptr(j);
                 for (int b = pc.loP + lane; b < top; b += 32)
                     acc_pair(*reinterpret_cast<const float2*>(ag + 2 * b), col[b], g0, g1);
-                for (int d = lane; d < D; d += 32) lin_feature(d, w_s[d], Y[size_t(j) * Np + d % N], g0, g1);
+                for (int d = lane; d < D; d += 32) lin_feature(d, r_s[d], Y[size_t(j) * Np + d % N], g0, g1);
                 warp_sum2(g0, g1);
                 if (lane == 0) {
                     hw[2 * q] = g0;
                     hw[2 * q + 1] = g1;
-                    yw[2 * q] = jb.y[2 * j];
-                    yw[2 * q + 1] = jb.y[2 * j + 1];
+                    yw[2 * q] = js.y[2 * j];
+                    yw[2 * q + 1] = js.y[2 * j + 1];
                     aw[2 * q] = ag[2 * j];
                     aw[2 * q + 1] = ag[2 * j + 1];
-                    nw[q] = jb.nrm[j];
+                    rd[q] = 1.f / fmaf(wL, js.nrm[j], wG);
                 }
-                const float4* bnd = band_ptr(j);
-                for (int b = max(e_lo, j - LB + 1) + lane; b <= j; b += 32) fill_band(j, b, bnd[b]);
+                for (int b = max(e_lo, j - LB + 1) + lane; b <= j; b += 32) fill_band(b % XSP, q, col[b]);
             }
         }
 
-        // ---- register prefetch for the pair entering at step tt ----
-        int pf_n = -1, pf_lo = 0, pf_top = 0, pf_fb = 0;
-        float4 pf_k[kPf];
-        float2 pf_a[kPf];
-        float4 pf_band = make_float4(0.f, 0.f, 0.f, 0.f);
-        float2 pf_y = make_float2(0.f, 0.f);
-        float pf_t0 = 0.f, pf_t1 = 0.f, pf_nv = 0.f;
-        auto prefetch = [&](int tt, int fb) {
-            pf_n = -1;
+        // ---- the entering-pair pipeline (see the header) ----
+        Entry e_cur{-1, 0, 0, 0, 0}, e_nxt{-1, 0, 0, 0, 0};
+        float4 colbuf[kPf];
+        float2 abuf[kPf];
+        float4 win_cur = make_float4(0.f, 0.f, 0.f, 0.f), win_nxt = win_cur;
+        float2 y_cur = make_float2(0.f, 0.f), y_nxt = y_cur;
+        float t_cur0 = 0.f, t_cur1 = 0.f, n_cur = 0.f, t_nxt0 = 0.f, t_nxt1 = 0.f, n_nxt = 0.f;
+        float gf0 = 0.f, gf1 = 0.f; // this thread's part of the frozen sum of e_cur
+        // stage 1: loads for the pair entering at step tt (frozen boundary F)
+        auto issue = [&](int tt, const int4& st_tt, const int4& st_prev, int F) {
+            e_nxt.n = -1;
+            e_nxt.slow = 0;
             if (tt <= 0 || tt >= n_steps) return;
-            const PairStep ps = pair_step(jb.steps[tt], capP), pv = pair_step(jb.steps[tt - 1], capP);
-            const int e_lo = max(pv.hiP, ps.sP);
-            if (ps.hiP - e_lo != 1 || pv.hiP - ps.loP > kThreads * kPf || LB > kThreads || D > kThreads)
-                return; // direct loads instead
+            const PairStep ps = pair_step(st_tt, capP), pv = pair_step(st_prev, capP);
+            const int e_lo = max(pv.hiP, ps.sP), ne = ps.hiP - e_lo;
+            if (ne <= 0) return;
+            e_nxt.n = e_lo;
+            e_nxt.lo = ps.loP;
+            e_nxt.top = pv.hiP;
+            e_nxt.F = min(max(F, e_nxt.lo), e_nxt.top);
+            if (ne != 1 || e_nxt.F - e_nxt.lo > kThreads * kPf || e_nxt.top - e_nxt.F > kThreads || D > kThreads) {
+                e_nxt.slow = 1;
+                return;
+            }
             const int n = e_lo;
-            pf_n = n;
-            pf_lo = ps.loP;
-            pf_top = pv.hiP;
-            pf_fb = min(fb, pf_top);
             const float4* col = col_ptr(n);
 #pragma unroll
             for (int k = 0; k < kPf; ++k) {
-                const int b = pf_lo + tid + k * kThreads;
-                pf_k[k] = b < pf_top ? __ldg(col + b) : make_float4(0.f, 0.f, 0.f, 0.f);
-                pf_a[k] = b < pf_fb ? *reinterpret_cast<const float2*>(ag + 2 * b) : make_float2(0.f, 0.f);
+                const int b = e_nxt.lo + tid + k * kThreads;
+                const bool ok = b < e_nxt.F;
+                colbuf[k] = ok ? __ldg(col + b) : make_float4(0.f, 0.f, 0.f, 0.f);
+                abuf[k] = ok ? *reinterpret_cast<const float2*>(ag + 2 * b) : make_float2(0.f, 0.f);
             }
-            if (tid < LB && n - LB + 1 + tid >= 0) pf_band = __ldg(band_ptr(n) + (n - LB + 1 + tid));
-            if (tid < D) pf_y = Y[size_t(n) * Np + tid % N];
+            const int bw = e_nxt.F + tid;
+            win_nxt = bw < e_nxt.top ? __ldg(col + bw) : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (tid < D) y_nxt = Y[size_t(n) * Np + tid % N];
             if (tid == 0) {
-                pf_t0 = jb.y[2 * n];
-                pf_t1 = jb.y[2 * n + 1];
-                pf_nv = jb.nrm[n];
+                t_nxt0 = js.y[2 * n];
+                t_nxt1 = js.y[2 * n + 1];
+                n_nxt = js.nrm[n];
             }
         };
-        prefetch(1, pc.sP);
+        // stage 2: this thread's share of the frozen sum of e_nxt, then e_nxt becomes e_cur
+        auto advance = [&]() {
+            gf0 = gf1 = 0.f;
+            if (e_nxt.n >= 0 && !e_nxt.slow) {
+#pragma unroll
+                for (int k = 0; k < kPf; ++k) acc_pair(abuf[k], colbuf[k], gf0, gf1);
+            }
+            e_cur = e_nxt;
+            win_cur = win_nxt;
+            y_cur = y_nxt;
+            t_cur0 = t_nxt0;
+            t_cur1 = t_nxt1;
+            n_cur = n_nxt;
+        };
+        issue(1, st_n, steps[0], pc.sP);
+        advance();
+        issue(2, st_nn, st_n, pc.sP);
         __syncthreads();
 
-        TrainStep s_nxt = n_steps > 1 ? jb.steps[1] : jb.steps[0];
+        int los = pc.sP % XSP; // slot of the window's first pair
 #pragma unroll 1
         for (int t = 0; t < n_steps; ++t) {
             const bool has_next = t + 1 < n_steps;
-            const PairStep pn = has_next ? pair_step(s_nxt, capP) : pc;
+            const PairStep pn = has_next ? pair_step(st_n, capP) : pc;
             const int e_lo = has_next ? max(pc.hiP, pn.sP) : 0;
             const int ne = has_next ? max(0, pn.hiP - e_lo) : 0; // pairs entering at t+1
+            const int4 st_4 = t + 4 < n_steps ? steps[t + 4] : st_3;
+            const float inv_wk = 1.f / float(pc.wk);
 
             // ================= phase 1 =================
             // (1a) window rows: fold the last update in; corrections of the active rows
             for (int r = tid; r < 2 * XSP; r += kThreads) {
                 const int q = r >> 1;
-                const int p = pair_in(q, pc.sP);
+                int d = q - los;
+                if (d < 0) d += XSP;
                 float c = 0.f;
-                if (p < pc.hiP) {
-                    const float h = hw[r] + ((red[r] + red[2 * XSPp + r]) + (red[4 * XSPp + r] + red[6 * XSPp + r]));
+                if (d < pc.hiP - pc.sP) {
+                    float h = hw[r];
+#pragma unroll
+                    for (int pt = 0; pt < kParts; ++pt) h += red[pt * 2 * XSPp + r];
                     hw[r] = h;
-                    if (p - pc.sP < pc.nAP) {
-                        c = hyperslab(__fsub_rn(yw[r], h), eB);
-                        c = __fdiv_rn(c, float(pc.wk));
-                        c = __fdiv_rn(c, __fadd_rn(__fmul_rn(wL, nw[q]), wG));
-                    }
+                    if (d < pc.nAP) c = hyperslab(__fsub_rn(yw[r], h), eB) * inv_wk * rd[q];
                 }
                 cs[r] = c;
             }
-            // (1b) w(t): fold the last w update in
-            float wd = 0.f;
-            if (tid < D) {
-                wd = w_s[tid] + (wred[tid] + wred[kMaxFeatures + tid]);
-                w_s[tid] = wd;
-            }
-            // (1c) pairs entering at t+1: data, window kernel, start of their predictions
-            if (ne == 1 && pf_n == e_lo) {
-                const int n = pf_n, qn = slot_of(n);
-                float g0 = 0.f, g1 = 0.f;
-#pragma unroll
-                for (int k = 0; k < kPf; ++k) {
-                    const int b = pf_lo + tid + k * kThreads;
-                    if (b < pf_top) {
-                        const float2 ab = b < pf_fb ? pf_a[k] : *reinterpret_cast<const float2*>(aw + 2 * slot_of(b));
-                        acc_pair(ab, pf_k[k], g0, g1);
-                    }
+            // (1b) pairs entering at t+1: data, window kernel, start of their predictions
+            if (ne == 1 && e_cur.n == e_lo && !e_cur.slow) {
+                const int n = e_cur.n, qn = n % XSP;
+                float g0 = gf0, g1 = gf1;
+                const int bw = e_cur.F + tid;
+                if (bw < e_cur.top) {
+                    const int sl = wrap_slot(e_cur.F % XSP + tid);
+                    acc_pair(*reinterpret_cast<const float2*>(aw + 2 * sl), win_cur, g0, g1);
+                    if (bw > n - LB) fill_band(sl, qn, win_cur);
                 }
-                if (tid < D) lin_feature(tid, wd, pf_y, g0, g1);
+                if (tid < D) lin_feature(tid, r_s[tid], y_cur, g0, g1);
                 warp_sum2(g0, g1);
                 if (lane == 0) {
                     wp[2 * warp] = g0;
                     wp[2 * warp + 1] = g1;
                 }
-                if (tid < LB && n - LB + 1 + tid >= 0) fill_band(n, n - LB + 1 + tid, pf_band);
-                if (tid < Np) Yw[qn * Np + tid] = tid < N ? pf_y : make_float2(0.f, 0.f);
+                if (tid < Np) Yw[qn * Np + tid] = tid < N ? y_cur : make_float2(0.f, 0.f);
                 if (tid == 0) {
-                    yw[2 * qn] = pf_t0;
-                    yw[2 * qn + 1] = pf_t1;
+                    yw[2 * qn] = t_cur0;
+                    yw[2 * qn + 1] = t_cur1;
                     aw[2 * qn] = aw[2 * qn + 1] = 0.f;
-                    nw[qn] = pf_nv;
+                    rd[qn] = 1.f / fmaf(wL, n_cur, wG);
+                    fill_diag(qn, n_cur);
                 }
             } else if (ne > 0) {
-                // direct loads (several pairs per step, or a column longer than the registers hold)
+                // direct loads (several pairs per step, or columns longer than the pipeline holds)
                 const int top = pc.hiP, lo = pn.loP, fb = pc.sP;
                 for (int e = 0; e < min(ne, kMaxEnter); ++e) {
-                    const int n = e_lo + e, qn = slot_of(n);
+                    const int n = e_lo + e, qn = n % XSP;
                     const float4* col = col_ptr(n);
                     float g0 = 0.f, g1 = 0.f;
                     for (int b = lo + tid; b < top; b += kThreads) {
                         const float2 ab = b < fb ? *reinterpret_cast<const float2*>(ag + 2 * b)
-                                                 : *reinterpret_cast<const float2*>(aw + 2 * slot_of(b));
+                                                 : *reinterpret_cast<const float2*>(aw + 2 * (b % XSP));
                         acc_pair(ab, col[b], g0, g1);
                     }
-                    if (tid < D) lin_feature(tid, wd, Y[size_t(n) * Np + tid % N], g0, g1);
+                    if (tid < D) lin_feature(tid, r_s[tid], Y[size_t(n) * Np + tid % N], g0, g1);
                     warp_sum2(g0, g1);
                     if (lane == 0) {
                         wp[(e * kWarps + warp) * 2] = g0;
                         wp[(e * kWarps + warp) * 2 + 1] = g1;
                     }
-                    const float4* bnd = band_ptr(n);
-                    for (int i = tid; i < LB; i += kThreads) {
-                        const int b = n - LB + 1 + i;
-                        if (b >= 0) fill_band(n, b, bnd[b]);
-                    }
+                    for (int b = max(0, n - LB + 1) + tid; b < n; b += kThreads) fill_band(b % XSP, qn, col[b]);
                     for (int k = tid; k < Np; k += kThreads) Yw[qn * Np + k] = Y[size_t(n) * Np + k];
                     if (tid == 0) {
-                        yw[2 * qn] = jb.y[2 * n];
-                        yw[2 * qn + 1] = jb.y[2 * n + 1];
+                        yw[2 * qn] = js.y[2 * n];
+                        yw[2 * qn + 1] = js.y[2 * n + 1];
                         aw[2 * qn] = aw[2 * qn + 1] = 0.f;
-                        nw[qn] = jb.nrm[n];
+                        rd[qn] = 1.f / fmaf(wL, js.nrm[n], wG);
+                        fill_diag(qn, js.nrm[n]);
                     }
                 }
             }
             __syncthreads();
 
             // ================= phase 2 =================
-            // (2a) window update partials and w-update partials
-            {
-                const int n_h = ncp * kParts, n_w = 2 * D;
-                for (int idx = tid; idx < n_h + n_w; idx += kThreads) {
-                    if (idx < n_h) {
-                        const int cp = idx % ncp, part = idx / ncp;
-                        const int p0 = part * Lp, p1 = min(XSP, p0 + Lp);
-                        float h00 = 0.f, h01 = 0.f, h10 = 0.f, h11 = 0.f;
-                        for (int p = p0; p < p1; ++p) {
-                            const float2 c = *reinterpret_cast<const float2*>(cs + 2 * p);
-                            const float2 A = *reinterpret_cast<const float2*>(KA + p * XSPp + 2 * cp);
-                            const float2 Bp = *reinterpret_cast<const float2*>(KP + p * XSPp + 2 * cp);
-                            const float2 Bm = *reinterpret_cast<const float2*>(KM + p * XSPp + 2 * cp);
-                            h00 = fmaf(c.x, A.x, fmaf(c.y, Bm.x, h00));
-                            h01 = fmaf(c.x, Bp.x, fmaf(c.y, A.x, h01));
-                            h10 = fmaf(c.x, A.y, fmaf(c.y, Bm.y, h10));
-                            h11 = fmaf(c.x, Bp.y, fmaf(c.y, A.y, h11));
-                        }
-                        *reinterpret_cast<float4*>(red + part * 2 * XSPp + 4 * cp) = make_float4(h00, h01, h10, h11);
-                    } else {
-                        const int u = idx - n_h, half = u / D, d = u % D, k = d % N;
-                        const int p0 = half * halfP, p1 = min(XSP, p0 + halfP);
-                        float acc = 0.f;
-                        for (int p = p0; p < p1; ++p) {
-                            const float2 c = *reinterpret_cast<const float2*>(cs + 2 * p);
-                            const float2 v = Yw[p * Np + k];
-                            acc = d < N ? fmaf(c.x, v.x, fmaf(c.y, v.y, acc)) : fmaf(c.x, v.y, fmaf(-c.y, v.x, acc));
-                        }
-                        wred[half * kMaxFeatures + d] = acc;
-                    }
+            // (2a) window update partials: red[part][row] = sum_{p in part} c_p Kt(p, .)
+            for (int idx = tid; idx < ncp * kParts; idx += kThreads) {
+                const int cp = idx % ncp, part = idx / ncp;
+                const int p0 = part * Lp, p1 = min(XSP, p0 + Lp);
+                float h00 = 0.f, h01 = 0.f, h10 = 0.f, h11 = 0.f;
+                const float* pa = KA + 2 * cp;
+                const float* pp = KP + 2 * cp;
+                const float* pm = KM + 2 * cp;
+#pragma unroll 2
+                for (int p = p0; p < p1; ++p) {
+                    const float2 c = *reinterpret_cast<const float2*>(cs + 2 * p);
+                    const float2 A = *reinterpret_cast<const float2*>(pa + p * XSPp);
+                    const float2 Bp = *reinterpret_cast<const float2*>(pp + p * XSPp);
+                    const float2 Bm = *reinterpret_cast<const float2*>(pm + p * XSPp);
+                    h00 = fmaf(c.x, A.x, fmaf(c.y, Bm.x, h00));
+                    h01 = fmaf(c.x, Bp.x, fmaf(c.y, A.x, h01));
+                    h10 = fmaf(c.x, A.y, fmaf(c.y, Bm.y, h10));
+                    h11 = fmaf(c.x, Bp.y, fmaf(c.y, A.y, h11));
                 }
+                *reinterpret_cast<float4*>(red + part * 2 * XSPp + 4 * cp) = make_float4(h00, h01, h10, h11);
             }
             // (2b) coefficients of the active rows (apsm_train.cu:407)
             for (int r = tid; r < 2 * XSP; r += kThreads) {
-                const int p = pair_in(r >> 1, pc.sP);
-                if (p < pc.hiP && p - pc.sP < pc.nAP) {
+                int d = (r >> 1) - los;
+                if (d < 0) d += XSP;
+                if (d < pc.nAP) {
                     const float v = __fadd_rn(aw[r], cs[r]);
                     aw[r] = v;
-                    ag[2 * p + (r & 1)] = v;
+                    ag[2 * (pc.sP + d) + (r & 1)] = v;
                 }
             }
-            // (2c) entering pairs: predictions start from the reduced partial sums
-            for (int i = tid; i < 2 * min(ne, kMaxEnter); i += kThreads) {
-                const int e = i >> 1, row = i & 1;
-                float s = 0.f;
-                for (int w2 = 0; w2 < kWarps; ++w2) s += wp[(e * kWarps + w2) * 2 + row];
-                hw[2 * slot_of(e_lo + e) + row] = s;
-            }
-            // (2d) evicted pairs leave the sums of the rows that stay in the window
-            if (has_next && pn.loP > pc.loP) {
-                for (int r = tid; r < 2 * XSP; r += kThreads) {
-                    const int p = pair_in(r >> 1, pn.sP);
+            // (2c) evicted pairs: dr = sum a_b x_b joins r; their Gaussian terms leave the rows that stay
+            const bool evict = has_next && pn.loP > pc.loP;
+            if (evict) {
+                for (int d = tid; d < kMaxFeatures; d += kThreads) {
+                    const float v = d < D ? ax_sum(d, pc.loP, pn.loP) : 0.f;
+                    dr[d] = v;
+                    r_s[d] += v;
+                }
+                const int lons = pn.sP % XSP;
+                for (int q = tid; q < XSP; q += kThreads) {
+                    int dd = q - lons;
+                    if (dd < 0) dd += XSP;
+                    const int p = pn.sP + dd;
                     if (p >= pc.hiP) continue;
                     const float4* col = col_ptr(p);
                     float g0 = 0.f, g1 = 0.f;
-                    for (int b = pc.loP; b < pn.loP; ++b)
-                        acc_pair(*reinterpret_cast<const float2*>(ag + 2 * b), col[b], g0, g1);
-                    hw[r] -= (r & 1) ? g1 : g0;
+                    for (int b = pc.loP; b < pn.loP; ++b) {
+                        float re = 0.f, im = 0.f;
+                        for (int k = 0; k < N; ++k) {
+                            const float2 yb = Y[size_t(b) * Np + k], yj = Yw[q * Np + k];
+                            re = fmaf(yb.x, yj.x, fmaf(yb.y, yj.y, re));
+                            im = fmaf(yb.x, yj.y, fmaf(-yb.y, yj.x, im));
+                        }
+                        const float4 kt = col[b]; // Kt = K + wL <x_b, x_p>: subtract the linear part
+                        const float4 kg = make_float4(fmaf(-wL, re, kt.x), fmaf(-wL, im, kt.y), fmaf(wL, im, kt.z), 0.f);
+                        acc_pair(*reinterpret_cast<const float2*>(ag + 2 * b), kg, g0, g1);
+                    }
+                    hw[2 * q] -= g0;
+                    hw[2 * q + 1] -= g1;
                 }
+                __syncthreads();
             }
-            // (2e) prefetch for the pair entering at t+2
-            prefetch(t + 2, pc.sP);
-            if (t + 2 < n_steps) s_nxt = jb.steps[t + 2];
+            // (2d) entering pairs: predictions start from the reduced partial sums (plus wL <x_n, dr>
+            //      after an eviction: their partial sums used r from before it)
+            for (int i = tid; i < 2 * min(ne, kMaxEnter); i += kThreads) {
+                const int e = i >> 1, row = i & 1, qn = (e_lo + e) % XSP;
+                float s = 0.f;
+                for (int w2 = 0; w2 < kWarps; ++w2) s += wp[(e * kWarps + w2) * 2 + row];
+                if (evict) {
+                    float l = 0.f;
+                    for (int k = 0; k < N; ++k) {
+                        const float2 v = Yw[qn * Np + k];
+                        l = row == 0 ? fmaf(dr[k], v.x, fmaf(dr[N + k], v.y, l)) : fmaf(dr[k], v.y, fmaf(-dr[N + k], v.x, l));
+                    }
+                    s = fmaf(wL, l, s);
+                }
+                hw[2 * qn + row] = s;
+            }
+            // (2e) pipeline: frozen part of the pair entering at t+2, loads for t+3
+            advance();
+            issue(t + 3, st_3, st_nn, pc.sP);
+            los += pn.sP - pc.sP;
+            if (los >= XSP) los -= XSP;
             pc = pn;
+            st_n = st_nn;
+            st_nn = st_3;
+            st_3 = st_4;
             __syncthreads();
         }
-        // final linear weights
-        if (tid < D) jb.w[tid] = w_s[tid] + (wred[tid] + wred[kMaxFeatures + tid]);
+        // w = r + sum over the visible pairs of a_b x_b
+        for (int d = tid; d < D; d += kThreads) js.w[d] = r_s[d] + ax_sum(d, pc.loP, pc.hiP);
     }
 }
 
@@ -394,7 +462,7 @@ int batch_sweep_threads() { return kThreads; }
 size_t batch_sweep_smem(const BatchCommon& cm)
 {
     const size_t f = 3 * size_t(cm.XSP) * cm.XSPp + 2 * size_t(cm.XSP) * cm.Np + 8 * size_t(cm.XSPp) + cm.XSPp +
-                     size_t(kParts) * 2 * cm.XSPp + 3 * kMaxFeatures + 2 * kMaxEnter * kWarps;
+                     size_t(kParts) * 2 * cm.XSPp + 2 * kMaxFeatures + 2 * kMaxEnter * kWarps;
     return sizeof(float) * f;
 }
 

@@ -29,22 +29,25 @@ from .detector import ApsmError
 
 JOB_TRAIN = 0
 JOB_DETECT = 1
+JOB_FRESH = 1  # train-job flag: resetState before training
 
 
 class _CJob(ctypes.Structure):
     _fields_ = [("detector", ctypes.c_uint32), ("kind", ctypes.c_uint32), ("length", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32), ("rx", ctypes.c_void_p), ("tx", ctypes.c_void_p),
+                ("flags", ctypes.c_uint32), ("rx", ctypes.c_void_p), ("tx", ctypes.c_void_p),
                 ("est", ctypes.c_void_p)]
 
 
 @dataclass
 class PoolJob:
-    """One train (tx given) or detect (tx None) call of one pool detector."""
+    """One train (tx given) or detect (tx None) call of one pool detector;
+    fresh=True resets the detector before a train job."""
 
     detector: int
     rx: Any
     tx: Any = None
     est: Any = None
+    fresh: bool = False
 
     @property
     def kind(self) -> int:
@@ -139,7 +142,7 @@ class DetectorPool:
                     if j.est is None or np.asarray(j.est).shape != (length,) or j.est.dtype != np.complex64:
                         j.est = np.zeros(length, np.complex64)
                     estp = j.est.ctypes.data
-            arr[i] = _CJob(int(j.detector), j.kind, length, 0, rxp, txp, estp)
+            arr[i] = _CJob(int(j.detector), j.kind, length, JOB_FRESH if j.fresh else 0, rxp, txp, estp)
         return arr, keep
 
     def run(self, jobs: Sequence[PoolJob], lane: int = 0) -> list[np.ndarray | None]:

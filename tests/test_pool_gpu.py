@@ -178,3 +178,19 @@ def test_pool_budget_admission(native_lib):
     with pytest.raises(ApsmError, match="OUT_OF_MEMORY"):
         pool.run([job])
     assert pool.bytes_in_use <= pool.budget
+
+
+def test_pool_fresh_flag_is_reset_then_train(native_lib):
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    pool = DetectorPool(CFG)
+    d = pool.add(8)
+    rx, tx, rxd = _frame(9, 8, 120, 64)
+    pool.run([PoolJob(d, rx, tx)])
+    (ref,) = pool.run([PoolJob(d, rxd)])
+    for _ in range(2):  # trained state present: fresh discards it
+        out = pool.run([PoolJob(d, rx, tx, fresh=True), PoolJob(d, rxd)])
+        assert np.array_equal(out[1], ref)
+    empty = np.zeros((8, 0), np.complex64)
+    (est,) = pool.run([PoolJob(d, empty, np.zeros(0, np.complex64), fresh=True), PoolJob(d, rxd)])[1:]
+    assert np.all(est == 0)
