@@ -34,7 +34,8 @@ typedef enum {
     APSM_ERR_CUDA = 3,             /* CUDA runtime error (reference: CUDA_CHECK prints and exits, cuda_errorhandling.cuh:98-108) */
     APSM_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed or would exceed the handle's memory budget */
     APSM_ERR_UNSUPPORTED = 5,      /* valid config the B200 kernels do not implement (e.g. antenna count above the maximum) */
-    APSM_ERR_NO_DEVICE = 6         /* no usable sm_100 device */
+    APSM_ERR_NO_DEVICE = 6,        /* no usable sm_100 device */
+    APSM_ERR_TIMEOUT = 7           /* a host-side wait ran out of time */
 } apsm_status;
 
 typedef struct apsm_detector apsm_detector;
@@ -167,16 +168,24 @@ apsm_status apsm_pool_add(apsm_pool* p, uint32_t num_antennas, uint32_t* detecto
 apsm_status apsm_pool_remove(apsm_pool* p, uint32_t detector);
 apsm_status apsm_pool_reset(apsm_pool* p, uint32_t detector);
 
+/* Run modes of apsm_pool_run. */
+#define APSM_RUN_HOST 0       /* host buffers; returns when the estimates are written */
+#define APSM_RUN_DEVICE 1     /* device buffers; returns once enqueued on the lane's stream */
+#define APSM_RUN_HOST_ASYNC 2 /* host buffers; returns once enqueued, estimates arrive with apsm_pool_wait */
+
 /* Runs a batch on a lane: all training jobs first (in one sweep launch; a
  * detector may be trained at most once per batch), then all detection jobs,
- * which see this batch's training.  device_buffers != 0: rx/tx/est are device
- * pointers and the call returns once the work is enqueued on the lane's
- * stream (apsm_pool_wait / apsm_pool_query); otherwise host buffers, staged
- * through the lane and the call returns when the estimates are written.  A
- * detector must not be in batches on two lanes at once. */
-apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs, int device_buffers);
+ * which see this batch's training.  Host modes stage every input through one
+ * pinned buffer (one host-to-device copy with the job descriptors) and bring
+ * every estimate back in one device-to-host copy; the caller keeps its
+ * buffers alive until the batch finished.  A detector must not be in batches
+ * on two lanes at once. */
+apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs, int mode);
+/* Waits for the lane's last batch and, for APSM_RUN_HOST_ASYNC, writes its
+ * estimates to the caller's buffers. */
 apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane);
-/* 1 when the lane is idle, 0 while its last batch runs, < 0 on error. */
+/* 1 when the lane's GPU work finished (call apsm_pool_wait for the estimates
+ * of an asynchronous host batch), 0 while it runs, < 0 on error. */
 int apsm_pool_query(apsm_pool* p, uint32_t lane);
 void* apsm_pool_stream(apsm_pool* p, uint32_t lane);
 
@@ -190,9 +199,45 @@ uint64_t apsm_pool_bytes_in_use(const apsm_pool* p);
  * columns + sweep) and detection stages; blocks until the batch finished. */
 apsm_status apsm_pool_last_ms(apsm_pool* p, uint32_t lane, float* train_ms, float* detect_ms);
 
+/* Kernels the lane's last batch launched (its own kernels; memsets and copies excluded). */
+int apsm_pool_last_launches(apsm_pool* p, uint32_t lane);
+
 /* Snapshot of a detector: rows in use, a (rows), w (2N); pointers may be NULL. */
 apsm_status apsm_pool_get_state(apsm_pool* p, uint32_t detector, uint32_t* rows, float* a, float* w);
 const char* apsm_pool_last_error(const apsm_pool* p);
+
+/* ======================================================================
+ * Request server: continuous batching of per-TTI requests over a pool.
+ *
+ * No counterpart in the reference (its CLI processes one frame per detector
+ * and thread, noma_detect.cpp:100-137).  A worker thread admits waiting
+ * requests into batches on the pool's first `lanes` lanes as they become
+ * free: per detector, requests keep their arrival order and a detector with
+ * a batch in flight waits; a batch is bounded by max_batch requests and by
+ * the device scratch the pool's HBM budget leaves per lane.  Batches on
+ * different lanes overlap on the GPU.  Every request is one apsm_job with
+ * host buffers that stay valid until the request finished.  A request's
+ * result is the same whichever requests share its batch.  The pool must not
+ * be used directly while a server runs on it.
+ * ==================================================================== */
+typedef struct apsm_server apsm_server;
+
+apsm_status apsm_server_create(apsm_pool* pool, uint32_t lanes, uint32_t max_batch, apsm_server** out);
+/* Finishes every submitted request, then stops the worker. */
+void apsm_server_destroy(apsm_server* s);
+apsm_status apsm_server_submit(apsm_server* s, const apsm_job* job, uint64_t* ticket);
+/* 1 when the request finished (*status its result), 0 while pending, -1 unknown ticket. */
+int apsm_server_poll(apsm_server* s, uint64_t ticket, apsm_status* status);
+/* Blocks until the request finished (its status) or timeout_s passed (APSM_ERR_TIMEOUT). */
+apsm_status apsm_server_wait(apsm_server* s, uint64_t ticket, double timeout_s);
+/* Host times (seconds, apsm_server_clock) of submission, admission into a batch, completion. */
+apsm_status apsm_server_times(apsm_server* s, uint64_t ticket, double* submit_s, double* start_s, double* done_s);
+/* Forget a finished request. */
+apsm_status apsm_server_release(apsm_server* s, uint64_t ticket);
+/* Batches launched and requests they held. */
+apsm_status apsm_server_stats(apsm_server* s, uint64_t* batches, uint64_t* jobs);
+/* The monotonic clock of the request times, in seconds. */
+double apsm_server_clock(void);
 
 #ifdef __cplusplus
 }

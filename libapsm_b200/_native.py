@@ -19,6 +19,7 @@ APSM_ERR_CUDA = 3
 APSM_ERR_OUT_OF_MEMORY = 4
 APSM_ERR_UNSUPPORTED = 5
 APSM_ERR_NO_DEVICE = 6
+APSM_ERR_TIMEOUT = 7
 
 STATUS_NAMES = {
     APSM_OK: "APSM_OK",
@@ -28,6 +29,7 @@ STATUS_NAMES = {
     APSM_ERR_OUT_OF_MEMORY: "APSM_ERR_OUT_OF_MEMORY",
     APSM_ERR_UNSUPPORTED: "APSM_ERR_UNSUPPORTED",
     APSM_ERR_NO_DEVICE: "APSM_ERR_NO_DEVICE",
+    APSM_ERR_TIMEOUT: "APSM_ERR_TIMEOUT",
 }
 
 # (name, restype, argtypes) of every exported entry point
@@ -66,6 +68,18 @@ SIGNATURES = [
     ("apsm_pool_last_ms", ctypes.c_int, [_P, _U32, _F, _F]),
     ("apsm_pool_get_state", ctypes.c_int, [_P, _U32, ctypes.POINTER(_U32), _P, _P]),
     ("apsm_pool_last_error", ctypes.c_char_p, [_P]),
+    ("apsm_pool_last_launches", ctypes.c_int, [_P, _U32]),
+    # request server (continuous batching over a pool)
+    ("apsm_server_create", ctypes.c_int, [_P, _U32, _U32, ctypes.POINTER(_P)]),
+    ("apsm_server_destroy", None, [_P]),
+    ("apsm_server_submit", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    ("apsm_server_poll", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]),
+    ("apsm_server_wait", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_double]),
+    ("apsm_server_times", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("apsm_server_release", ctypes.c_int, [_P, ctypes.c_uint64]),
+    ("apsm_server_stats", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    ("apsm_server_clock", ctypes.c_double, []),
 ]
 
 _lib = None

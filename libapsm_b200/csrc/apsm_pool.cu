@@ -47,9 +47,17 @@ struct Lane {
     bool have_train = false, have_detect = false;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
-    void* pinned = nullptr;
+    void* pinned = nullptr; // descriptors and staged host inputs of a batch (one H2D copy)
     size_t pinned_bytes = 0;
-    int* err = nullptr; // error flag of the last batch (in the scratch)
+    void* pinned_out = nullptr; // estimates of a host-buffer batch (one D2H copy)
+    size_t pinned_out_bytes = 0;
+    struct CopyOut {
+        void* dst;
+        size_t off, bytes;
+    };
+    std::vector<CopyOut> pending; // estimates to hand to the caller once the batch finished
+    int* err = nullptr;           // error flag of the last batch (in the scratch)
+    int launches = 0;             // kernels launched by the last batch
 };
 
 int detect_class(uint32_t N)
@@ -93,8 +101,9 @@ struct apsm_pool {
     }
     size_t train_bytes(const PoolDet& d, uint32_t P, bool host) const;
     size_t detect_bytes(const PoolDet& d, uint32_t S, bool host) const;
-    apsm_status run(uint32_t lane, const apsm_job* jobs, uint32_t n, bool device_buffers);
+    apsm_status run(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode);
     apsm_status check_lane(uint32_t lane);
+    apsm_status finish(uint32_t lane); // wait for the lane, hand out estimates, check its error flag
 };
 
 #define POOL_CK(call)                                                                  \
@@ -109,6 +118,7 @@ apsm_pool::~apsm_pool()
         if (l.stream) cudaStreamSynchronize(l.stream);
         if (l.scratch) cudaFree(l.scratch);
         if (l.pinned) cudaFreeHost(l.pinned);
+        if (l.pinned_out) cudaFreeHost(l.pinned_out);
         for (auto& e : l.ev)
             if (e) cudaEventDestroy(e);
         if (l.done) cudaEventDestroy(l.done);
@@ -194,11 +204,15 @@ size_t apsm_pool::detect_bytes(const PoolDet& d, uint32_t S, bool host) const
     return b + sizeof(BatchDetectJob) + sizeof(BatchPackJob);
 }
 
-apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, bool device_buffers)
+apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, int mode)
 {
     apsm_pool* p = this;
     Lane& L = lanes[lane_id];
-    const bool host = !device_buffers;
+    const bool host = mode != APSM_RUN_DEVICE;
+    if (!L.pending.empty()) {
+        apsm_status st = finish(lane_id); // the lane's previous host batch
+        if (st != APSM_OK) return st;
+    }
     const uint32_t cap = 2 * cfg.dict_size;
 
     // ---------- validate ----------
@@ -321,14 +335,21 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
             t.perm_off = perm_off[t.P];
         }
     o = align_up(o, 256);
-    const size_t desc_bytes = o;
+    if (host) { // staged host inputs travel with the descriptors
+        for (auto& t : tp) {
+            t.off_rx = o; o = align_up(o + sizeof(float2) * size_t(t.det->N) * t.P, 16);
+            t.off_tx = o; o = align_up(o + sizeof(float2) * t.P, 16);
+        }
+        for (auto& d : dp) {
+            d.off_rx = o;
+            o = align_up(o + sizeof(float2) * size_t(d.det->N) * d.S, 16);
+        }
+        o = align_up(o, 256);
+    }
+    const size_t desc_bytes = o; // bytes of the one host-to-device copy
     const size_t off_counter = o; o = align_up(o + 256, 256); // sweep job counter, error flag
     for (auto& t : tp) {
         const PoolDet& d = *t.det;
-        if (host) {
-            t.off_rx = o; o = align_up(o + sizeof(float2) * size_t(d.N) * t.P, 256);
-            t.off_tx = o; o = align_up(o + sizeof(float2) * t.P, 256);
-        }
         t.off_Y = o; o = align_up(o + sizeof(float2) * size_t(t.nP) * d.Np, 256);
         t.off_nrm = o; o = align_up(o + sizeof(float) * t.nP, 256);
         t.off_y = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
@@ -336,10 +357,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         t.off_kc = o; o = align_up(o + sizeof(float4) * size_t(std::max<long long>(t.n_kc, 1)), 256);
     }
     for (auto& d : dp) {
-        if (host) {
-            d.off_rx = o; o = align_up(o + sizeof(float2) * size_t(d.det->N) * d.S, 256);
-            d.off_est = o; o = align_up(o + sizeof(float2) * d.S, 256);
-        }
         d.off_Y = o; o = align_up(o + sizeof(float2) * size_t(d.S) * d.det->Np, 256);
         d.off_nrm = o; o = align_up(o + sizeof(float) * d.S, 256);
         if (d.gram) {
@@ -349,6 +366,14 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
             d.off_lin = o; o = align_up(o + sizeof(float2) * d.S, 256);
         }
     }
+    const size_t est_begin = o;
+    if (host)
+        for (auto& d : dp) {
+            d.off_est = o;
+            o = align_up(o + sizeof(float2) * d.S, 16);
+        }
+    const size_t est_bytes = o - est_begin;
+    o = align_up(o, 256);
     const size_t scratch_need = o;
 
     // ---------- memory ----------
@@ -370,8 +395,18 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
         if (L.pinned) POOL_CK(cudaFreeHost(L.pinned));
         L.pinned = nullptr;
         L.pinned_bytes = 0;
-        POOL_CK(cudaMallocHost(&L.pinned, std::max<size_t>(desc_bytes, 1 << 16)));
-        L.pinned_bytes = std::max<size_t>(desc_bytes, 1 << 16);
+        const size_t want = std::max<size_t>(desc_bytes + desc_bytes / 2, 1 << 16);
+        POOL_CK(cudaMallocHost(&L.pinned, want));
+        L.pinned_bytes = want;
+    }
+    if (est_bytes > L.pinned_out_bytes) {
+        POOL_CK(cudaStreamSynchronize(L.stream));
+        if (L.pinned_out) POOL_CK(cudaFreeHost(L.pinned_out));
+        L.pinned_out = nullptr;
+        L.pinned_out_bytes = 0;
+        const size_t want = std::max<size_t>(est_bytes + est_bytes / 2, 1 << 16);
+        POOL_CK(cudaMallocHost(&L.pinned_out, want));
+        L.pinned_out_bytes = want;
     }
     POOL_CK(cudaEventSynchronize(L.desc_copied)); // the previous batch's descriptors were consumed
     char* dev = static_cast<char*>(L.scratch);
@@ -497,12 +532,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
     if (host) {
         for (const auto& t : tp) {
             const apsm_job& j = jobs[t.job];
-            POOL_CK(cudaMemcpyAsync(D(t.off_rx), j.rx, sizeof(float2) * size_t(t.det->N) * t.P, cudaMemcpyHostToDevice, s));
-            POOL_CK(cudaMemcpyAsync(D(t.off_tx), j.tx, sizeof(float2) * t.P, cudaMemcpyHostToDevice, s));
+            std::memcpy(hst + t.off_rx, j.rx, sizeof(float2) * size_t(t.det->N) * t.P);
+            std::memcpy(hst + t.off_tx, j.tx, sizeof(float2) * t.P);
         }
-        for (const auto& q : dp)
-            POOL_CK(cudaMemcpyAsync(D(q.off_rx), jobs[q.job].rx, sizeof(float2) * size_t(q.det->N) * q.S,
-                                    cudaMemcpyHostToDevice, s));
+        for (const auto& q : dp) std::memcpy(hst + q.off_rx, jobs[q.job].rx, sizeof(float2) * size_t(q.det->N) * q.S);
     }
     POOL_CK(cudaMemcpyAsync(dev, hst, desc_bytes, cudaMemcpyHostToDevice, s));
     POOL_CK(cudaEventRecord(L.desc_copied, s));
@@ -516,17 +549,23 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
     int* d_err = d_counter + 4;
     POOL_CK(cudaMemsetAsync(d_counter, 0, 32, s));
     L.err = d_err;
+    L.launches = 0;
     if (nT > 0) {
         POOL_CK(cudaEventRecord(L.ev[0], s));
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_ci)), int(nCopyIn), max_pairs_in, max_np, s));
+        L.launches += nCopyIn > 0 && max_pairs_in > 0;
     }
-    if (nPack > 0) POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)), int(nPack), max_len, max_n, s));
+    if (nPack > 0) {
+        POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)), int(nPack), max_len, max_n, s));
+        L.launches += max_len > 0;
+    }
     if (nT > 0) {
         const auto* d_tj = reinterpret_cast<const BatchTrainJob*>(D(off_tj));
         POOL_CK(launch_batch_kcol(d_tj, int(nT), max_cols, max_n, cm, s));
         const int grid = int(std::min<size_t>(nT, size_t(sweep_ctas) * sms));
         POOL_CK(launch_batch_sweep(d_tj, int(nT), cm, grid, d_counter, d_err, s));
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_co)), int(nT), max_pairs_out, max_np, s));
+        L.launches += (max_cols > 0) + 1 + (max_pairs_out > 0);
         POOL_CK(cudaEventRecord(L.ev[1], s));
         for (const auto& t : tp) t.det->used = 2 * t.usedP_new;
     }
@@ -543,6 +582,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
                 ++k1;
             }
             POOL_CK(launch_batch_detect(d_dj + k0, int(k1 - k0), tiles, dp[k0].cls, cfg.wL, cfg.wG, s));
+            L.launches += tiles > 0;
             k0 = k1;
         }
         const auto* d_gj = reinterpret_cast<const BatchGramJob*>(D(off_gj));
@@ -551,18 +591,27 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, b
             const size_t base = size_t(g[0]) - nC;
             POOL_CK(launch_batch_gram(d_gj + base, g[1] - g[0], g[4], g[5], d_gp + g[2], g[3], dp[g[0]].cls, cfg.wL,
                                       cfg.wG, d_err, s));
+            L.launches += (g[4] > 0) + (g[5] > 0) + (g[3] > 0);
         }
         POOL_CK(cudaEventRecord(L.ev[3], s));
-        if (host)
-            for (const auto& q : dp)
-                POOL_CK(cudaMemcpyAsync(jobs[q.job].est, D(q.off_est), sizeof(float2) * q.S, cudaMemcpyDeviceToHost, s));
+        if (host && est_bytes > 0) {
+            POOL_CK(cudaMemcpyAsync(L.pinned_out, D(est_begin), est_bytes, cudaMemcpyDeviceToHost, s));
+            for (const auto& q : dp) L.pending.push_back({jobs[q.job].est, q.off_est - est_begin, sizeof(float2) * q.S});
+        }
     }
     POOL_CK(cudaEventRecord(L.done, s));
-    if (host) {
-        POOL_CK(cudaStreamSynchronize(s));
-        return check_lane(lane_id);
-    }
+    if (mode == APSM_RUN_HOST) return finish(lane_id);
     return APSM_OK;
+}
+
+apsm_status apsm_pool::finish(uint32_t lane_id)
+{
+    apsm_pool* p = this;
+    Lane& L = lanes[lane_id];
+    POOL_CK(cudaEventSynchronize(L.done));
+    for (const auto& c : L.pending) std::memcpy(c.dst, static_cast<char*>(L.pinned_out) + c.off, c.bytes);
+    L.pending.clear();
+    return check_lane(lane_id);
 }
 
 apsm_status apsm_pool::check_lane(uint32_t lane_id)
@@ -761,15 +810,15 @@ extern "C" apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job
     std::lock_guard<std::mutex> g(p->mu);
     if (lane >= p->lanes.size()) return p->fail(APSM_ERR_INVALID_ARGUMENT, "lane out of range");
     if (n_jobs > 0 && !jobs) return p->fail(APSM_ERR_INVALID_ARGUMENT, "null job list");
-    return p->run(lane, jobs, n_jobs, device_buffers != 0);
+    if (device_buffers < 0 || device_buffers > 2) return p->fail(APSM_ERR_INVALID_ARGUMENT, "unknown run mode");
+    return p->run(lane, jobs, n_jobs, device_buffers);
 }
 
 extern "C" apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane)
 {
     if (!p || lane >= p->lanes.size()) return APSM_ERR_INVALID_ARGUMENT;
-    cudaError_t e = cudaEventSynchronize(p->lanes[lane].done);
-    if (e != cudaSuccess) return p->cuda_fail(e, "cudaEventSynchronize");
-    return p->check_lane(lane);
+    std::lock_guard<std::mutex> g(p->mu);
+    return p->finish(lane);
 }
 
 extern "C" int apsm_pool_query(apsm_pool* p, uint32_t lane)
@@ -838,4 +887,10 @@ extern "C" apsm_status apsm_pool_get_state(apsm_pool* p, uint32_t detector, uint
         if (e != cudaSuccess) return p->cuda_fail(e, "cudaMemcpy(w)");
     }
     return APSM_OK;
+}
+
+extern "C" int apsm_pool_last_launches(apsm_pool* p, uint32_t lane)
+{
+    if (!p || lane >= p->lanes.size()) return -1;
+    return p->lanes[lane].launches;
 }

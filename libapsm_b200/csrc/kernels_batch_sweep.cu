@@ -40,6 +40,8 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kPf = 8;        // frozen column entries per thread: up to kThreads * kPf pairs per column
 constexpr int kParts = 6;     // row-slot parts of the window update
 constexpr int kMaxEnter = 4;  // pairs entering per step (sampleStep <= 8)
+constexpr int kRowThreads = 192;              // warps 0-5: the window rows' corrections
+constexpr int kEntThreads = kThreads - kRowThreads; // warps 6-7: the entering pair (window part, linear term)
 
 struct PairStep {
     int hiP, sP, nAP, loP, wk;
@@ -115,7 +117,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     float* red = rd + XSPp;                                  // [kParts][2 XSPp] window-update partials
     float* r_s = red + kParts * 2 * XSPp;                    // [kMaxFeatures] residual weights r
     float* dr = r_s + kMaxFeatures;                          // [kMaxFeatures] r increment of an eviction
-    float* wp = dr + kMaxFeatures;                           // [kMaxEnter][kWarps][2] entering partial sums
+    float* wp = dr + kMaxFeatures;                           // [kMaxEnter][kWarps][2] entering partial sums (direct loads)
+    float* wpf = wp + 2 * kMaxEnter * kWarps;                // [2][kWarps][2] frozen partial sums by step parity
+    float* wpe = wpf + 4 * kWarps;                           // [2][2] window part + linear term (warps 6-7)
 
     for (;;) {
         __syncthreads();
@@ -202,8 +206,9 @@ __global__ void __launch_bounds__(kThreads, 2)
                 for (int k = lane; k < Np; k += 32) Yw[q * Np + k] = Y[size_t(j) * Np + k];
                 float g0 = 0.f, g1 = 0.f;
                 const float4* col = col_ptr(j);
+#pragma unroll 8
                 for (int b = pc.loP + lane; b < top; b += 32)
-                    acc_pair(*reinterpret_cast<const float2*>(ag + 2 * b), col[b], g0, g1);
+                    acc_pair(*reinterpret_cast<const float2*>(ag + 2 * b), __ldg(col + b), g0, g1);
                 for (int d = lane; d < D; d += 32) lin_feature(d, r_s[d], Y[size_t(j) * Np + d % N], g0, g1);
                 warp_sum2(g0, g1);
                 if (lane == 0) {
@@ -223,8 +228,9 @@ __global__ void __launch_bounds__(kThreads, 2)
         Entry e_cur{-1, 0, 0, 0, 0}, e_nxt{-1, 0, 0, 0, 0};
         float4 colbuf[kPf];
         float2 abuf[kPf];
-        float4 win_cur = make_float4(0.f, 0.f, 0.f, 0.f), win_nxt = win_cur;
-        float2 y_cur = make_float2(0.f, 0.f), y_nxt = y_cur;
+        const int et = tid - kRowThreads; // index among the entering warps' threads (< 0: row warps)
+        float4 win_cur0 = make_float4(0.f, 0.f, 0.f, 0.f), win_cur1 = win_cur0, win_nxt0 = win_cur0, win_nxt1 = win_cur0;
+        float2 y_cur0 = make_float2(0.f, 0.f), y_cur1 = y_cur0, y_nxt0 = y_cur0, y_nxt1 = y_cur0;
         float t_cur0 = 0.f, t_cur1 = 0.f, n_cur = 0.f, t_nxt0 = 0.f, t_nxt1 = 0.f, n_nxt = 0.f;
         float gf0 = 0.f, gf1 = 0.f; // this thread's part of the frozen sum of e_cur
         // stage 1: loads for the pair entering at step tt (frozen boundary F)
@@ -239,7 +245,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             e_nxt.lo = ps.loP;
             e_nxt.top = pv.hiP;
             e_nxt.F = min(max(F, e_nxt.lo), e_nxt.top);
-            if (ne != 1 || e_nxt.F - e_nxt.lo > kThreads * kPf || e_nxt.top - e_nxt.F > kThreads || D > kThreads) {
+            if (ne != 1 || e_nxt.F - e_nxt.lo > kThreads * kPf || e_nxt.top - e_nxt.F > 2 * kEntThreads ||
+                D > 2 * kEntThreads) {
                 e_nxt.slow = 1;
                 return;
             }
@@ -252,31 +259,42 @@ __global__ void __launch_bounds__(kThreads, 2)
                 colbuf[k] = ok ? __ldg(col + b) : make_float4(0.f, 0.f, 0.f, 0.f);
                 abuf[k] = ok ? *reinterpret_cast<const float2*>(ag + 2 * b) : make_float2(0.f, 0.f);
             }
-            const int bw = e_nxt.F + tid;
-            win_nxt = bw < e_nxt.top ? __ldg(col + bw) : make_float4(0.f, 0.f, 0.f, 0.f);
-            if (tid < D) y_nxt = Y[size_t(n) * Np + tid % N];
-            if (tid == 0) {
+            if (et >= 0) {
+                const int b0 = e_nxt.F + et, b1 = b0 + kEntThreads;
+                win_nxt0 = b0 < e_nxt.top ? __ldg(col + b0) : make_float4(0.f, 0.f, 0.f, 0.f);
+                win_nxt1 = b1 < e_nxt.top ? __ldg(col + b1) : make_float4(0.f, 0.f, 0.f, 0.f);
+                if (et < D) y_nxt0 = Y[size_t(n) * Np + et % N];
+                if (et + kEntThreads < D) y_nxt1 = Y[size_t(n) * Np + (et + kEntThreads) % N];
+            }
+            if (et == 0) {
                 t_nxt0 = js.y[2 * n];
                 t_nxt1 = js.y[2 * n + 1];
                 n_nxt = js.nrm[n];
             }
         };
-        // stage 2: this thread's share of the frozen sum of e_nxt, then e_nxt becomes e_cur
-        auto advance = [&]() {
+        // stage 2: the frozen sum of e_nxt (per-warp partials into wpf[buf]), then e_nxt becomes e_cur
+        auto advance = [&](int buf) {
             gf0 = gf1 = 0.f;
             if (e_nxt.n >= 0 && !e_nxt.slow) {
 #pragma unroll
                 for (int k = 0; k < kPf; ++k) acc_pair(abuf[k], colbuf[k], gf0, gf1);
+                warp_sum2(gf0, gf1);
+                if (lane == 0) {
+                    wpf[(buf * kWarps + warp) * 2] = gf0;
+                    wpf[(buf * kWarps + warp) * 2 + 1] = gf1;
+                }
             }
             e_cur = e_nxt;
-            win_cur = win_nxt;
-            y_cur = y_nxt;
+            win_cur0 = win_nxt0;
+            win_cur1 = win_nxt1;
+            y_cur0 = y_nxt0;
+            y_cur1 = y_nxt1;
             t_cur0 = t_nxt0;
             t_cur1 = t_nxt1;
             n_cur = n_nxt;
         };
         issue(1, st_n, steps[0], pc.sP);
-        advance();
+        advance(1);
         issue(2, st_nn, st_n, pc.sP);
         __syncthreads();
 
@@ -292,7 +310,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
             // ================= phase 1 =================
             // (1a) window rows: fold the last update in; corrections of the active rows
-            for (int r = tid; r < 2 * XSP; r += kThreads) {
+            for (int r = tid; r < 2 * XSP && tid < kRowThreads; r += kRowThreads) {
                 const int q = r >> 1;
                 int d = q - los;
                 if (d < 0) d += XSP;
@@ -307,29 +325,39 @@ __global__ void __launch_bounds__(kThreads, 2)
                 cs[r] = c;
             }
             // (1b) pairs entering at t+1: data, window kernel, start of their predictions
-            if (ne == 1 && e_cur.n == e_lo && !e_cur.slow) {
+            const bool fast = ne == 1 && e_cur.n == e_lo && !e_cur.slow;
+            if (fast) {
+              if (et >= 0) {
                 const int n = e_cur.n, qn = n % XSP;
-                float g0 = gf0, g1 = gf1;
-                const int bw = e_cur.F + tid;
-                if (bw < e_cur.top) {
-                    const int sl = wrap_slot(e_cur.F % XSP + tid);
-                    acc_pair(*reinterpret_cast<const float2*>(aw + 2 * sl), win_cur, g0, g1);
-                    if (bw > n - LB) fill_band(sl, qn, win_cur);
+                float g0 = 0.f, g1 = 0.f;
+                const int Fs = e_cur.F % XSP;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int i = et + h * kEntThreads;
+                    const int bw = e_cur.F + i;
+                    if (bw < e_cur.top) {
+                        const float4 kv = h == 0 ? win_cur0 : win_cur1;
+                        const int sl = wrap_slot(Fs + i);
+                        acc_pair(*reinterpret_cast<const float2*>(aw + 2 * sl), kv, g0, g1);
+                        if (bw > n - LB) fill_band(sl, qn, kv);
+                    }
                 }
-                if (tid < D) lin_feature(tid, r_s[tid], y_cur, g0, g1);
+                if (et < D) lin_feature(et, r_s[et], y_cur0, g0, g1);
+                if (et + kEntThreads < D) lin_feature(et + kEntThreads, r_s[et + kEntThreads], y_cur1, g0, g1);
                 warp_sum2(g0, g1);
                 if (lane == 0) {
-                    wp[2 * warp] = g0;
-                    wp[2 * warp + 1] = g1;
+                    wpe[2 * (warp - kRowThreads / 32)] = g0;
+                    wpe[2 * (warp - kRowThreads / 32) + 1] = g1;
                 }
-                if (tid < Np) Yw[qn * Np + tid] = tid < N ? y_cur : make_float2(0.f, 0.f);
-                if (tid == 0) {
+                if (et < Np) Yw[qn * Np + et] = et < N ? y_cur0 : make_float2(0.f, 0.f);
+                if (et == 0) {
                     yw[2 * qn] = t_cur0;
                     yw[2 * qn + 1] = t_cur1;
                     aw[2 * qn] = aw[2 * qn + 1] = 0.f;
                     rd[qn] = 1.f / fmaf(wL, n_cur, wG);
                     fill_diag(qn, n_cur);
                 }
+              }
             } else if (ne > 0) {
                 // direct loads (several pairs per step, or columns longer than the pipeline holds)
                 const int top = pc.hiP, lo = pn.loP, fb = pc.sP;
@@ -427,10 +455,16 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
             // (2d) entering pairs: predictions start from the reduced partial sums (plus wL <x_n, dr>
             //      after an eviction: their partial sums used r from before it)
-            for (int i = tid; i < 2 * min(ne, kMaxEnter); i += kThreads) {
+            for (int i = kThreads - 1 - tid; i < 2 * min(ne, kMaxEnter) && i >= 0; i += kThreads) {
                 const int e = i >> 1, row = i & 1, qn = (e_lo + e) % XSP;
                 float s = 0.f;
-                for (int w2 = 0; w2 < kWarps; ++w2) s += wp[(e * kWarps + w2) * 2 + row];
+                if (fast) {
+                    const int fb = (t + 1) & 1; // frozen partials of the pair entering at t+1
+                    for (int w2 = 0; w2 < kWarps; ++w2) s += wpf[(fb * kWarps + w2) * 2 + row];
+                    s += wpe[row] + wpe[2 + row];
+                } else {
+                    for (int w2 = 0; w2 < kWarps; ++w2) s += wp[(e * kWarps + w2) * 2 + row];
+                }
                 if (evict) {
                     float l = 0.f;
                     for (int k = 0; k < N; ++k) {
@@ -442,7 +476,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 hw[2 * qn + row] = s;
             }
             // (2e) pipeline: frozen part of the pair entering at t+2, loads for t+3
-            advance();
+            advance(t & 1); // the pair entering at t+2: parity (t + 2) & 1
             issue(t + 3, st_3, st_nn, pc.sP);
             los += pn.sP - pc.sP;
             if (los >= XSP) los -= XSP;
@@ -462,7 +496,7 @@ int batch_sweep_threads() { return kThreads; }
 size_t batch_sweep_smem(const BatchCommon& cm)
 {
     const size_t f = 3 * size_t(cm.XSP) * cm.XSPp + 2 * size_t(cm.XSP) * cm.Np + 8 * size_t(cm.XSPp) + cm.XSPp +
-                     size_t(kParts) * 2 * cm.XSPp + 2 * kMaxFeatures + 2 * kMaxEnter * kWarps;
+                     size_t(kParts) * 2 * cm.XSPp + 2 * kMaxFeatures + 2 * kMaxEnter * kWarps + 4 * kWarps + 4;
     return sizeof(float) * f;
 }
 

@@ -174,6 +174,10 @@ class DetectorPool:
         self._check(self._lib.apsm_pool_last_ms(self._h, int(lane), ctypes.byref(t), ctypes.byref(d)))
         return t.value, d.value
 
+    def last_launches(self, lane: int = 0) -> int:
+        """Kernels the lane's last batch launched."""
+        return int(self._lib.apsm_pool_last_launches(self._h, int(lane)))
+
     def job_bytes(self, job: PoolJob) -> int:
         n = self.antennas[job.detector]
         length = int(job.rx.shape[1])

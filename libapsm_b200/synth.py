@@ -125,3 +125,48 @@ def config2_detectors(n: int = 512, seed: int = 2, users_per_cell: int = 4,
         out.append(DetectorFrame(f.rx_train, np.ascontiguousarray(f.tx_train[0]), f.rx_data,
                                  np.ascontiguousarray(f.tx_data[0]), f.modulation, snr))
     return out
+
+
+@dataclass
+class ServedDetector:
+    """A resident detector of the serving workload: the frame it is first
+    trained on, then one pilot chunk and one data chunk that its per-TTI
+    requests take prefixes of (same channel)."""
+
+    frame: DetectorFrame
+    pilots_rx: np.ndarray   # (N, 64) complex64
+    pilots_tx: np.ndarray   # (64,) complex64
+    data_rx: np.ndarray     # (N, 4000) complex64
+    data_tx: np.ndarray     # (4000,) complex64
+
+
+def config4_population(n: int = 512, seed: int = 4, users_per_cell: int = 4) -> list[ServedDetector]:
+    """Detectors of the serving workload, sizes as config2_detectors: each is
+    trained on its frame's pilots first; its TTIs append 16-64 pilots and
+    detect 500-4000 symbols."""
+    out = []
+    for d in config2_detectors(n, seed=seed, users_per_cell=users_per_cell, data=(4000, 4000)):
+        # the frame's data symbols feed the TTIs: first 64 as pilots, the rest as data
+        out.append(ServedDetector(d, d.rx_data[:, :64].copy(), d.tx_data[:64].copy(),
+                                  np.ascontiguousarray(d.rx_data), np.ascontiguousarray(d.tx_data)))
+    return out
+
+
+def config4_requests(pop: list[ServedDetector], rate_hz: float, duration_s: float, seed: int = 5):
+    """Poisson arrivals at rate_hz over duration_s: (arrival time, detector
+    index, kind, length) with each detector alternating train (16-64 new
+    pilots) and detect (500-4000 symbols), starting with a train."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    phase = np.zeros(len(pop), np.int8)
+    while True:
+        t += float(rng.exponential(1.0 / rate_hz))
+        if t >= duration_s:
+            break
+        d = int(rng.integers(0, len(pop)))
+        if phase[d] == 0:
+            out.append((t, d, "train", int(rng.integers(16, 65))))
+        else:
+            out.append((t, d, "detect", int(rng.integers(500, 4001))))
+        phase[d] ^= 1
+    return out
