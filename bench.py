@@ -1,22 +1,30 @@
 #!/usr/bin/env python3
-"""Benchmark: detected symbols/s of APSM training + detection on one B200.
+"""Benchmark: detected symbols/s of batched APSM detection on one B200, with
+the plain per-detector form and the served (per-TTI request) form beside it.
 
-Workload (one "step" = one frame): 16QAM, K = 8 users, N = 16 antennas,
-P = 1000 pilots, S = 8000 data symbols, window 80, dictionary 1000 entries,
-FP32; every user is trained on the frame's pilots from a fresh state and then
-detects the frame's data.  Metric: detected symbols/s = users x S / frame time.
-Seeded synthetic frames (Rayleigh channel, Rapp PA, AWGN at 20 dB); the
-reference publishes no dataset for this path.
+Headline workload (one "step" = one batch): 512 independent detectors (users
+x cells), antennas uniform over {4, 8, 16, 32}, pilots over [200, 2000], data
+symbols over [1000, 16000], SNR over [10, 25] dB, QPSK or 16QAM, Rapp PA;
+window 80, dictionary 2000 entries, the reference's defaults otherwise.  Each
+detector is trained from a fresh state on its pilots and detects its data:
+all of it one detector-pool batch (one persistent training launch, tensor-core
+detection in TF32 hi/lo form, FP32-accurate).  Seeded synthetic frames
+(Rayleigh channel, Rapp PA, AWGN); the reference publishes no dataset.
 
-  value   device-resident inputs: train + detect kernels only
-  e2e     the public C ABI with host buffers (apsm_train / apsm_detect):
-          H2D of the frame and D2H of the estimates inside the timed region
+  value    device-resident inputs: the batch's kernels (CUDA events on its stream)
+  e2e      the public C ABI with host buffers (apsm_pool_run, APSM_RUN_HOST):
+           staging, host-to-device copy, kernels, device-to-host copy
+  plain    the per-detector form (NomaDetector per user, the reference's API)
+           on one 8-user 16QAM frame (N=16, 1000 pilots, 8000 symbols)
+  serving  Poisson per-TTI requests (train-append 16-64 pilots / detect
+           500-4000 symbols) against 512 resident detectors through the
+           request server: p50 / p99 latency and detected symbols/s
 
-``--impl reference`` times the reference algorithm on the host CPU cores
-(the reference has no CPU implementation of APSM, so this is the repository's
-FP32 C restatement of it, OpenMP over all host threads) on a bounded sample of
-the same workload, plus the reference's own CUDA library on this GPU when it
-was built (``reference_cuda``).
+``--impl reference`` times the reference algorithm on the host cores (the
+reference has no CPU implementation of APSM: this is the repository's FP32 C
+restatement of it, OpenMP over all host threads) on a bounded sample of the
+same workload, plus the reference's own CUDA library on this GPU when it was
+built (``reference_cuda``, one NomaDetector per detector as its API runs).
 
 With torchrun (N > 1) every rank runs an independent replica (detectors do
 not shard and need no collective); value = all ranks' symbols / max time.
@@ -38,11 +46,13 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "detected symbols/s (APSM train + detect per frame, all users)"
+METRIC = "detected symbols/s (batched APSM train + detect, 512 heterogeneous detectors)"
 UNIT = "symbols/s"
-WORKLOAD = {"workload": "16QAM K=8 users N=16 P=1000 S=8000 window=80 dictionary=1000 FP32 train+detect per frame",
-            "users": 8, "antennas": 16, "pilots": 1000, "data_symbols": 8000, "window": 80, "dictionary": 1000,
-            "snr_db": 20, "l2": "flushed between timed steps (256 MiB write)"}
+N_DET = 512
+WORKLOAD = {"workload": "512 detectors: N~U{4,8,16,32}, P~U[200,2000], S~U[1000,16000], SNR~U[10,25] dB, "
+                        "QPSK/16QAM, window 80, dictionary 2000, fresh train + detect per step",
+            "detectors": N_DET, "window": 80, "dictionary": 2000, "detect": "gram_tf32x3 (FP32-accurate)",
+            "l2": "inputs 0.6 GB (> L2) and a 256 MiB write between timed steps"}
 
 
 # ------------------------------------------------------------------ clocks --
@@ -61,7 +71,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                          "-i", str(self.index), "-lms", "100"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -98,16 +108,21 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
-# ---------------------------------------------------------------- B200 arm --
-def algorithmic_sweep_bytes(users: int, P: int, D: int) -> int:
-    """Minimum HBM bytes of one training sweep launch: the pilot rows (2P x D),
-    their norms, each user's targets and coefficients (read + write) and
-    linear weights."""
-    rows = 2 * P
-    return 4 * (rows * D + rows + users * (rows + 2 * rows + 2 * D))
+# ------------------------------------------------------- batched (headline) --
+def sweep_algorithmic_bytes(dets, window: int, dict_size: int) -> int:
+    """Minimum HBM bytes of one batched training-sweep launch: every kernel-
+    column entry it combines (16 B, each read once: pair n against the pairs
+    before it), the pilots (8N B per complex sample), targets and
+    coefficients (read + write) of every job."""
+    total = 0
+    for d in dets:
+        nP, capP = d.P, dict_size
+        cols = sum(min(n, capP) for n in range(nP))
+        total += 16 * cols + 8 * d.N * nP + 4 * (2 * nP) * 3
+    return total
 
 
-def run_b200(args, rank: int, world: int) -> dict | None:
+def run_batched(args, rank: int, world: int) -> dict | None:
     import torch
 
     import libapsm_b200 as L
@@ -115,34 +130,26 @@ def run_b200(args, rank: int, world: int) -> dict | None:
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    frame = synth.config1_frame(seed=1 + rank)
-    cfg = dict(synth.CONFIG1_ALGORITHM)
-    if args.detect_version:
-        cfg["detectVersion"] = args.detect_version
-    U, N = frame.tx_train.shape[0], frame.rx_train.shape[0]
-    P, S = frame.rx_train.shape[1], frame.rx_data.shape[1]
-    det = L.NomaDetectorFactory.build(cfg, N, num_users=U)
-    stream = torch.cuda.ExternalStream(det.stream)
-    rx = torch.from_numpy(frame.rx_train).cuda()
-    tx = torch.from_numpy(frame.tx_train).cuda()
-    rxd = torch.from_numpy(frame.rx_data).cuda()
-    est = torch.empty((U, S), dtype=torch.complex64, device="cuda")
+    dets = synth.config2_detectors(N_DET, seed=2 + rank)
+    cfg = dict(synth.CONFIG2_ALGORITHM, detectVersion="gram_tf32x3")
+    pool = L.DetectorPool(cfg)
+    ids = [pool.add(d.N) for d in dets]
+    stream = torch.cuda.ExternalStream(pool.stream(0))
+    dev_in = [(torch.from_numpy(d.rx_train).cuda(), torch.from_numpy(d.tx_train).cuda(),
+               torch.from_numpy(d.rx_data).cuda(), torch.empty(d.S, dtype=torch.complex64, device="cuda"))
+              for d in dets]
+    jobs = pool.prepare([L.PoolJob(i, x[0], x[1], fresh=True) for i, x in zip(ids, dev_in)] +
+                        [L.PoolJob(i, x[2], est=x[3]) for i, x in zip(ids, dev_in)], device=True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    # pack pilots, gather targets, kernel columns, sweep, pack data, detect
-    # (+ operand packing x2, coefficients, reduction for the tensor-core detect)
-    launches_per_step = 10 if cfg.get("detectVersion", "").startswith("gram") else 6
-
-    def step():
-        det.reset_state()
-        det.train_device(rx, tx)
-        det.detect_device(rxd, est)
+    torch.cuda.synchronize()
 
     for _ in range(args.warmup):
-        step()
-    det.synchronize()
+        pool.run_prepared(jobs, mode=1)
+    pool.wait()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    sweep_ms, detect_ms = [], []
+    stage = {"train": [], "sweep": [], "detect": []}
+    launches = 0
     clocks = ClockSampler(dev)
     if world > 1:
         torch.distributed.barrier()
@@ -152,113 +159,193 @@ def run_b200(args, rank: int, world: int) -> dict | None:
         with torch.cuda.stream(stream):
             flush.zero_()
             ev[i][0].record(stream)
-        step()
+        pool.run_prepared(jobs, mode=1)
         with torch.cuda.stream(stream):
             ev[i][1].record(stream)
-        s_ms, d_ms = det.last_kernel_ms()
-        sweep_ms.append(s_ms)
-        detect_ms.append(d_ms)
+        pool.wait()
+        t_ms, d_ms = pool.last_ms()
+        stage["train"].append(t_ms)
+        stage["detect"].append(d_ms)
+        stage["sweep"].append(pool.last_sweep_ms())
+        launches += pool.last_launches()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     clk = clocks.stop()
     total_ms = sum(a.elapsed_time(b) for a, b in ev)
 
-    # ---- e2e through the host C ABI (pinned host buffers, H2D/D2H inside) ----
-    h_rx = torch.from_numpy(frame.rx_train).pin_memory()
-    h_tx = torch.from_numpy(frame.tx_train).pin_memory()
-    h_rxd = torch.from_numpy(frame.rx_data).pin_memory()
-    h_est = torch.empty((U, S), dtype=torch.complex64).pin_memory()
-    lib = det._lib
-    import ctypes
+    # SER of the estimates (hard decisions of the reference's Gray map)
+    sers = [L.symbol_error_rate(x[3].cpu().numpy(), d.tx_data, d.modulation) for d, x in zip(dets, dev_in)]
 
-    def e2e_step():
-        det.reset_state()
-        lib.apsm_train(det._h, h_rx.data_ptr(), h_tx.data_ptr(), P, None)
-        lib.apsm_detect(det._h, h_rxd.data_ptr(), S, h_est.data_ptr(), None)
-
+    # ---- e2e: host buffers through the C ABI (staging + copies inside) ----
+    host_jobs = ([L.PoolJob(i, d.rx_train, d.tx_train, fresh=True) for i, d in zip(ids, dets)] +
+                 [L.PoolJob(i, d.rx_data, est=np.zeros(d.S, np.complex64)) for i, d in zip(ids, dets)])
+    prepared = pool.prepare(host_jobs)
     for _ in range(args.warmup):
-        e2e_step()
-    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        pool.run_prepared(prepared)
     if world > 1:
         torch.distributed.barrier()
-    torch.cuda.synchronize()
-    for i in range(args.steps):
+    e2e_ms = []
+    for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
-            ev2[i][0].record(stream)
-        e2e_step()
-        with torch.cuda.stream(stream):
-            ev2[i][1].record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = sum(a.elapsed_time(b) for a, b in ev2)
-    est_ok = np.isfinite(h_est.numpy()).all()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pool.run_prepared(prepared)  # apsm_pool_run, APSM_RUN_HOST
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    h2d = sum(d.rx_train.nbytes + d.tx_train.nbytes + d.rx_data.nbytes for d in dets)
+    d2h = sum(8 * d.S for d in dets)
 
-    # ---- max over ranks ----
-    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    t = torch.tensor([total_ms, sum(e2e_ms)], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms, e2e_ms = float(t[0]), float(t[1])
+    total_ms, e2e_total = float(t[0]), float(t[1])
     if rank != 0:
         return None
 
-    symbols = world * U * S
+    symbols = world * sum(d.S for d in dets)
     ms_step = total_ms / args.steps
-    sweep = float(np.median(sweep_ms))
+    sweep = float(np.median(stage["sweep"]))
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak_gbs = float(peaks.get("hbm_gbs", 6650.0))
-    alg_bytes = algorithmic_sweep_bytes(U, P, 2 * N)
-    achieved = alg_bytes / (sweep * 1e-3) / 1e9
-    ser = float(np.mean([L.symbol_error_rate(h_est.numpy()[u], frame.tx_data[u], frame.modulation)
-                         for u in range(U)]))
+    alg = sweep_algorithmic_bytes(dets, 80, 2000)
+    achieved = alg / (sweep * 1e-3) / 1e9
     return {
         "metric": METRIC, "value": symbols / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded NOMA frames; no public dataset)",
-        "config": dict(WORKLOAD, parallelism=f"replicas x{world}", detect_version=cfg.get("detectVersion", "balanced")),
-        "e2e": {"value": symbols / (e2e_ms / args.steps * 1e-3), "unit": UNIT,
-                "h2d_bytes_per_step": int(h_rx.numel() * 8 + h_tx.numel() * 8 + h_rxd.numel() * 8),
-                "d2h_bytes_per_step": int(h_est.numel() * 8), "ms_per_step": e2e_ms / args.steps},
-        "gpu_launches": launches_per_step * args.steps,
-        "roofline": {"bound": "hbm", "kernel": "train_exact_kernel (training sweep)", "achieved": achieved,
-                     "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
-                     # dram read + write of one sweep launch on this workload, ncu
-                     # (profiles/train_sweep_kernel_config1_frame.md): the kernel columns
-                     "traffic": 9772544,
-                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": sweep,
-                     "note": "sweep is a chain of P dependent steps; latency-bound, see DESIGN.md",
+        "config": dict(WORKLOAD, parallelism=f"replicas x{world}"),
+        "e2e": {"value": symbols / (e2e_total / args.steps * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_total / args.steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "batch_sweep_kernel (training sweep, all 512 jobs)",
+                     "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
+                     "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_ms": sweep,
+                     "note": "a chain of P dependent steps per detector: latency / shared-memory bound, "
+                             "not HBM; see profiles/",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
-        "stage_ms": {"sweep": sweep, "detect": float(np.median(detect_ms))},
-        "ser_mean": ser, "estimates_finite": bool(est_ok),
-        "clocks": clk,
+        "stage_ms": {k: float(np.median(v)) for k, v in stage.items()},
+        "ser_mean": float(np.mean(sers)), "clocks": clk,
     }
 
 
+# -------------------------------------------------- plain per-detector form --
+def run_plain(steps: int = 5, warmup: int = 3) -> dict:
+    """The reference's per-detector API (NomaDetector per user) on one
+    config-1 frame: 8 users, N=16, 1000 pilots, 8000 symbols, FP32."""
+    import torch
+
+    import libapsm_b200 as L
+    from libapsm_b200 import synth
+
+    frame = synth.config1_frame(seed=1)
+    cfg = dict(synth.CONFIG1_ALGORITHM)
+    U, N = frame.tx_train.shape[0], frame.rx_train.shape[0]
+    S = frame.rx_data.shape[1]
+    det = L.NomaDetectorFactory.build(cfg, N, num_users=U)
+    stream = torch.cuda.ExternalStream(det.stream)
+    rx, tx, rxd = (torch.from_numpy(a).cuda() for a in (frame.rx_train, frame.tx_train, frame.rx_data))
+    est = torch.empty((U, S), dtype=torch.complex64, device="cuda")
+
+    def step():
+        det.reset_state()
+        det.train_device(rx, tx)
+        det.detect_device(rxd, est)
+
+    for _ in range(warmup):
+        step()
+    det.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        with torch.cuda.stream(stream):
+            ev[i][0].record(stream)
+        step()
+        with torch.cuda.stream(stream):
+            ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+    return {"value": U * S / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+            "workload": "16QAM K=8 users N=16 P=1000 S=8000 window=80 dictionary=1000, NomaDetector per user "
+                        "(exact FP32 sweep + BALANCED-order detect)"}
+
+
+# ------------------------------------------------------------ serving form --
+def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = N_DET) -> dict:
+    """Poisson per-TTI requests against resident detectors through the
+    request server (continuous batching, 2 lanes)."""
+    import libapsm_b200 as L
+    from libapsm_b200 import synth
+    from libapsm_b200.server import clock
+
+    pop = synth.config4_population(n_det)
+    reqs = synth.config4_requests(pop, rate_hz, duration_s)
+    cfg = dict(synth.CONFIG2_ALGORITHM)
+    pool = L.DetectorPool(cfg, lanes=2)
+    ids = [pool.add(p.frame.N) for p in pop]
+    pool.run([L.PoolJob(i, p.frame.rx_train, p.frame.tx_train) for i, p in zip(ids, pop)])
+    srv = L.DetectorServer(pool, max_batch=64)
+    prepared = []
+    for (ta, d, kind, n) in reqs:
+        p = pop[d]
+        j = (L.PoolJob(ids[d], p.pilots_rx[:, :n], p.pilots_tx[:n]) if kind == "train"
+             else L.PoolJob(ids[d], p.data_rx[:, :n]))
+        prepared.append((ta, kind, n, srv.make_job(j)))
+    warm = [srv.submit_prepared(srv.make_job(L.PoolJob(ids[k], pop[k].data_rx[:, :1000]))) for k in range(64)]
+    for t in warm:
+        srv.wait(t)
+    b0, _ = srv.stats()
+    start = clock() + 0.01
+    tickets = []
+    for (ta, kind, n, prep) in prepared:
+        target = start + ta
+        while clock() < target:
+            pass
+        tickets.append(srv.submit_prepared(prep))
+    lat, syms, done = [], 0, []
+    for (ta, kind, n, prep), tk in zip(prepared, tickets):
+        srv.wait(tk)
+        s0, s1, s2 = srv.times(tk)
+        lat.append(s2 - s0)
+        done.append(s2)
+        syms += n if kind == "detect" else 0
+    b, _ = srv.stats()
+    srv.close()
+    lat_us = np.array(lat) * 1e6
+    return {"p50_us": float(np.percentile(lat_us, 50)), "p99_us": float(np.percentile(lat_us, 99)),
+            "deadline_500us_met": float(np.mean(lat_us <= 500.0)), "symbols_per_s": syms / (max(done) - start),
+            "requests": len(reqs), "rate_hz": rate_hz, "duration_s": duration_s, "batches": int(b - b0),
+            "detect": "FP32 CUDA-core pair form",
+            "workload": "512 resident detectors (config-2 sizes); requests alternate train-append (16-64 pilots) "
+                        "and detect (500-4000 symbols) per detector; request server, 2 lanes"}
+
+
 # ----------------------------------------------------------- reference arm --
-def cpu_baseline(sample_users: int = 1) -> dict:
-    """The FP32 restatement of the reference algorithm on the host cores,
-    on a bounded sample of the workload (sample_users of the frame's users)."""
+def cpu_baseline(n_sample: int = 2) -> dict:
+    """The FP32 restatement of the reference algorithm on the host cores, on
+    a bounded sample of the batched workload (the first n_sample detectors)."""
     from libapsm_b200 import synth
     from oracle import oracle as O
 
     threads = O.set_threads(os.cpu_count() or 1)
-    frame = synth.config1_frame(seed=1)
-    cfg = dict(synth.CONFIG1_ALGORITHM)
-    S = frame.rx_data.shape[1]
+    dets = synth.config2_detectors(n_sample, seed=2)
+    cfg = dict(synth.CONFIG2_ALGORITHM)
     t0 = time.perf_counter()
-    for u in range(sample_users):
-        d = O.OracleDetector(cfg, frame.rx_train.shape[0], O.F32)
-        d.train(frame.rx_train, frame.tx_train[u])
-        d.detect(frame.rx_data)
+    syms = 0
+    for d in dets:
+        o = O.OracleDetector(cfg, d.N, O.F32)
+        o.train(d.rx_train, d.tx_train)
+        o.detect(d.rx_data)
+        syms += d.S
     dt = time.perf_counter() - t0
-    return {"value": sample_users * S / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{sample_users} of 8 users of one frame (train 1000 pilots + detect 8000 symbols each), "
-                      f"{dt:.2f} s"}
+    return {"value": syms / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n_sample} of the 512 detectors (train + detect each, {syms} symbols), {dt:.2f} s"}
 
 
-def reference_cuda(warmup: int, steps: int) -> dict | None:
-    """The reference library (built from its sources for sm_100a) on this GPU,
-    as its CLI's -p mode runs it: one detector and host thread per user."""
+def reference_cuda(n_sample: int = 16) -> dict | None:
+    """The reference library (built from its sources for sm_100a) on this
+    GPU: one NomaDetector per detector, train + detect, eight host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+
     from libapsm_b200 import synth
     from oracle import oracle as O
 
@@ -271,17 +358,22 @@ def reference_cuda(warmup: int, steps: int) -> dict | None:
             return None
     except Exception:
         return None
-    frame = synth.config1_frame(seed=1)
-    cfg = dict(synth.CONFIG1_ALGORITHM)
-    U, S = frame.tx_train.shape[0], frame.rx_data.shape[1]
-    for _ in range(warmup):
-        O.reference_users_threaded(cfg, frame.rx_train, frame.tx_train, frame.rx_data)
+    dets = synth.config2_detectors(n_sample, seed=2)
+    cfg = dict(synth.CONFIG2_ALGORITHM)
+
+    def one(d):
+        r = O.ReferenceDetector(cfg, d.N)
+        r.train(d.rx_train, d.tx_train)
+        r.detect(d.rx_data)
+
+    one(dets[0])  # warm-up (context, module load)
     t0 = time.perf_counter()
-    for _ in range(steps):
-        O.reference_users_threaded(cfg, frame.rx_train, frame.tx_train, frame.rx_data)
-    dt = (time.perf_counter() - t0) / steps
-    return {"value": U * S / dt, "unit": UNIT, "ms_per_step": dt * 1e3,
-            "what": "reference CUDA kernels (libapsm built for sm_100a), 8 detectors on 8 host threads, wall clock"}
+    with ThreadPoolExecutor(8) as ex:
+        list(ex.map(one, dets))
+    dt = time.perf_counter() - t0
+    return {"value": sum(d.S for d in dets) / dt, "unit": UNIT, "ms": dt * 1e3,
+            "what": f"reference CUDA kernels (libapsm built for sm_100a), {n_sample} of the 512 detectors, "
+                    "8 host threads, wall clock"}
 
 
 def run_reference(args, rank: int) -> dict | None:
@@ -290,13 +382,12 @@ def run_reference(args, rank: int) -> dict | None:
     base = cpu_baseline()
     line = {
         "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": WORKLOAD["users"] * WORKLOAD["data_symbols"] / base["value"] * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded NOMA frames; no public dataset)", "config": dict(WORKLOAD),
-        "impl": "reference", "cpu_baseline": base,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded NOMA frames; no public dataset)",
+        "config": dict(WORKLOAD), "impl": "reference", "cpu_baseline": base,
         "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    rc = reference_cuda(min(args.warmup, 1), min(args.steps, 3))
+    rc = reference_cuda()
     if rc is not None:
         line["reference_cuda"] = rc
     return line
@@ -305,12 +396,11 @@ def run_reference(args, rank: int) -> dict | None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--detect-version", default=None,
-                    help="detectVersion of the algorithm config (default: the reference's 'balanced')")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain and serving measurements")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -330,7 +420,10 @@ def main():
 
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = run_b200(args, rank, world)
+    line = run_batched(args, rank, world)
+    if line is not None and not args.no_extras:
+        line["plain"] = run_plain()
+        line["serving"] = run_serving()
     if line is not None and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if world > 1:

@@ -199,6 +199,9 @@ uint64_t apsm_pool_bytes_in_use(const apsm_pool* p);
  * columns + sweep) and detection stages; blocks until the batch finished. */
 apsm_status apsm_pool_last_ms(apsm_pool* p, uint32_t lane, float* train_ms, float* detect_ms);
 
+/* GPU time (ms) of the persistent training sweep kernel of the lane's last batch (-1: none). */
+apsm_status apsm_pool_last_sweep_ms(apsm_pool* p, uint32_t lane, float* sweep_ms);
+
 /* Kernels the lane's last batch launched (its own kernels; memsets and copies excluded). */
 int apsm_pool_last_launches(apsm_pool* p, uint32_t lane);
 

@@ -41,7 +41,7 @@ struct PoolDet {
 
 struct Lane {
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr}; // train start/end, detect start/end
+    cudaEvent_t ev[6] = {};     // train start/end, detect start/end, sweep start/end
     cudaEvent_t done = nullptr;                                // end of the last batch
     cudaEvent_t desc_copied = nullptr;                         // the pinned descriptors were consumed
     bool have_train = false, have_detect = false;
@@ -563,7 +563,9 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         const auto* d_tj = reinterpret_cast<const BatchTrainJob*>(D(off_tj));
         POOL_CK(launch_batch_kcol(d_tj, int(nT), max_cols, max_n, cm, s));
         const int grid = int(std::min<size_t>(nT, size_t(sweep_ctas) * sms));
+        POOL_CK(cudaEventRecord(L.ev[4], s));
         POOL_CK(launch_batch_sweep(d_tj, int(nT), cm, grid, d_counter, d_err, s));
+        POOL_CK(cudaEventRecord(L.ev[5], s));
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_co)), int(nT), max_pairs_out, max_np, s));
         L.launches += (max_cols > 0) + 1 + (max_pairs_out > 0);
         POOL_CK(cudaEventRecord(L.ev[1], s));
@@ -893,4 +895,16 @@ extern "C" int apsm_pool_last_launches(apsm_pool* p, uint32_t lane)
 {
     if (!p || lane >= p->lanes.size()) return -1;
     return p->lanes[lane].launches;
+}
+
+extern "C" apsm_status apsm_pool_last_sweep_ms(apsm_pool* p, uint32_t lane, float* sweep_ms)
+{
+    if (!p || lane >= p->lanes.size() || !sweep_ms) return APSM_ERR_INVALID_ARGUMENT;
+    Lane& L = p->lanes[lane];
+    cudaError_t e = cudaEventSynchronize(L.done);
+    if (e != cudaSuccess) return p->cuda_fail(e, "cudaEventSynchronize");
+    *sweep_ms = -1.f;
+    if (L.have_train && cudaEventElapsedTime(sweep_ms, L.ev[4], L.ev[5]) != cudaSuccess) *sweep_ms = -1.f;
+    cudaGetLastError();
+    return APSM_OK;
 }

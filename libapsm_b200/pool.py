@@ -152,6 +152,17 @@ class DetectorPool:
         del keep
         return [j.est if j.kind == JOB_DETECT else None for j in jobs]
 
+    def prepare(self, jobs: Sequence[PoolJob], device: bool = False):
+        """The native job list of a batch, for repeated apsm_pool_run calls
+        (run_prepared); keeps the host arrays it points to alive."""
+        arr, keep = self._cjobs(jobs, device=device)
+        return (arr, len(jobs), keep, list(jobs))
+
+    def run_prepared(self, prepared, lane: int = 0, mode: int = 0) -> None:
+        """apsm_pool_run on a prepared job list (mode 0: host buffers, 1: device buffers)."""
+        arr, n, _, _ = prepared
+        self._check(self._lib.apsm_pool_run(self._h, int(lane), ctypes.cast(arr, ctypes.c_void_p), n, int(mode)))
+
     def run_device(self, jobs: Sequence[PoolJob], lane: int = 0) -> None:
         """Device buffers (torch complex64 CUDA tensors); asynchronous on the lane's stream."""
         arr, _ = self._cjobs(jobs, device=True)
@@ -173,6 +184,12 @@ class DetectorPool:
         t, d = ctypes.c_float(), ctypes.c_float()
         self._check(self._lib.apsm_pool_last_ms(self._h, int(lane), ctypes.byref(t), ctypes.byref(d)))
         return t.value, d.value
+
+    def last_sweep_ms(self, lane: int = 0) -> float:
+        """GPU time of the last batch's training sweep kernel."""
+        v = ctypes.c_float()
+        self._check(self._lib.apsm_pool_last_sweep_ms(self._h, int(lane), ctypes.byref(v)))
+        return v.value
 
     def last_launches(self, lane: int = 0) -> int:
         """Kernels the lane's last batch launched."""
