@@ -95,6 +95,21 @@ apsm_status apsm_reset(apsm_detector* h);
 apsm_status apsm_train_device(apsm_detector* h, const float* d_rx, const float* d_tx, uint32_t P, void* stream);
 apsm_status apsm_detect_device(apsm_detector* h, const float* d_rx, uint32_t S, float* d_est, void* stream);
 
+/*
+ * Detection that allocates no device memory: the exact FP32 detection of
+ * apsm_detect_device, with the packed data rows in a fixed 8 MiB device array
+ * of the library instead of a buffer of the handle that grows with S.  For
+ * callers that must not allocate on the call path.  No counterpart in the
+ * reference (its detect allocates and copies per call, cuda_matrix_host.cu:105-149).
+ * Limit: 2 * S * Dp * 4 bytes <= 8 MiB, Dp = 2N rounded up to 4 (S <= 32768
+ * at N = 16); larger S returns APSM_ERR_INVALID_ARGUMENT.  APSM handles with
+ * the reference's detectVersion values only (else APSM_ERR_UNSUPPORTED).  The
+ * first call on a device looks up the array's address (make it before any
+ * stream capture); the array is shared by all handles on the device, so calls
+ * that overlap on a device race and must be serialised by the caller.
+ */
+apsm_status apsm_detect_device_noalloc(apsm_detector* h, const float* d_rx, uint32_t S, float* d_est, void* stream);
+
 /* The handle's CUDA stream (cudaStream_t) and a blocking wait on it. */
 void* apsm_stream(apsm_detector* h);
 apsm_status apsm_synchronize(apsm_detector* h);

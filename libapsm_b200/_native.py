@@ -45,6 +45,7 @@ SIGNATURES = [
     ("apsm_reset", ctypes.c_int, [_P]),
     ("apsm_train_device", ctypes.c_int, [_P, _P, _P, _U32, _P]),
     ("apsm_detect_device", ctypes.c_int, [_P, _P, _U32, _P, _P]),
+    ("apsm_detect_device_noalloc", ctypes.c_int, [_P, _P, _U32, _P, _P]),
     ("apsm_stream", _P, [_P]),
     ("apsm_synchronize", ctypes.c_int, [_P]),
     ("apsm_rows", _U32, [_P]),
