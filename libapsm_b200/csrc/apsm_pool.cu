@@ -17,6 +17,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace apsm;
@@ -59,6 +60,35 @@ struct Lane {
     int* err = nullptr;           // error flag of the last batch (in the scratch)
     int launches = 0;             // kernels launched by the last batch
 };
+
+// Page-locked host memory (cudaMallocHost or cudaHostRegister): copies need no staging.
+bool is_pinned(const void* p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Copies the inputs into the pinned staging buffer, on several threads for large batches.
+template <class In> void staged_copy(char* dst, const std::vector<In>& ins)
+{
+    size_t total = 0;
+    for (const auto& in : ins) total += in.bytes;
+    const unsigned nt = total > (size_t(16) << 20) ? std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1u;
+    if (nt <= 1) {
+        for (const auto& in : ins) std::memcpy(dst + in.off, in.src, in.bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned k = 0; k < nt; ++k)
+        th.emplace_back([&, k] {
+            for (size_t i = k; i < ins.size(); i += nt) std::memcpy(dst + ins[i].off, ins[i].src, ins[i].bytes);
+        });
+    for (auto& t : th) t.join();
+}
 
 int detect_class(uint32_t N)
 {
@@ -335,6 +365,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             t.perm_off = perm_off[t.P];
         }
     o = align_up(o, 256);
+    const size_t desc_only = o; // the descriptors alone
     if (host) { // staged host inputs travel with the descriptors
         for (auto& t : tp) {
             t.off_rx = o; o = align_up(o + sizeof(float2) * size_t(t.det->N) * t.P, 16);
@@ -529,15 +560,32 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
 
     // ---------- enqueue ----------
     cudaStream_t s = L.stream;
+    // host inputs: copied straight from the caller's buffers when they are page-locked,
+    // else staged through the lane's pinned buffer (one copy together with the descriptors)
+    struct HostIn {
+        const void* src;
+        size_t off, bytes;
+    };
+    std::vector<HostIn> ins;
+    bool direct = false;
     if (host) {
         for (const auto& t : tp) {
             const apsm_job& j = jobs[t.job];
-            std::memcpy(hst + t.off_rx, j.rx, sizeof(float2) * size_t(t.det->N) * t.P);
-            std::memcpy(hst + t.off_tx, j.tx, sizeof(float2) * t.P);
+            ins.push_back({j.rx, t.off_rx, sizeof(float2) * size_t(t.det->N) * t.P});
+            ins.push_back({j.tx, t.off_tx, sizeof(float2) * t.P});
         }
-        for (const auto& q : dp) std::memcpy(hst + q.off_rx, jobs[q.job].rx, sizeof(float2) * size_t(q.det->N) * q.S);
+        for (const auto& q : dp) ins.push_back({jobs[q.job].rx, q.off_rx, sizeof(float2) * size_t(q.det->N) * q.S});
+        direct = !ins.empty();
+        for (const auto& in : ins)
+            if (!is_pinned(in.src)) {
+                direct = false;
+                break;
+            }
+        if (!direct) staged_copy(hst, ins);
     }
-    POOL_CK(cudaMemcpyAsync(dev, hst, desc_bytes, cudaMemcpyHostToDevice, s));
+    POOL_CK(cudaMemcpyAsync(dev, hst, direct ? desc_only : desc_bytes, cudaMemcpyHostToDevice, s));
+    if (direct)
+        for (const auto& in : ins) POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, s));
     POOL_CK(cudaEventRecord(L.desc_copied, s));
     L.have_train = nT > 0;
     L.have_detect = nD > 0;
@@ -597,8 +645,20 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         }
         POOL_CK(cudaEventRecord(L.ev[3], s));
         if (host && est_bytes > 0) {
-            POOL_CK(cudaMemcpyAsync(L.pinned_out, D(est_begin), est_bytes, cudaMemcpyDeviceToHost, s));
-            for (const auto& q : dp) L.pending.push_back({jobs[q.job].est, q.off_est - est_begin, sizeof(float2) * q.S});
+            bool out_direct = true;
+            for (const auto& q : dp)
+                if (!is_pinned(jobs[q.job].est)) {
+                    out_direct = false;
+                    break;
+                }
+            if (out_direct) {
+                for (const auto& q : dp)
+                    POOL_CK(cudaMemcpyAsync(jobs[q.job].est, D(q.off_est), sizeof(float2) * q.S, cudaMemcpyDeviceToHost, s));
+            } else {
+                POOL_CK(cudaMemcpyAsync(L.pinned_out, D(est_begin), est_bytes, cudaMemcpyDeviceToHost, s));
+                for (const auto& q : dp)
+                    L.pending.push_back({jobs[q.job].est, q.off_est - est_begin, sizeof(float2) * q.S});
+            }
         }
     }
     POOL_CK(cudaEventRecord(L.done, s));

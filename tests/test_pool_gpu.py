@@ -194,3 +194,30 @@ def test_pool_fresh_flag_is_reset_then_train(native_lib):
     empty = np.zeros((8, 0), np.complex64)
     (est,) = pool.run([PoolJob(d, empty, np.zeros(0, np.complex64), fresh=True), PoolJob(d, rxd)])[1:]
     assert np.all(est == 0)
+
+
+def test_pool_pinned_host_buffers_equal_pageable(native_lib):
+    """Page-locked host buffers are copied directly (no staging); the results
+    equal those of ordinary host buffers."""
+    import torch
+
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    pool = DetectorPool(CFG)
+    specs = [(4, 90, 70), (8, 120, 33), (16, 60, 128)]
+    frames = [_frame(40 + i, *s_) for i, s_ in enumerate(specs)]
+    dets = [pool.add(n) for n, _, _ in specs]
+    ref = pool.run([PoolJob(d, f[0], f[1], fresh=True) for d, f in zip(dets, frames)] +
+                   [PoolJob(d, f[2]) for d, f in zip(dets, frames)])
+    keep = []
+
+    def pin(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        keep.append(t)
+        return t.numpy()
+
+    outs = [pin(np.zeros(f[2].shape[1], np.complex64)) for f in frames]
+    pool.run([PoolJob(d, pin(f[0]), pin(f[1]), fresh=True) for d, f in zip(dets, frames)] +
+             [PoolJob(d, pin(f[2]), est=o) for d, f, o in zip(dets, frames, outs)])
+    for k in range(3):
+        assert np.array_equal(outs[k], ref[3 + k])
