@@ -145,25 +145,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v)
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// 2^x on the FMA pipe, for x <= 0: x = n + f with n = floor(x), 2^f from a
-// degree-5 polynomial (coefficients fitted here to 2^f on [0, 1) by weighted
-// least squares on Chebyshev nodes; max relative error 1.6e-7 in FP32, like
-// the SFU's ex2.approx), 2^n added to the exponent field.  Arguments below
-// -126 give 2^-126 p(f), a normal number below 1.2e-38.
-__device__ __forceinline__ float exp2_fma(float x)
-{
-    x = fmaxf(x, -126.f);
-    const float fl = floorf(x);
-    const float f = x - fl;
-    float p = 0.0018762329127639532f;
-    p = fmaf(p, f, 0.00899258442223072f);
-    p = fmaf(p, f, 0.05582360550761223f);
-    p = fmaf(p, f, 0.24015453457832336f);
-    p = fmaf(p, f, 0.6931529641151428f);
-    p = fmaf(p, f, 0.9999999403953552f);
-    return __int_as_float(__float_as_int(p) + (__float2int_rn(fl) << 23));
-}
-
 __device__ __forceinline__ float ex2(float x)
 {
     float y;

@@ -8,8 +8,8 @@
 // product A B^T holds r and m in adjacent columns.  One CTA takes a tile of
 // 128 samples of one job against every chunk of 64 dictionary pairs
 // (UMMA M=128, N=128, FP32 accumulators in tensor memory, double-buffered);
-// the epilogue forms the three distances with FP32 norms, exponentiates (two
-// of the three on the SFU, one on the FMA pipe) and accumulates a_2b K(2b, .) + a_2b+1 K(2b+1, .) for the two soft
+// the epilogue forms the three distances with FP32 norms, exponentiates on
+// the SFU and accumulates a_2b K(2b, .) + a_2b+1 K(2b+1, .) for the two soft
 // outputs of the sample (reference model cpp/lib/apsm/apsm_detect.cu:690-876).
 //
 // Roles (320 threads): warps 0-7 epilogue (warp w: TMEM lanes 32*(w%4)..,
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const float sum = xn + nb.x, re = gv[2 * j], im = gv[2 * j + 1];
                         const float kA = ex2(ew2 * fmaxf(fmaf(-2.f, re, sum), 0.f));
                         const float kP = ex2(ew2 * fmaxf(fmaf(-2.f, im, sum), 0.f));
-                        const float kM = exp2_fma(ew2 * fmaxf(fmaf(2.f, im, sum), 0.f)); // FMA pipe: the SFU is the bound
+                        const float kM = ex2(ew2 * fmaxf(fmaf(2.f, im, sum), 0.f));
                         f0 = fmaf(aw.x, kA, fmaf(aw.y, kM, f0));
                         f1 = fmaf(aw.x, kP, fmaf(aw.y, kA, f1));
                     }
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const float sum = xn + nb.y, re = gv[2 * j + 2], im = gv[2 * j + 3];
                         const float kA = ex2(ew2 * fmaxf(fmaf(-2.f, re, sum), 0.f));
                         const float kP = ex2(ew2 * fmaxf(fmaf(-2.f, im, sum), 0.f));
-                        const float kM = exp2_fma(ew2 * fmaxf(fmaf(2.f, im, sum), 0.f));
+                        const float kM = ex2(ew2 * fmaxf(fmaf(2.f, im, sum), 0.f));
                         f0 = fmaf(aw.z, kA, fmaf(aw.w, kM, f0));
                         f1 = fmaf(aw.z, kP, fmaf(aw.w, kA, f1));
                     }
