@@ -108,6 +108,22 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+# ------------------------------------------------------------- replicas --
+def replica_totals(symbols: int, total_ms: float, e2e_ms: float, world: int, device="cpu"):
+    """Whole-job totals of independent replicas: detected symbols summed over
+    the ranks, timed milliseconds as the maximum over the ranks.  Every rank
+    calls this (a collective when world > 1)."""
+    if world <= 1:
+        return symbols, total_ms, e2e_ms
+    import torch
+
+    s = torch.tensor([float(symbols)], dtype=torch.float64, device=device)
+    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(s, op=torch.distributed.ReduceOp.SUM)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return int(s.item()), float(t[0]), float(t[1])
+
+
 # ------------------------------------------------------- batched (headline) --
 def sweep_algorithmic_bytes(dets, window: int, dict_size: int) -> int:
     """Minimum HBM bytes of one batched training-sweep launch: every kernel-
@@ -203,14 +219,10 @@ def run_batched(args, rank: int, world: int) -> dict | None:
     h2d = sum(d.rx_train.nbytes + d.tx_train.nbytes + d.rx_data.nbytes for d in dets)
     d2h = sum(8 * d.S for d in dets)
 
-    t = torch.tensor([total_ms, sum(e2e_ms)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms, e2e_total = float(t[0]), float(t[1])
+    symbols, total_ms, e2e_total = replica_totals(sum(d.S for d in dets), total_ms, sum(e2e_ms), world, "cuda")
     if rank != 0:
         return None
 
-    symbols = world * sum(d.S for d in dets)
     ms_step = total_ms / args.steps
     sweep = float(np.median(stage["sweep"]))
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}

@@ -14,13 +14,6 @@ namespace apsm {
 
 namespace {
 
-__device__ __forceinline__ float ex2f_approx(float x)
-{
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
 constexpr int kColGroup = 8;   // columns per block
 constexpr int kColRows = 128;  // column entries per block pass (= threads)
 
@@ -32,7 +25,7 @@ __global__ void __launch_bounds__(kColRows)
     const int n0 = jb.n_first + blockIdx.x * kColGroup;
     if (n0 >= nP || N > smem_n) return; // shared memory is sized for smem_n antennas
     const int nc = min(kColGroup, nP - n0);
-    const float ew2 = jb.ew * 1.4426950408889634f, wG = cm.wG, wL = cm.wL; // exp(ew d) = 2^(ew log2(e) d)
+    const float ew = jb.ew, wG = cm.wG, wL = cm.wL;
     const int tid = threadIdx.x;
 
     extern __shared__ float2 smk[];
@@ -81,9 +74,9 @@ __global__ void __launch_bounds__(kColRows)
             const int n = n0 + c;
             if (b < col_begin(n, capP) || b >= col_end(n, qP, nP)) continue;
             const float s = nb + nn[c];
-            const float A = wG * ex2f_approx(ew2 * fmaxf(fmaf(-2.f, re[c], s), 0.f));
-            const float Bp = wG * ex2f_approx(ew2 * fmaxf(fmaf(-2.f, im[c], s), 0.f));
-            const float Bm = wG * ex2f_approx(ew2 * fmaxf(fmaf(2.f, im[c], s), 0.f));
+            const float A = wG * expf(ew * fmaxf(fmaf(-2.f, re[c], s), 0.f));
+            const float Bp = wG * expf(ew * fmaxf(fmaf(-2.f, im[c], s), 0.f));
+            const float Bm = wG * expf(ew * fmaxf(fmaf(2.f, im[c], s), 0.f));
             const long long off = column_prefix(n, qP, nP, capP) - jb.kc_base + (b - col_begin(n, capP));
             const_cast<float4*>(jb.Kc)[off] = make_float4(fmaf(wL, re[c], A), fmaf(wL, im[c], Bp), fmaf(-wL, im[c], Bm), 0.f);
         }
