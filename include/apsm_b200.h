@@ -77,6 +77,30 @@ void apsm_destroy(apsm_detector* h);
 apsm_status apsm_train(apsm_detector* h, const float* rx, const float* tx, uint32_t P, float* ms);
 
 /*
+ * Training with a per-step history: NomaDetector::train with a NomaValSet
+ * (noma_detector.cuh:69, noma_train_history.cuh:64-99; recorded by
+ * apsm_train.cu:147-156, computed as noma_train_history.cu:65-248).  Trains
+ * exactly like apsm_train and, for the model after every step, records EVM,
+ * SER and BER of this call's training symbols and of the validation set
+ * rx_val (N x S complex) / tx_val (num_users x S complex, S > 0).
+ * history: num_users x steps x 6 floats, per step train EVM, SER, BER,
+ * validation EVM, SER, BER; steps = apsm_train_steps(h, P), which must be
+ * <= max_steps (else APSM_ERR_INVALID_ARGUMENT before any work).
+ * bits_per_symbol / modulation_scale: Modulation::getBitPerSymbol / getScale
+ * of the symbols (the reference's NomaTrainHistory constructor arguments).
+ * An LLS detector trains and records nothing (*n_steps = 0), as the
+ * reference's LLS detector ignores the validation set (lls_detector.cu:136).
+ */
+apsm_status apsm_train_history(apsm_detector* h, const float* rx, const float* tx, uint32_t P, const float* rx_val,
+                               const float* tx_val, uint32_t S, uint32_t bits_per_symbol, float modulation_scale,
+                               float* history, uint32_t max_steps, uint32_t* n_steps, float* ms);
+
+/* Training steps (history rows per user) a train call with P pilots runs on
+ * the detector's current state; 0 for LLS detectors.  No reference
+ * counterpart (its history vectors grow as they are filled). */
+uint32_t apsm_train_steps(const apsm_detector* h, uint32_t P);
+
+/*
  * Detection of S data symbols: NomaDetector::detect (noma_detector.cuh:70;
  * apsm_noma_detector.cu:130-143 -> apsm_detect.cu:948-992).
  * rx: N x S complex, est: num_users x S complex (written).

@@ -4,6 +4,7 @@
 // Mirrors fraunhoferhhi/libapsm:
 //   class NomaDetector            cpp/lib/noma/noma_detector.cuh:65-75
 //   NomaDetectorFactory::build    cpp/lib/noma/noma_detector_factory.cu:57-65
+//   NomaTrainHistory, NomaValSet  cpp/lib/noma/noma_train_history.cuh:64-99
 //   sample typedefs               cpp/lib/noma/types.cuh:69-100
 // Same signatures and semantics: train/detect return the GPU time in ms,
 // detect resizes estData, configuration errors throw std::invalid_argument
@@ -16,9 +17,13 @@
 
 #include <complex>
 #include <cstdint>
+#include <fstream>
+#include <functional>
 #include <memory>
+#include <optional>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 namespace apsm_b200 {
@@ -30,10 +35,43 @@ typedef std::complex<RealSample> ComplexSample;
 typedef std::vector<ComplexSample> ComplexSampleVector;
 typedef std::vector<ComplexSampleVector> ComplexSampleMatrix;
 
+// Per-step metrics of a training call with a validation set: after every
+// training step EVM, SER and BER of the training symbols and of the
+// validation set under that step's model (computed on the GPU by
+// apsm_train_history).  toCsv writes the reference's CSV
+// (noma_train_history.cu:237-248).
+class NomaTrainHistory {
+public:
+    NomaTrainHistory(uint32_t bitPerSymbol, float modulationScale)
+        : bitPerSymbol(bitPerSymbol), modulationScale(modulationScale)
+    {
+    }
+    NomaTrainHistory() = delete;
+    NomaTrainHistory(const NomaTrainHistory&) = delete;
+    NomaTrainHistory& operator=(const NomaTrainHistory&) = delete;
+
+    void toCsv(const std::string& filename) const
+    {
+        std::ofstream file(filename, std::ios::out | std::ios::trunc);
+        file << "step,train_evm,train_ser,train_ber,val_evm,val_ser,val_ber" << std::endl;
+        for (size_t i = 0; i < evmTrain.size(); ++i) {
+            file << i << "," << evmTrain[i] << "," << serTrain[i] << "," << berTrain[i] << ",";
+            file << evmVal[i] << "," << serVal[i] << "," << berVal[i] << std::endl;
+        }
+    }
+
+    RealSampleVector evmTrain, evmVal, serTrain, serVal, berTrain, berVal;
+    const uint32_t bitPerSymbol;
+    const float modulationScale;
+};
+
+typedef std::optional<std::tuple<NomaTrainHistory&, const ComplexSampleMatrix&, const ComplexSampleVector&>> NomaValSet;
+
 class NomaDetector {
 public:
     virtual ~NomaDetector() {}
-    virtual float train(const ComplexSampleMatrix& rxSigTraining, const ComplexSampleVector& txSigTraining) = 0;
+    virtual float train(const ComplexSampleMatrix& rxSigTraining, const ComplexSampleVector& txSigTraining,
+                        NomaValSet valSet = std::nullopt) = 0;
     virtual float detect(const ComplexSampleMatrix& rxSigData, ComplexSampleVector& estData) = 0;
     virtual void resetState() = 0;
 };
@@ -79,10 +117,39 @@ public:
     ApsmB200Detector(const ApsmB200Detector&) = delete;
     ApsmB200Detector& operator=(const ApsmB200Detector&) = delete;
 
-    float train(const ComplexSampleMatrix& rxSigTraining, const ComplexSampleVector& txSigTraining) override
+    float train(const ComplexSampleMatrix& rxSigTraining, const ComplexSampleVector& txSigTraining,
+                NomaValSet valSet = std::nullopt) override
     {
         if (numUsers_ != 1) throw std::invalid_argument("multi-user detector: use trainUsers");
-        return trainUsers(rxSigTraining, {txSigTraining});
+        if (!valSet) return trainUsers(rxSigTraining, {txSigTraining});
+        NomaTrainHistory& hist = std::get<0>(*valSet);
+        size_t P = 0, S = 0;
+        std::vector<ComplexSample> rx = detail::flatten(rxSigTraining, numAntennas_, &P);
+        std::vector<ComplexSample> rxv = detail::flatten(std::get<1>(*valSet), numAntennas_, &S);
+        const ComplexSampleVector& txv = std::get<2>(*valSet);
+        if (txSigTraining.size() != P) throw std::invalid_argument("pilot vector length differs from rxSigTraining");
+        if (txv.size() != S) throw std::invalid_argument("validation symbols differ in length from their samples");
+        if (P == 0) throw std::invalid_argument("no training samples");
+        const uint32_t steps = apsm_train_steps(h_, uint32_t(P));
+        std::vector<float> out(size_t(steps) * 6 + 6);
+        uint32_t n = 0;
+        float ms = 0.f;
+        detail::throw_status(apsm_train_history(h_, reinterpret_cast<const float*>(rx.data()),
+                                                reinterpret_cast<const float*>(txSigTraining.data()), uint32_t(P),
+                                                reinterpret_cast<const float*>(rxv.data()),
+                                                reinterpret_cast<const float*>(txv.data()), uint32_t(S),
+                                                hist.bitPerSymbol, hist.modulationScale, out.data(), steps, &n, &ms),
+                             apsm_last_error(h_));
+        for (uint32_t t = 0; t < n; ++t) {
+            const float* r = &out[size_t(t) * 6];
+            hist.evmTrain.push_back(r[0]);
+            hist.serTrain.push_back(r[1]);
+            hist.berTrain.push_back(r[2]);
+            hist.evmVal.push_back(r[3]);
+            hist.serVal.push_back(r[4]);
+            hist.berVal.push_back(r[5]);
+        }
+        return ms;
     }
 
     float detect(const ComplexSampleMatrix& rxSigData, ComplexSampleVector& estData) override

@@ -41,6 +41,9 @@ SIGNATURES = [
     ("apsm_create", ctypes.c_int, [ctypes.c_char_p, _U32, _U32, ctypes.POINTER(_P), ctypes.c_char_p, ctypes.c_size_t]),
     ("apsm_destroy", None, [_P]),
     ("apsm_train", ctypes.c_int, [_P, _P, _P, _U32, _F]),
+    ("apsm_train_history", ctypes.c_int, [_P, _P, _P, _U32, _P, _P, _U32, _U32, ctypes.c_float, _P, _U32,
+                                          ctypes.POINTER(_U32), _F]),
+    ("apsm_train_steps", _U32, [_P, _U32]),
     ("apsm_detect", ctypes.c_int, [_P, _P, _U32, _P, _F]),
     ("apsm_reset", ctypes.c_int, [_P]),
     ("apsm_train_device", ctypes.c_int, [_P, _P, _P, _U32, _P]),

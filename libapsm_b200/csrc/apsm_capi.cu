@@ -297,6 +297,26 @@ extern "C" apsm_status apsm_train(apsm_detector* h, const float* rx, const float
     return h->train_host(reinterpret_cast<const float2*>(rx), reinterpret_cast<const float2*>(tx), P, ms);
 }
 
+extern "C" apsm_status apsm_train_history(apsm_detector* h, const float* rx, const float* tx, uint32_t P,
+                                          const float* rx_val, const float* tx_val, uint32_t S,
+                                          uint32_t bits_per_symbol, float modulation_scale, float* history,
+                                          uint32_t max_steps, uint32_t* n_steps, float* ms)
+{
+    if (!h) return APSM_ERR_INVALID_ARGUMENT;
+    if (n_steps) *n_steps = 0;
+    if (!rx || !tx || P == 0) return fail(h, APSM_ERR_INVALID_ARGUMENT, "train: null buffer or P == 0");
+    if (!rx_val || !tx_val || S == 0) return fail(h, APSM_ERR_INVALID_ARGUMENT, "train history: empty validation set");
+    if (bits_per_symbol == 0 || bits_per_symbol > 16 || (bits_per_symbol > 1 && bits_per_symbol % 2) ||
+        !(modulation_scale > 0.f))
+        return fail(h, APSM_ERR_INVALID_ARGUMENT, "train history: invalid modulation (bits per symbol / scale)");
+    if (!history && apsm_train_steps(h, P) > 0) return fail(h, APSM_ERR_INVALID_ARGUMENT, "train history: null output");
+    return h->train_history_host(reinterpret_cast<const float2*>(rx), reinterpret_cast<const float2*>(tx), P,
+                                 reinterpret_cast<const float2*>(rx_val), reinterpret_cast<const float2*>(tx_val), S,
+                                 bits_per_symbol, modulation_scale, history, max_steps, n_steps, ms);
+}
+
+extern "C" uint32_t apsm_train_steps(const apsm_detector* h, uint32_t P) { return h ? h->train_steps(P) : 0; }
+
 extern "C" apsm_status apsm_detect(apsm_detector* h, const float* rx, uint32_t S, float* est, float* ms)
 {
     if (!h) return APSM_ERR_INVALID_ARGUMENT;

@@ -112,8 +112,10 @@ apsm_status apsm_detector::reset()
     return APSM_OK;
 }
 
-apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_t P, cudaStream_t s, float* ms)
+apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_t P, cudaStream_t s, float* ms,
+                                 HistoryRequest* hist)
 {
+    if (hist) hist->n_steps = 0;
     if (is_lls || cfg.lls_init) {
         // LlsNomaDetector::train (lls_detector.cu:136-161) on the unshuffled pilots;
         // for llsInitialization (apsm_noma_detector.cu:98-99, 331-346) w = w_lls / wL
@@ -170,6 +172,34 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
     APSM_CK(uy.ensure(size_t(U) * nU));
     APSM_CK(ua.ensure(size_t(U) * nU));
 
+    const int T_steps = int(h_steps.size());
+    uint32_t hist_nE = 0;
+    int hist_tiles = 0;
+    if (hist && T_steps > 0) {
+        if (uint32_t(T_steps) > hist->max_steps) {
+            last_error = "train history: " + std::to_string(T_steps) + " steps, the output holds " +
+                         std::to_string(hist->max_steps);
+            return APSM_ERR_INVALID_ARGUMENT;
+        }
+        hist_nE = 2 * P + 2 * hist->S;
+        hist_tiles = history_tiles(int(hist_nE));
+        const size_t UT = size_t(U) * T_steps;
+        const size_t floats = UT * (q2 + D + nU + size_t(hist_tiles) * 6) + size_t(U) * nU + size_t(hist_nE) * Dp +
+                              size_t(U) * hist_nE;
+        if (floats * sizeof(float) > (size_t(8) << 30)) {
+            last_error = "train history needs " + std::to_string(floats * sizeof(float) >> 20) +
+                         " MiB of scratch (steps x universe rows); more than the 8 GiB it may take";
+            return APSM_ERR_UNSUPPORTED;
+        }
+        APSM_CK(h_snap_a.ensure(UT * q2));
+        APSM_CK(h_snap_w.ensure(UT * D));
+        APSM_CK(h_a0.ensure(size_t(U) * nU));
+        APSM_CK(h_A.ensure(UT * nU));
+        APSM_CK(h_E.ensure(size_t(hist_nE) * Dp));
+        APSM_CK(h_Ey.ensure(size_t(U) * hist_nE));
+        APSM_CK(h_part.ensure(UT * hist_tiles * 6));
+    }
+
     const int* d_perm = nullptr;
     if (cfg.shuffle) {
         std::vector<int> pm = shuffle_permutation(P);
@@ -199,6 +229,8 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         APSM_CK(cudaGetLastError());
     }
 
+    if (hist_nE > 0) // coefficients before the first step (rows of earlier calls; new rows 0)
+        APSM_CK(cudaMemcpyAsync(h_a0.p, ua.p, sizeof(float) * size_t(U) * nU, cudaMemcpyDeviceToDevice, s));
     APSM_CK(cudaEventRecord(ev0, s));
     if (!h_steps.empty()) {
         const int T = int(h_steps.size());
@@ -251,6 +283,8 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         ta.y_stride = nU;
         ta.a_stride = nU;
         ta.mp = mp;
+        ta.snap_a = hist_nE > 0 ? h_snap_a.p : nullptr;
+        ta.snap_w = hist_nE > 0 ? h_snap_w.p : nullptr;
 
         ta.XP = int(Dp) + 4; // padded window-row pitch (conflict-free column reads)
         ta.err = train_err.p;
@@ -377,6 +411,52 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         last_train_staged = best.staged;
     }
 sweep_done:
+    if (hist_nE > 0) {
+        // evaluation rows: this call's training rows (universe order), then the validation samples
+        APSM_CK(cudaMemcpyAsync(h_E.p, uX.p + size_t(used) * Dp, sizeof(float) * size_t(rows_new) * Dp,
+                                cudaMemcpyDeviceToDevice, s));
+        APSM_CK(cudaMemcpy2DAsync(h_Ey.p, sizeof(float) * hist_nE, uy.p + used, sizeof(float) * nU,
+                                  sizeof(float) * rows_new, U, cudaMemcpyDeviceToDevice, s));
+        dim3 grid((hist->S + kPackSamples - 1) / kPackSamples);
+        pack_rows_kernel<<<grid, 256, sizeof(float2) * N * kPackSamples, s>>>(hist->rx_val, int(N), int(hist->S),
+                                                                            nullptr, h_E.p, int(Dp), int(rows_new),
+                                                                            nullptr);
+        APSM_CK(cudaGetLastError());
+        const int nt = int(hist->S * U);
+        gather_targets_kernel<<<(nt + 255) / 256, 256, 0, s>>>(hist->tx_val, int(hist->S), int(U), nullptr, h_Ey.p,
+                                                               hist_nE, int(rows_new));
+        APSM_CK(cudaGetLastError());
+        HistoryArgs ha;
+        ha.steps = steps.p;
+        ha.n_steps = T_steps;
+        ha.snap_a = h_snap_a.p;
+        ha.snap_w = h_snap_w.p;
+        ha.a0 = h_a0.p;
+        ha.a0_stride = nU;
+        ha.used_before = int(used);
+        ha.nU = int(nU);
+        ha.cap = int(cap);
+        ha.q2 = int(q2);
+        ha.D = int(D);
+        ha.Dp = int(Dp);
+        ha.users = int(U);
+        ha.A = h_A.p;
+        ha.X = uX.p;
+        ha.E = h_E.p;
+        ha.Ey = h_Ey.p;
+        ha.nE = int(hist_nE);
+        ha.n_train = int(rows_new);
+        ha.mp = mp;
+        ha.bps = int(hist->bps);
+        ha.mod_scale = hist->mod_scale;
+        ha.rev_scale = float(1.0 / double(hist->mod_scale));
+        ha.max_val = float((1u << (hist->bps / 2)) - 1u) * hist->mod_scale;
+        ha.n_tiles = hist_tiles;
+        ha.part = h_part.p;
+        ha.out = hist->out;
+        APSM_CK(launch_history(ha, s));
+        hist->n_steps = uint32_t(T_steps);
+    }
     APSM_CK(cudaEventRecord(ev1, s));
 
     // the dictionary after the sweep is the last min(final_hi, cap) universe rows
@@ -455,6 +535,54 @@ apsm_status apsm_detector::train_host(const float2* rx, const float2* tx, uint32
     APSM_CK(cudaStreamSynchronize(stream));
     st = check_train_error();
     if (st != APSM_OK) return st;
+    if (ms) *ms = t;
+    return APSM_OK;
+}
+
+uint32_t apsm_detector::train_steps(uint32_t P) const
+{
+    if (is_lls || P == 0) return 0;
+    int final_hi = 0;
+    return uint32_t(build_schedule(cfg, used, P, cap, &final_hi).size());
+}
+
+apsm_status apsm_detector::train_history_host(const float2* rx, const float2* tx, uint32_t P, const float2* rx_val,
+                                              const float2* tx_val, uint32_t S, uint32_t bps, float mod_scale,
+                                              float* history, uint32_t max_steps, uint32_t* n_steps, float* ms)
+{
+    const uint32_t T = train_steps(P);
+    if (n_steps) *n_steps = T;
+    if (T > max_steps) {
+        last_error = "train history: " + std::to_string(T) + " steps, the output holds " + std::to_string(max_steps);
+        return APSM_ERR_INVALID_ARGUMENT;
+    }
+    APSM_CK(rx_stage.ensure(size_t(N) * P));
+    APSM_CK(tx_stage.ensure(size_t(U) * P));
+    APSM_CK(h_rx.ensure(size_t(N) * S));
+    APSM_CK(h_tx.ensure(size_t(U) * S));
+    APSM_CK(h_out.ensure(size_t(U) * std::max<uint32_t>(T, 1) * 6));
+    APSM_CK(cudaMemcpyAsync(rx_stage.p, rx, sizeof(float2) * size_t(N) * P, cudaMemcpyHostToDevice, stream));
+    APSM_CK(cudaMemcpyAsync(tx_stage.p, tx, sizeof(float2) * size_t(U) * P, cudaMemcpyHostToDevice, stream));
+    APSM_CK(cudaMemcpyAsync(h_rx.p, rx_val, sizeof(float2) * size_t(N) * S, cudaMemcpyHostToDevice, stream));
+    APSM_CK(cudaMemcpyAsync(h_tx.p, tx_val, sizeof(float2) * size_t(U) * S, cudaMemcpyHostToDevice, stream));
+    HistoryRequest req;
+    req.rx_val = h_rx.p;
+    req.tx_val = h_tx.p;
+    req.S = S;
+    req.bps = bps;
+    req.mod_scale = mod_scale;
+    req.out = h_out.p;
+    req.max_steps = T;
+    float t = 0.f;
+    apsm_status st = train(rx_stage.p, tx_stage.p, P, stream, &t, &req);
+    if (st != APSM_OK) return st;
+    if (req.n_steps > 0)
+        APSM_CK(cudaMemcpyAsync(history, h_out.p, sizeof(float) * size_t(U) * req.n_steps * 6, cudaMemcpyDeviceToHost,
+                                stream));
+    APSM_CK(cudaStreamSynchronize(stream));
+    st = check_train_error();
+    if (st != APSM_OK) return st;
+    if (n_steps) *n_steps = req.n_steps;
     if (ms) *ms = t;
     return APSM_OK;
 }

@@ -66,6 +66,19 @@ template <class T> struct DevBuf {
     }
 };
 
+// Validation set and output of a training call that records its per-step
+// history (device buffers).
+struct HistoryRequest {
+    const float2* rx_val; // N x S antenna-major
+    const float2* tx_val; // users x S
+    uint32_t S = 0;
+    uint32_t bps = 0;
+    float mod_scale = 0.f;
+    float* out = nullptr; // users x n_steps x 6
+    uint32_t max_steps = 0;
+    uint32_t n_steps = 0; // set by train(): steps recorded
+};
+
 struct GramWorkspace; // tensor-core detection operands (kernels_detect_gram.cu)
 struct LlsWorkspace;  // least-squares solver state (kernels_lls.cu)
 
@@ -93,6 +106,10 @@ struct apsm_detector {
     apsm::DevBuf<int> train_err; // set by the sweep when a bounded wait expired
     apsm::DevBuf<int> perm;
     apsm::DevBuf<float2> rx_stage, tx_stage, est_stage;
+    // training-history scratch: per-step snapshots, initial coefficients, dense
+    // per-step coefficients, evaluation rows / targets, partial sums, output
+    apsm::DevBuf<float> h_snap_a, h_snap_w, h_a0, h_A, h_E, h_Ey, h_part, h_out;
+    apsm::DevBuf<float2> h_rx, h_tx;
     apsm::GramWorkspace* gram = nullptr;
     apsm::LlsWorkspace* lls = nullptr; // least-squares detector / llsInitialization
     bool is_lls = false;               // "otype": "LLS"
@@ -106,7 +123,12 @@ struct apsm_detector {
     ~apsm_detector();
     apsm_status init(const apsm::Config& c, uint32_t num_antennas, uint32_t num_users);
     apsm_status reset();
-    apsm_status train(const float2* d_rx, const float2* d_tx, uint32_t P, cudaStream_t s, float* ms);
+    apsm_status train(const float2* d_rx, const float2* d_tx, uint32_t P, cudaStream_t s, float* ms,
+                      apsm::HistoryRequest* hist = nullptr);
+    apsm_status train_history_host(const float2* rx, const float2* tx, uint32_t P, const float2* rx_val,
+                                   const float2* tx_val, uint32_t S, uint32_t bps, float mod_scale, float* history,
+                                   uint32_t max_steps, uint32_t* n_steps, float* ms);
+    uint32_t train_steps(uint32_t P) const;
     apsm_status detect(const float2* d_rx, uint32_t S, float2* d_est, cudaStream_t s);
     apsm_status train_host(const float2* rx, const float2* tx, uint32_t P, float* ms);
     apsm_status detect_host(const float2* rx, uint32_t S, float2* est, float* ms);

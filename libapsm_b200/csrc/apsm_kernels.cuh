@@ -39,7 +39,38 @@ struct TrainArgs {
     ModelParams mp;
     unsigned long long* prof; // phase timestamps (profiling builds only), kProfSteps x kProfMarks
     int* err;                 // set to 1 when a bounded wait expired
+    float* snap_a;            // users x n_steps x q2: the active rows' coefficients after each step (nullptr: off)
+    float* snap_w;            // users x n_steps x D: the linear weights after each step
 };
+
+// Training history (kernels_history.cu): every step's model evaluated on the
+// call's training rows and a validation set after the sweep.
+struct HistoryArgs {
+    const TrainStep* steps; // n_steps (the sweep's schedule)
+    int n_steps;
+    const float* snap_a;    // users x n_steps x q2: active-row coefficients after each step
+    const float* snap_w;    // users x n_steps x D: linear weights after each step
+    const float* a0;        // users x a0_stride: coefficients of the rows present before the call
+    size_t a0_stride;
+    int used_before, nU, cap, q2, D, Dp, users;
+    float* A;               // users x n_steps x nU: dense coefficients of every step
+    const float* X;         // universe rows nU x Dp
+    const float* E;         // evaluation rows nE x Dp: the call's training rows, then the validation rows
+    const float* Ey;        // users x nE targets of the evaluation rows
+    int nE, n_train;        // evaluation rows (even), of which the first n_train are training rows
+    ModelParams mp;
+    int bps;                // bits per symbol of the modulation
+    float mod_scale;        // constellation scale (unit energy)
+    float rev_scale;        // float(1 / scale), as the reference passes it
+    float max_val;          // outermost constellation coordinate ((2^(bps/2) - 1) scale)
+    int n_tiles;            // evaluation-row tiles
+    float* part;            // users x n_steps x n_tiles x 6 partial sums
+    float* out;             // users x n_steps x 6: train EVM, SER, BER, validation EVM, SER, BER
+};
+
+size_t history_eval_smem(int D);
+int history_tiles(int nE);
+cudaError_t launch_history(const HistoryArgs& h, cudaStream_t s);
 
 constexpr int kProfSteps = 4096;
 constexpr int kProfMarks = 8;

@@ -326,6 +326,16 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
             acc = __fadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, 4));
             if (d < D && g == 0) w_s[d] = __fadd_rn(w_s[d], acc);
         }
+        if (args.snap_a) {
+            // training history: the model after this step (every CTA holds the same copy)
+            __syncthreads();
+            if (rank == 0) {
+                float* sa = args.snap_a + (size_t(user) * n_steps + t) * q2;
+                for (int i = tid; i < st.n_active; i += nthreads) sa[i] = a_ring[(start + i) & amask];
+                float* sw = args.snap_w + (size_t(user) * n_steps + t) * D;
+                for (int d = tid; d < D; d += nthreads) sw[d] = w_s[d];
+            }
+        }
 #pragma unroll
         for (int k = 0; k < kLookahead + 1; ++k) sv[k] = sv[k + 1];
         sv[kLookahead + 1] = next;

@@ -419,6 +419,14 @@ __global__ void __launch_bounds__(kThreads, 1) train_inc_kernel(TrainArgs args)
             }
         }
         __syncthreads(); // Kwin entries complete
+        if (args.snap_a && rank == 0) {
+            // training history: the model after this step (a_j and w are final here and not
+            // written again before the next step's barriers)
+            float* sa = args.snap_a + (size_t(user) * n_steps + t) * args.q2;
+            for (int i = tid; i < st.n_active; i += kThreads) sa[i] = a_ring[(start + i) & amask];
+            float* sw = args.snap_w + (size_t(user) * n_steps + t) * D;
+            for (int d = tid; d < D; d += kThreads) sw[d] = w_s[d];
+        }
         // (B3) owned column sums: g += sum_si cs[si] Kwin[si][so]
         for (int idx = tid; idx < kParts * NSOp; idx += kThreads) {
             const int part = idx / NSOp, so = idx % NSOp;

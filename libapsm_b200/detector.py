@@ -97,8 +97,15 @@ class NomaDetector:
         raise ApsmError(st, msg)
 
     # -- the reference API ------------------------------------------------
-    def train(self, rx_sig_training: Any, tx_sig_training: Any) -> float:
-        """NomaDetector::train: rx (N, P) complex, tx (P,) or (users, P). Returns GPU ms."""
+    def train(self, rx_sig_training: Any, tx_sig_training: Any, val_set: tuple | None = None) -> float:
+        """NomaDetector::train: rx (N, P) complex, tx (P,) or (users, P). Returns GPU ms.
+
+        val_set = (history, rx_val, tx_val) mirrors the reference's NomaValSet
+        (noma_train_history.cuh:99): ``history`` is a NomaTrainHistory that
+        receives, for the model after every training step, EVM / SER / BER of
+        the training symbols and of the validation set rx_val (N, S) / tx_val
+        (S,) or (users, S).  With several users the history keeps user 0's
+        rows; ``history.per_user`` holds all of them."""
         rx = _as_complex_matrix(rx_sig_training, self.num_antennas, "rxSigTraining")
         P = rx.shape[1]
         tx = _as_complex_matrix(np.atleast_2d(tx_sig_training), self.num_users, "txSigTraining")
@@ -107,7 +114,25 @@ class NomaDetector:
         if P == 0:
             raise ValueError("no training samples")
         ms = ctypes.c_float(0.0)
-        self._check(self._lib.apsm_train(self._h, rx.ctypes.data, tx.ctypes.data, P, ctypes.byref(ms)))
+        if val_set is None:
+            self._check(self._lib.apsm_train(self._h, rx.ctypes.data, tx.ctypes.data, P, ctypes.byref(ms)))
+            return float(ms.value)
+        history, rx_val, tx_val = val_set
+        rxv = _as_complex_matrix(rx_val, self.num_antennas, "rxSigVal")
+        S = rxv.shape[1]
+        txv = _as_complex_matrix(np.atleast_2d(tx_val), self.num_users, "txSigVal")
+        if txv.shape[1] != S:
+            raise ValueError(f"txSigVal has {txv.shape[1]} samples, rxSigVal {S}")
+        steps = int(self._lib.apsm_train_steps(self._h, P))
+        out = np.zeros((self.num_users, max(steps, 1), 6), dtype=np.float32)
+        n = ctypes.c_uint32(0)
+        self._check(self._lib.apsm_train_history(self._h, rx.ctypes.data, tx.ctypes.data, P, rxv.ctypes.data,
+                                                 txv.ctypes.data, S, int(history.bit_per_symbol),
+                                                 float(history.modulation_scale), out.ctypes.data, steps,
+                                                 ctypes.byref(n), ctypes.byref(ms)))
+        # the library writes users x n x 6 contiguously
+        flat = out.reshape(-1)[: self.num_users * n.value * 6].reshape(self.num_users, n.value, 6)
+        history.extend(flat)
         return float(ms.value)
 
     def detect(self, rx_sig_data: Any) -> tuple[np.ndarray, float]:

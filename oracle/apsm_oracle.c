@@ -305,7 +305,129 @@ static void step_f64(apsm_oracle* o, uint32_t start, uint32_t n_active, uint32_t
  * block b updates logical row used - Wk + b (apsm_train.cu:118-119, 333-346).
  * For a call that appends to an existing dictionary the launch count also
  * counts the rows already present, so the window slides on continuously. */
+/* Per-step history (NomaTrainHistory, cpp/lib/noma/noma_train_history.cu:65-248;
+ * recorded by apsm_train.cu:147-156 after every step): the training rows of this
+ * call and the validation samples are detected with the current model and EVM,
+ * SER and BER of both are computed in the reference's float order. */
+typedef struct {
+    const float* rx_val; /* antenna-major complex, S samples */
+    const float* tx_val; /* S complex */
+    uint32_t S, bps;
+    float mod_scale;
+    float* out;          /* max_steps x 6: train evm, ser, ber, val evm, ser, ber */
+    uint32_t max_steps, n;
+} history_ctx;
+
+/* demap1D (noma_train_history.cu:186-196): round half away from zero, clamp, Gray code. */
+static uint32_t hist_demap1d(float x, uint32_t num_symbols)
+{
+    float v = (x + (float)num_symbols - 1.f) / 2.f;
+    int32_t xi = (int32_t)roundf(v);
+    if (xi < 0) xi = 0;
+    if (xi > (int32_t)num_symbols - 1) xi = (int32_t)num_symbols - 1;
+    return (uint32_t)(xi ^ (xi >> 1));
+}
+
+static int hist_symbol_error_1d(float t, float h, float s, float mx)
+{
+    return fabsf(t - h) > s && !(h > +mx && t > +mx - s) && !(h < -mx && t < -mx + s);
+}
+
+/* kernelComputeEvm / kernelComputeSer(Bpsk) / kernelComputeBer (noma_train_history.cu:96-235):
+ * one block of LANES threads, thread l sums symbols l, l+LANES, ... then a halving tree.
+ * y_true / y_hat: n symbols, (re, im) interleaved. */
+static void hist_metrics(const float* y_true, const float* y_hat, uint32_t n, uint32_t bps, float mod_scale,
+                         float* evm, float* ser, float* ber)
+{
+    float se[LANES], ss[LANES], sb[LANES];
+    memset(se, 0, sizeof(se));
+    memset(ss, 0, sizeof(ss));
+    memset(sb, 0, sizeof(sb));
+    const float mx = (float)((1u << (bps / 2)) - 1u) * mod_scale;
+    const float rev = (float)(1.0 / (double)mod_scale);
+    const uint32_t nsym = bps == 1 ? 2u : 1u << (bps / 2);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t l = i % LANES;
+        const float dr = y_true[2 * i] - y_hat[2 * i];
+        const float di = y_true[2 * i + 1] - y_hat[2 * i + 1];
+        se[l] = se[l] + fmaf(dr, dr, di * di);
+        int err;
+        if (bps == 1) err = signbit(y_true[2 * i]) != signbit(y_hat[2 * i]);
+        else err = hist_symbol_error_1d(y_true[2 * i], y_hat[2 * i], mod_scale, mx) ||
+                   hist_symbol_error_1d(y_true[2 * i + 1], y_hat[2 * i + 1], mod_scale, mx);
+        ss[l] = ss[l] + (float)err;
+        uint32_t b = (uint32_t)__builtin_popcount(hist_demap1d(y_true[2 * i] * rev, nsym) ^
+                                                  hist_demap1d(y_hat[2 * i] * rev, nsym));
+        sb[l] = sb[l] + (float)b;
+        if (bps > 1) {
+            b = (uint32_t)__builtin_popcount(hist_demap1d(y_true[2 * i + 1] * rev, nsym) ^
+                                             hist_demap1d(y_hat[2 * i + 1] * rev, nsym));
+            sb[l] = sb[l] + (float)b;
+        }
+    }
+    for (uint32_t size = LANES / 2; size > 0; size /= 2)
+        for (uint32_t l = 0; l < size; ++l) {
+            se[l] = se[l] + se[l + size];
+            ss[l] = ss[l] + ss[l + size];
+            sb[l] = sb[l] + sb[l + size];
+        }
+    *evm = sqrtf(se[0] / (float)n);
+    *ser = ss[0] / (float)n;
+    *ber = sb[0] / (float)(n * bps);
+}
+
+static void hist_record(apsm_oracle* o, history_ctx* h, const float* staged, const float* ys, uint32_t rows)
+{
+    if (h->n >= h->max_steps) {
+        h->n++;
+        return;
+    }
+    const uint32_t D = o->D;
+    const uint32_t nv = 2 * h->S;
+    float* est = (float*)malloc((size_t)(rows + nv) * sizeof(float));
+    float* yv = (float*)malloc((size_t)nv * sizeof(float));
+#pragma omp parallel
+    {
+        float xf[256];
+#pragma omp for schedule(static)
+        for (uint32_t r = 0; r < rows + nv; ++r) {
+            const float* x = &staged[(size_t)r * D];
+            if (r >= rows) {
+                dedup_column(h->rx_val, o->n_ant, h->S, r - rows, xf);
+                x = xf;
+            }
+            est[r] = detect_one_f32(o, x);
+        }
+    }
+    for (uint32_t c = 0; c < nv; ++c) yv[c] = h->tx_val[c];
+    float* out = &h->out[(size_t)h->n * 6];
+    hist_metrics(ys, est, rows / 2, h->bps, h->mod_scale, &out[0], &out[1], &out[2]);
+    hist_metrics(yv, est + rows, h->S, h->bps, h->mod_scale, &out[3], &out[4], &out[5]);
+    free(est);
+    free(yv);
+    h->n++;
+}
+
+static int train_impl(apsm_oracle* o, const float* rx, const float* tx, uint32_t P, history_ctx* hist);
+
 int apsm_oracle_train(apsm_oracle* o, const float* rx, const float* tx, uint32_t P)
+{
+    return train_impl(o, rx, tx, P, NULL);
+}
+
+int apsm_oracle_train_history(apsm_oracle* o, const float* rx, const float* tx, uint32_t P, const float* rx_val,
+                              const float* tx_val, uint32_t S, uint32_t bps, float mod_scale, float* history,
+                              uint32_t max_steps, uint32_t* n_steps)
+{
+    if (!o || o->prec != APSM_ORACLE_F32 || !rx_val || !tx_val || S == 0 || bps == 0 || !history) return 1;
+    history_ctx h = {rx_val, tx_val, S, bps, mod_scale, history, max_steps, 0};
+    int st = train_impl(o, rx, tx, P, &h);
+    if (n_steps) *n_steps = h.n;
+    if (st == 0 && h.n > max_steps) return 3;
+    return st;
+}
+
+static int train_impl(apsm_oracle* o, const float* rx, const float* tx, uint32_t P, history_ctx* hist)
 {
     if (!o || !rx || !tx || P == 0) return 1;
     const apsm_oracle_params* p = &o->par;
@@ -340,6 +462,7 @@ int apsm_oracle_train(apsm_oracle* o, const float* rx, const float* tx, uint32_t
             if (n_active == 0) continue;
             if (o->prec == APSM_ORACLE_F32) step_f32(o, start, n_active, wk, ff, cf);
             else step_f64(o, start, n_active, wk, fd, cd);
+            if (hist) hist_record(o, hist, staged, ys, rows);
         }
     }
     free(ff); free(cf); free(fd); free(cd);

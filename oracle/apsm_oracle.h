@@ -51,6 +51,15 @@ int apsm_oracle_set_threads(int n);
 
 /* rx: antenna-major complex (re,im) pairs, rx[2*(a*P+n)+{0,1}]; tx: P complex. */
 int apsm_oracle_train(apsm_oracle* o, const float* rx, const float* tx, uint32_t P);
+/* Training that records the reference's per-step history (NomaTrainHistory,
+ * noma_train_history.cu:65-248, apsm_train.cu:147-156): after every step the
+ * rows of this call and S validation samples (rx_val antenna-major, tx_val S
+ * complex) are detected and history[step * 6 + {0..5}] = train EVM, SER, BER,
+ * validation EVM, SER, BER.  F32 oracles only.  *n_steps = steps trained;
+ * returns 3 when that exceeds max_steps (the first max_steps are written). */
+int apsm_oracle_train_history(apsm_oracle* o, const float* rx, const float* tx, uint32_t P, const float* rx_val,
+                              const float* tx_val, uint32_t S, uint32_t bps, float mod_scale, float* history,
+                              uint32_t max_steps, uint32_t* n_steps);
 /* est: S complex (re,im). */
 int apsm_oracle_detect(apsm_oracle* o, const float* rx, uint32_t S, float* est);
 

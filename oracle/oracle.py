@@ -88,6 +88,9 @@ def _load_oracle() -> ctypes.CDLL:
         lib.apsm_oracle_set_threads.restype = ctypes.c_int
         lib.apsm_oracle_train.argtypes = [P, P, P, ctypes.c_uint32]
         lib.apsm_oracle_train.restype = ctypes.c_int
+        lib.apsm_oracle_train_history.argtypes = [P, P, P, ctypes.c_uint32, P, P, ctypes.c_uint32, ctypes.c_uint32,
+                                                  ctypes.c_float, P, ctypes.c_uint32, P]
+        lib.apsm_oracle_train_history.restype = ctypes.c_int
         lib.apsm_oracle_detect.argtypes = [P, P, ctypes.c_uint32, P]
         lib.apsm_oracle_detect.restype = ctypes.c_int
         lib.apsm_oracle_rows.argtypes = [P]
@@ -179,7 +182,10 @@ class OracleDetector:
     def reset_state(self):
         self._lib.apsm_oracle_reset(self._h)
 
-    def train(self, rx: np.ndarray, tx: np.ndarray) -> None:
+    def train(self, rx: np.ndarray, tx: np.ndarray, val_set: tuple | None = None) -> np.ndarray | None:
+        """Train on rx (N, P) / tx (P,).  With val_set = (rx_val, tx_val, bits_per_symbol, modulation_scale)
+        the reference's per-step history is recorded and returned as (steps, 6): train EVM, SER, BER,
+        validation EVM, SER, BER (NomaTrainHistory, noma_train_history.cu:65-248)."""
         rx = np.ascontiguousarray(rx, dtype=np.complex64)
         tx = np.ascontiguousarray(np.asarray(tx).reshape(-1), dtype=np.complex64)
         assert rx.shape == (self.N, tx.shape[0])
@@ -194,8 +200,23 @@ class OracleDetector:
         if self.params.gaussian_variance == 0:
             self.params.gaussian_variance = variance_heuristic(rx)
             self._lib.apsm_oracle_set_variance(self._h, self.params.gaussian_variance)
+        if val_set is not None:
+            rxv, txv, bps, scale = val_set
+            rxv = np.ascontiguousarray(rxv, dtype=np.complex64)
+            txv = np.ascontiguousarray(np.asarray(txv).reshape(-1), dtype=np.complex64)
+            assert rxv.shape == (self.N, txv.shape[0])
+            cap = 2 * tx.shape[0] * max(1, self.params.train_passes) + 1
+            hist = np.zeros((cap, 6), dtype=np.float32)
+            n = ctypes.c_uint32(0)
+            st = self._lib.apsm_oracle_train_history(self._h, rx.ctypes.data, tx.ctypes.data, tx.shape[0],
+                                                     rxv.ctypes.data, txv.ctypes.data, txv.shape[0], int(bps),
+                                                     float(scale), hist.ctypes.data, cap, ctypes.byref(n))
+            if st != 0:
+                raise RuntimeError(f"oracle train (history) failed: {st}")
+            return hist[:n.value].copy()
         if self._lib.apsm_oracle_train(self._h, rx.ctypes.data, tx.ctypes.data, tx.shape[0]) != 0:
             raise RuntimeError("oracle train failed")
+        return None
 
     def detect(self, rx: np.ndarray) -> np.ndarray:
         rx = np.ascontiguousarray(rx, dtype=np.complex64)
@@ -242,6 +263,10 @@ def _load_ref() -> ctypes.CDLL:
         lib.ref_train.restype = ctypes.c_int
         lib.ref_detect.argtypes = [P, P, ctypes.c_uint32, ctypes.c_uint32, P, ctypes.POINTER(ctypes.c_float)]
         lib.ref_detect.restype = ctypes.c_int
+        lib.ref_train_history.argtypes = [P, P, P, ctypes.c_uint32, ctypes.c_uint32, P, P, ctypes.c_uint32,
+                                          ctypes.c_uint32, ctypes.c_float, P, ctypes.c_uint32, P,
+                                          ctypes.POINTER(ctypes.c_float)]
+        lib.ref_train_history.restype = ctypes.c_int
         lib.ref_reset.argtypes = [P]
         lib.ref_destroy.argtypes = [P]
         lib.ref_run_users_threaded.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, P, P,
@@ -277,6 +302,23 @@ class ReferenceDetector:
         if self._lib.ref_train(self._h, rx.ctypes.data, tx.ctypes.data, self.N, tx.shape[0], ctypes.byref(ms)):
             raise RuntimeError("reference train failed")
         return ms.value
+
+    def train_history(self, rx: np.ndarray, tx: np.ndarray, rx_val: np.ndarray, tx_val: np.ndarray, bps: int,
+                      scale: float, max_steps: int = 1 << 16) -> tuple[np.ndarray, float]:
+        """train() with a NomaValSet: (steps, 6) history and the train time (ms)."""
+        rx = np.ascontiguousarray(rx, dtype=np.complex64)
+        tx = np.ascontiguousarray(np.asarray(tx).reshape(-1), dtype=np.complex64)
+        rxv = np.ascontiguousarray(rx_val, dtype=np.complex64)
+        txv = np.ascontiguousarray(np.asarray(tx_val).reshape(-1), dtype=np.complex64)
+        out = np.zeros((max_steps, 6), dtype=np.float32)
+        n = ctypes.c_uint32()
+        ms = ctypes.c_float()
+        st = self._lib.ref_train_history(self._h, rx.ctypes.data, tx.ctypes.data, self.N, tx.shape[0],
+                                         rxv.ctypes.data, txv.ctypes.data, txv.shape[0], int(bps), float(scale),
+                                         out.ctypes.data, max_steps, ctypes.byref(n), ctypes.byref(ms))
+        if st:
+            raise RuntimeError(f"reference train (history) failed: {st}")
+        return out[:n.value].copy(), ms.value
 
     def detect(self, rx: np.ndarray) -> tuple[np.ndarray, float]:
         rx = np.ascontiguousarray(rx, dtype=np.complex64)

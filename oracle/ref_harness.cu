@@ -25,6 +25,7 @@
 #include <nlohmann/json.hpp>
 
 #include "noma/noma_detector_factory.cuh"
+#include "noma/noma_train_history.cuh"
 
 namespace {
 
@@ -90,6 +91,31 @@ int ref_detect(ref_handle* h, const float* rx, uint32_t n_ant, uint32_t S, float
     if (out.size() != S) return 3;
     std::memcpy(est, out.data(), sizeof(float) * 2 * S);
     return 0;
+}
+
+// NomaDetector::train with a validation set (NomaValSet, cpp/lib/noma/noma_train_history.cuh:99;
+// used so by the reference CLI, cpp/cli/detect/noma_detect.cpp:124-145).  out: max_steps x 6 =
+// train EVM, SER, BER, validation EVM, SER, BER per recorded step; *n_steps = steps recorded.
+int ref_train_history(ref_handle* h, const float* rx, const float* tx, uint32_t n_ant, uint32_t P,
+                      const float* rx_val, const float* tx_val, uint32_t S, uint32_t bps, float mod_scale,
+                      float* out, uint32_t max_steps, uint32_t* n_steps, float* ms)
+{
+    NomaTrainHistory stats(bps, mod_scale);
+    const ComplexSampleMatrix rxv = to_matrix(rx_val, n_ant, S);
+    const ComplexSampleVector txv = to_vector(tx_val, S);
+    NomaValSet vs;
+    vs.emplace(std::make_tuple(std::ref(stats), std::cref(rxv), std::cref(txv)));
+    float t = h->det->train(to_matrix(rx, n_ant, P), to_vector(tx, P), vs);
+    if (ms) *ms = t;
+    if (cudaDeviceSynchronize() != cudaSuccess) return 2;
+    const size_t n = stats.evmTrain.size();
+    if (n_steps) *n_steps = uint32_t(n);
+    for (size_t i = 0; i < n && i < max_steps; ++i) {
+        const float row[6] = {stats.evmTrain[i], stats.serTrain[i], stats.berTrain[i],
+                              stats.evmVal[i],   stats.serVal[i],   stats.berVal[i]};
+        std::memcpy(out + 6 * i, row, sizeof(row));
+    }
+    return n > max_steps ? 3 : 0;
 }
 
 void ref_reset(ref_handle* h) { h->det->resetState(); }

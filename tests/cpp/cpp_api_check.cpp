@@ -2,6 +2,9 @@
 // reference CLI drives its NomaDetector (cpp/cli/detect/noma_detect.cpp:
 // 130-137): build from an algorithm JSON, train on pilots, detect data.
 // Usage: cpp_api_check <json> <N> <P> <S> <rx_train.f32> <tx.f32> <rx_data.f32> <est_out.f32>
+//                      [<tx_data.f32> <history.csv>]
+// With the last two arguments training takes the data as its validation set
+// (NomaValSet, as the CLI's -th option) and the history is written as CSV.
 // The float files hold interleaved complex64 samples (antenna-major for rx).
 #include "apsm_b200.hpp"
 
@@ -37,8 +40,8 @@ int main(int argc, char** argv)
             return 4;
         }
     }
-    if (argc != 9) {
-        std::cerr << "usage: cpp_api_check json N P S rx_train tx rx_data est_out" << std::endl;
+    if (argc != 9 && argc != 11) {
+        std::cerr << "usage: cpp_api_check json N P S rx_train tx rx_data est_out [tx_data history.csv]" << std::endl;
         return 2;
     }
     const uint32_t N = uint32_t(std::atoi(argv[2])), P = uint32_t(std::atoi(argv[3])), S = uint32_t(std::atoi(argv[4]));
@@ -51,7 +54,15 @@ int main(int argc, char** argv)
         rxData[a].assign(rxd.begin() + ptrdiff_t(a) * S, rxd.begin() + ptrdiff_t(a + 1) * S);
     }
     std::unique_ptr<NomaDetector> d = NomaDetectorFactory::build(std::string(argv[1]), N);
-    float trainTime = d->train(rxTraining, tx);
+    NomaTrainHistory stats(2, 0.70710677f); // QPSK
+    NomaValSet valSet = std::nullopt;
+    ComplexSampleVector txData;
+    if (argc == 11) {
+        txData = read_c64(argv[9], S);
+        valSet.emplace(std::make_tuple(std::ref(stats), std::cref(rxData), std::cref(txData)));
+    }
+    float trainTime = d->train(rxTraining, tx, valSet);
+    if (valSet.has_value()) std::get<0>(*valSet).toCsv(argv[10]);
     ComplexSampleVector est;
     float detectTime = d->detect(rxData, est);
     std::cout << "Train time = " << trainTime << " ms, detect time = " << detectTime << " ms" << std::endl;

@@ -14,10 +14,14 @@ train -> detect) on a B200.
   python tests/golden/make_golden.py run --out DIR
       (on a GPU box) runs the reference library on every case and writes
       DIR/golden_<case>.npz: inputs, config and the reference's estimates.
+  python tests/golden/make_golden.py history --out DIR
+      (on a GPU box) trains the reference with a validation set and writes
+      DIR/golden_history_<case>.npz: inputs, config, the per-step history.
 
 Synthetic cases use libapsm_b200.synth with fixed seeds; 2S is a multiple of
 32 in every case (the reference BALANCED detect mis-handles a partial last
-block, see tests/test_parity_gpu.py).
+block, see tests/test_parity_gpu.py), and so is 2P in the history cases, whose
+training-set metrics run that detection on the pilots.
 """
 from __future__ import annotations
 
@@ -110,9 +114,70 @@ def run(out: Path) -> None:
     print("lls: done")
 
 
+# Training-history cases: (frame, algorithm config, modulation).  The reference
+# records EVM / SER / BER of the training rows and a validation set after every
+# step (NomaValSet, apsm_train.cu:147-156).
+HISTORY_CASES = {
+    "qpsk_small": (dict(seed=201, K=2, N=4, P=64, S=64, modulation="QPSK"),
+                   {"otype": "APSM", "windowSize": 8, "gaussianKernelVariance": 0.5, "eB": 0.01}),
+    "qam16_sfw_step1": (dict(seed=202, K=3, N=6, P=112, S=96, modulation="QAM16"),
+                        {"otype": "APSM", "windowSize": 15, "startWithFullWindow": True, "sampleStep": 1,
+                         "gaussianKernelVariance": 0.3, "eB": 0.005}),
+    "qam16_passes2_shuffle": (dict(seed=203, K=3, N=6, P=96, S=96, modulation="QAM16"),
+                              {"otype": "APSM", "windowSize": 10, "trainPasses": 2, "dictionarySize": 96,
+                               "trainingShuffle": True}),
+    "bpsk_var0": (dict(seed=204, K=2, N=4, P=128, S=64, modulation="BPSK"),
+                  {"otype": "APSM", "windowSize": 6, "gaussianKernelVariance": 0.0}),
+}
+# 2P and 2S are multiples of 32 (see the module docstring).  A case with more
+# pilots than the dictionary holds (2P > 2 dictionarySize) is kept apart as
+# race_<case>.npz: there the reference's result depends on a data race
+# (tests/test_reference_eviction.py).
+RACE_CASES = {
+    "bpsk_evict": (dict(seed=204, K=2, N=4, P=120, S=64, modulation="BPSK"),
+                   {"otype": "APSM", "windowSize": 6, "dictionarySize": 30, "gaussianKernelVariance": 0.4}),
+}
+
+
+def history(out: Path) -> None:
+    from libapsm_b200 import synth
+    from libapsm_b200.modulation import Modulation
+    from oracle import oracle as O
+
+    out.mkdir(parents=True, exist_ok=True)
+    todo = []
+    for name, (fr, cfg) in HISTORY_CASES.items():
+        f = synth.generate_frame(fr["seed"], K=fr["K"], N=fr["N"], P=fr["P"], S=fr["S"], modulation=fr["modulation"],
+                                 snr_db=20)
+        todo.append((name, cfg, f.rx_train, f.tx_train[USER], f.rx_data, f.tx_data[USER], fr["modulation"]))
+    cap = np.load(HERE / "captured_qpsk_inputs.npz")
+    todo.append(("captured_qpsk", CAPTURED_CFG, cap["rx_train"], cap["tx_train"][USER], cap["rx_data"],
+                 cap["tx_data"][USER], "QPSK"))
+    for name, (fr, cfg) in RACE_CASES.items():
+        f = synth.generate_frame(fr["seed"], K=fr["K"], N=fr["N"], P=fr["P"], S=fr["S"], modulation=fr["modulation"],
+                                 snr_db=20)
+        todo.append(("race:" + name, cfg, f.rx_train, f.tx_train[USER], f.rx_data, f.tx_data[USER],
+                     fr["modulation"]))
+    for name, cfg, rxt, txt, rxd, txd, mod in todo:
+        m = Modulation(mod)
+        r = O.ReferenceDetector(cfg, rxt.shape[0])
+        hist, tms = r.train_history(rxt, txt, rxd, txd, m.bps, m.scale)
+        est, _ = r.detect(rxd)
+        fname = f"race_{name[5:]}.npz" if name.startswith("race:") else f"golden_history_{name}.npz"
+        np.savez_compressed(out / fname, config=json.dumps(cfg), modulation=mod,
+                            rx_train=rxt, tx_train=txt, rx_data=rxd, tx_data=txd, hist_ref=hist, est_ref=est,
+                            ref_train_ms=tms)
+        print(f"history {name}: {hist.shape[0]} steps, ref train {tms:.3f} ms, last {hist[-1]}")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", choices=["capture", "run"])
+    ap.add_argument("mode", choices=["capture", "run", "history"])
     ap.add_argument("--out", default=str(HERE))
     a = ap.parse_args()
-    capture() if a.mode == "capture" else run(Path(a.out))
+    if a.mode == "capture":
+        capture()
+    elif a.mode == "run":
+        run(Path(a.out))
+    else:
+        history(Path(a.out))

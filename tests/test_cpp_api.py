@@ -53,3 +53,28 @@ def test_cpp_api_matches_python_api(cpp_check, tmp_path):
     det.train(f.rx_train, f.tx_train[0])
     est_py, _ = det.detect(f.rx_data)
     np.testing.assert_array_equal(est_cpp, est_py)
+
+
+@pytest.mark.gpu
+def test_cpp_api_train_history(cpp_check, tmp_path):
+    import libapsm_b200 as L
+    from libapsm_b200 import synth
+
+    f = synth.generate_frame(32, K=2, N=4, P=64, S=96, modulation="QPSK")
+    cfg = '{"otype":"APSM","windowSize":8,"gaussianKernelVariance":0.5}'
+    files = {}
+    for name, arr in (("rxt", f.rx_train), ("tx", f.tx_train[0]), ("rxd", f.rx_data), ("txd", f.tx_data[0])):
+        p = tmp_path / f"{name}.f32"
+        np.ascontiguousarray(arr, dtype=np.complex64).tofile(p)
+        files[name] = str(p)
+    csv = tmp_path / "h.csv"
+    r = subprocess.run([str(cpp_check), cfg, "4", "64", "96", files["rxt"], files["tx"], files["rxd"],
+                        str(tmp_path / "est.f32"), files["txd"], str(csv)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    rows = csv.read_text().splitlines()
+    assert rows[0] == "step,train_evm,train_ser,train_ber,val_evm,val_ser,val_ber" and len(rows) == 65
+    det = L.NomaDetectorFactory.build(cfg, 4)
+    hist = L.NomaTrainHistory(2, L.Modulation("QPSK").scale)
+    det.train(f.rx_train, f.tx_train[0], val_set=(hist, f.rx_data, f.tx_data[0]))
+    got = np.array([[float(v) for v in row.split(",")[1:]] for row in rows[1:]])
+    np.testing.assert_allclose(got, hist.steps, rtol=1e-5, atol=1e-6)  # %g keeps 6 digits
