@@ -70,8 +70,8 @@ apsm_status apsm_detector::init(const Config& c, uint32_t num_antennas, uint32_t
     Dp = row_pitch(D);
     U = num_users;
     is_lls = cfg.otype == "LLS";
-    if (cfg.norm_constraint > 0.f) {
-        last_error = "normConstraint > 0 is not available in this build";
+    if (cfg.norm_constraint > 0.f && cfg.train_incremental) {
+        last_error = "normConstraint > 0 runs with the exact training sweep only (trainVersion \"exact\")";
         return APSM_ERR_UNSUPPORTED;
     }
     cap = 2 * cfg.dict_size;
@@ -193,6 +193,7 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         }
         APSM_CK(h_snap_a.ensure(UT * q2));
         APSM_CK(h_snap_w.ensure(UT * D));
+        APSM_CK(h_snap_scale.ensure(UT));
         APSM_CK(h_a0.ensure(size_t(U) * nU));
         APSM_CK(h_A.ensure(UT * nU));
         APSM_CK(h_E.ensure(size_t(hist_nE) * Dp));
@@ -236,6 +237,8 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         const int T = int(h_steps.size());
         int v_first = h_steps[0].hi - h_steps[0].wk;
         for (const auto& st : h_steps) v_first = std::min(v_first, st.hi - st.wk);
+        // normConstraint sums over every dictionary row's column, not only the window rows'
+        if (cfg.norm_constraint > 0.f) v_first = 0;
         const int nV = int(nU) - v_first;
         // longest kernel column (rows column_base(v) .. min(nU, v + q2), 16-byte multiple)
         int Lk = 4;
@@ -285,6 +288,8 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         ta.mp = mp;
         ta.snap_a = hist_nE > 0 ? h_snap_a.p : nullptr;
         ta.snap_w = hist_nE > 0 ? h_snap_w.p : nullptr;
+        ta.norm_c = cfg.norm_constraint;
+        ta.snap_scale = hist_nE > 0 && cfg.norm_constraint > 0.f ? h_snap_scale.p : nullptr;
 
         ta.XP = int(Dp) + 4; // padded window-row pitch (conflict-free column reads)
         ta.err = train_err.p;
@@ -352,8 +357,8 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
             *nwarps_out = nwarps;
             *ns_out = ns;
             return sizeof(float) * (size_t(ta.XW) * ta.XP + size_t(ns) * Lk + size_t(ta.A_ring) + kMaxFeatures +
-                                    2 * q2 + size_t(nwarps) * 32 + 2 * size_t(ta.XW)) +
-                   32;
+                                    2 * q2 + size_t(nwarps) * 32 + 2 * size_t(ta.XW) + 64) +
+                   48;
         };
         const size_t smem_limit = 227 * 1024;
         struct Choice {
@@ -431,6 +436,7 @@ sweep_done:
         ha.n_steps = T_steps;
         ha.snap_a = h_snap_a.p;
         ha.snap_w = h_snap_w.p;
+        ha.snap_scale = cfg.norm_constraint > 0.f ? h_snap_scale.p : nullptr;
         ha.a0 = h_a0.p;
         ha.a0_stride = nU;
         ha.used_before = int(used);

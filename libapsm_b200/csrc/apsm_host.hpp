@@ -108,7 +108,7 @@ struct apsm_detector {
     apsm::DevBuf<float2> rx_stage, tx_stage, est_stage;
     // training-history scratch: per-step snapshots, initial coefficients, dense
     // per-step coefficients, evaluation rows / targets, partial sums, output
-    apsm::DevBuf<float> h_snap_a, h_snap_w, h_a0, h_A, h_E, h_Ey, h_part, h_out;
+    apsm::DevBuf<float> h_snap_a, h_snap_w, h_snap_scale, h_a0, h_A, h_E, h_Ey, h_part, h_out;
     apsm::DevBuf<float2> h_rx, h_tx;
     apsm::GramWorkspace* gram = nullptr;
     apsm::LlsWorkspace* lls = nullptr; // least-squares detector / llsInitialization

@@ -41,6 +41,8 @@ struct TrainArgs {
     int* err;                 // set to 1 when a bounded wait expired
     float* snap_a;            // users x n_steps x q2: the active rows' coefficients after each step (nullptr: off)
     float* snap_w;            // users x n_steps x D: the linear weights after each step
+    float* snap_scale;        // users x n_steps: the normConstraint factor of each step (1: none)
+    float norm_c;             // normConstraint: bound of ||f_G|| after every step (0: off; exact sweep only)
 };
 
 // Training history (kernels_history.cu): every step's model evaluated on the
@@ -50,6 +52,7 @@ struct HistoryArgs {
     int n_steps;
     const float* snap_a;    // users x n_steps x q2: active-row coefficients after each step
     const float* snap_w;    // users x n_steps x D: linear weights after each step
+    const float* snap_scale; // users x n_steps: normConstraint factor of each step (nullptr: none)
     const float* a0;        // users x a0_stride: coefficients of the rows present before the call
     size_t a0_stride;
     int used_before, nU, cap, q2, D, Dp, users;

@@ -64,6 +64,7 @@ __global__ void history_expand_kernel(HistoryArgs h)
         const TrainStep st = h.steps[t];
         const int start = st.hi - st.wk;
         if (b >= start && b < start + st.n_active) cur = sa[size_t(t) * h.q2 + (b - start)];
+        else if (h.snap_scale) cur *= h.snap_scale[size_t(u) * h.n_steps + t]; // normConstraint of step t
         const int lo = max(0, st.hi - h.cap);
         A[size_t(t) * h.nU + b] = (b >= lo && b < st.hi) ? cur : 0.f;
     }

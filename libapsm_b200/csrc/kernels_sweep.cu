@@ -125,6 +125,8 @@ __device__ __forceinline__ void st_async_f32(const float* local, const uint64_t*
 //   cbuf   [2][q2]    the step's corrections (st.async from their owner CTAs)
 //   red    [nwarps][32] lane partials of the predictions
 //   yw, nw [XW]       targets and squared norms of the window rows
+//   nbuf   [2][16]    normConstraint: the CTAs' partial sums of ||f_G||^2 (st.async)
+//   npart  [32]       normConstraint: warp partials
 template <bool kStaged>
 __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
 {
@@ -145,8 +147,11 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
     float* red = cbuf + 2 * q2;
     float* yw = red + nwarps * 32;
     float* nw = yw + args.XW;
-    uint64_t* cfull = reinterpret_cast<uint64_t*>(nw + args.XW); // [2]
-    volatile int* abort_flag = reinterpret_cast<volatile int*>(cfull + 2);
+    float* nbuf = nw + args.XW;
+    float* npart = nbuf + 32;
+    uint64_t* cfull = reinterpret_cast<uint64_t*>(npart + 32); // [2] corrections
+    uint64_t* nfull = cfull + 2;                               // [2] normConstraint partials
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(cfull + 4);
 
     const int amask = args.A_ring - 1, xmask = args.XW - 1;
     const int n_steps = args.n_steps;
@@ -195,6 +200,8 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
     if (tid == 0) {
         mbar_init(&cfull[0], 1);
         mbar_init(&cfull[1], 1);
+        mbar_init(&nfull[0], 1);
+        mbar_init(&nfull[1], 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -226,6 +233,7 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
         float* cb = cbuf + (t & 1) * q2;
         uint64_t* bar = &cfull[t & 1];
         if (tid == 0) mbar_expect_tx(bar, uint32_t(st.n_active) * 4u);
+        if (tid == 0 && args.norm_c > 0.f) mbar_expect_tx(&nfull[t & 1], uint32_t(C) * 4u);
 
         // predictions with the pre-step coefficients; this CTA owns window rows v % C == rank
         const int first = start + ((rank - start % C) + C) % C;
@@ -325,6 +333,44 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
             acc = __fadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, 2));
             acc = __fadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, 4));
             if (d < D && g == 0) w_s[d] = __fadd_rn(w_s[d], acc);
+        }
+        if (args.norm_c > 0.f) {
+            // normConstraint (kernel_adapt_coeffs, apsm_train.cu:190-256): ||f_G||^2 =
+            // sum_v a_v (wG a_v + 2 sum_{u<v} K(u, v) a_u) over the dictionary [lo, hi), column v of
+            // K holding K(u, v) for its older rows; CTA r takes the columns v = r mod C.  The CTAs'
+            // partials go to every CTA (st.async), each adds them in rank order, so all CTAs see
+            // the same norm and scale their copies of the coefficients alike.
+            __syncthreads(); // this step's a_j are final
+            const int lo = max(0, st.hi - cap);
+            float acc = 0.f;
+            for (int v = lo + ((rank - lo % C) + C) % C + C * warp; v < st.hi; v += C * nwarps) {
+                const float* kc = K + size_t(v - args.v_first) * args.Lk - column_base(v, cap);
+                float sv = 0.f;
+                for (int u = lo + lane; u < v; u += 32) sv = fmaf(__ldg(kc + u), a_ring[u & amask], sv);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(0xffffffffu, sv, o);
+                const float av = a_ring[v & amask];
+                acc = fmaf(av, fmaf(2.f, sv, mp.wG * av), acc);
+            }
+            if (lane == 0) npart[warp] = acc;
+            __syncthreads();
+            if (warp == 0) {
+                float x = lane < nwarps ? npart[lane] : 0.f;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                if (lane < C) st_async_f32(nbuf + (t & 1) * 16 + rank, &nfull[t & 1], uint32_t(lane), x);
+            }
+            if (!mbar_wait_bounded(&nfull[t & 1], uint32_t(t >> 1) & 1u)) *abort_flag = 1;
+            float norm = 0.f;
+            for (int r = 0; r < C; ++r) norm += nbuf[(t & 1) * 16 + r];
+            if (norm > 0.f) norm = sqrtf(norm);
+            float factor = 1.f;
+            if (norm > args.norm_c) {
+                factor = __fdiv_rn(args.norm_c, norm);
+                for (int u = lo + tid; u < st.hi; u += nthreads) a_ring[u & amask] = __fmul_rn(a_ring[u & amask], factor);
+            }
+            if (args.snap_scale && rank == 0 && tid == 0) args.snap_scale[size_t(user) * n_steps + t] = factor;
+            if (!args.snap_a) __syncthreads(); // scaled coefficients visible before the next step
         }
         if (args.snap_a) {
             // training history: the model after this step (every CTA holds the same copy)

@@ -249,6 +249,71 @@ static float detect_one_f32(const apsm_oracle* o, const float* x)
     return part[0];
 }
 
+/* normConstraint (kernel_adapt_coeffs, apsm_train.cu:190-256, run after every
+ * step by :142-145): ||f_G||^2 = sum_i sum_j wG k(d_i, d_j) a_i a_j over the
+ * dictionary, summed as the reference does -- block i, lane t over
+ * j = t, t+32, ... (((wG k) a_i) a_j, fma-contracted into the lane sum), lanes
+ * added in order, then rows in order -- and if its square root exceeds the
+ * bound every coefficient is multiplied by bound / norm.  (The reference stages
+ * d_j in a 32-float array: dictionary rows wider than 32 features overflow it.) */
+static void adapt_coeffs_f32(apsm_oracle* o)
+{
+    const apsm_oracle_params* p = &o->par;
+    const float ew = -0.5f / p->gaussian_variance;
+    const uint32_t M = o->used, D = o->D;
+    float* rowsum = (float*)malloc((size_t)(M ? M : 1) * sizeof(float));
+#pragma omp parallel for schedule(static) if (M > 64)
+    for (uint32_t i = 0; i < M; ++i) {
+        const uint32_t ri = phys(o, i);
+        const float ai = o->Af[ri];
+        float lane[LANES];
+        memset(lane, 0, sizeof(lane));
+        for (uint32_t j = 0; j < M; ++j) {
+            const uint32_t rj = phys(o, j);
+            const float k = kern_f32(&o->Xf[(size_t)ri * D], &o->Xf[(size_t)rj * D], D, ew);
+            const float t = (p->gaussian_weight * k) * ai;
+            lane[j % LANES] = fmaf(t, o->Af[rj], lane[j % LANES]);
+        }
+        float r = 0.f;
+        for (uint32_t l = 0; l < LANES && l < M; ++l) r = r + lane[l];
+        rowsum[i] = r;
+    }
+    float norm = 0.f;
+    for (uint32_t i = 0; i < M; ++i) norm = norm + rowsum[i];
+    free(rowsum);
+    if (norm > 0.f) norm = sqrtf(norm);
+    if (norm > p->norm_constraint) {
+        const float factor = p->norm_constraint / norm;
+        for (uint32_t i = 0; i < M; ++i) o->Af[phys(o, i)] *= factor;
+    }
+}
+
+static void adapt_coeffs_f64(apsm_oracle* o)
+{
+    const apsm_oracle_params* p = &o->par;
+    const double ew = -0.5 / (double)p->gaussian_variance;
+    const uint32_t M = o->used, D = o->D;
+    double norm = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : norm) if (M > 64)
+    for (uint32_t i = 0; i < M; ++i) {
+        const uint32_t ri = phys(o, i);
+        for (uint32_t j = 0; j < M; ++j) {
+            const uint32_t rj = phys(o, j);
+            double acc = 0.0;
+            for (uint32_t k = 0; k < D; ++k) {
+                const double diff = o->Xd[(size_t)ri * D + k] - o->Xd[(size_t)rj * D + k];
+                acc += diff * diff;
+            }
+            norm += (double)p->gaussian_weight * exp(ew * acc) * o->Ad[ri] * o->Ad[rj];
+        }
+    }
+    if (norm > 0.0) norm = sqrt(norm);
+    if (norm > (double)p->norm_constraint) {
+        const double factor = (double)p->norm_constraint / norm;
+        for (uint32_t i = 0; i < M; ++i) o->Ad[phys(o, i)] *= factor;
+    }
+}
+
 /* ---------------------------------------------------------------- FP64 -- */
 
 static double predict_f64(const apsm_oracle* o, const double* x)
@@ -462,6 +527,10 @@ static int train_impl(apsm_oracle* o, const float* rx, const float* tx, uint32_t
             if (n_active == 0) continue;
             if (o->prec == APSM_ORACLE_F32) step_f32(o, start, n_active, wk, ff, cf);
             else step_f64(o, start, n_active, wk, fd, cd);
+            if (p->norm_constraint > 0.f) {
+                if (o->prec == APSM_ORACLE_F32) adapt_coeffs_f32(o);
+                else adapt_coeffs_f64(o);
+            }
             if (hist) hist_record(o, hist, staged, ys, rows);
         }
     }

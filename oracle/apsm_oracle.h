@@ -40,6 +40,7 @@ typedef struct {
     uint32_t train_passes;
     uint32_t start_full_window;
     uint32_t dictionary_size; /* complex entries; 2x real rows */
+    float norm_constraint;    /* > 0: RKHS-norm bound of the Gaussian part, applied after every step */
 } apsm_oracle_params;
 
 typedef struct apsm_oracle apsm_oracle;

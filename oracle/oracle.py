@@ -40,7 +40,8 @@ class OracleParams(ctypes.Structure):
     _fields_ = [("linear_weight", ctypes.c_float), ("gaussian_weight", ctypes.c_float),
                 ("gaussian_variance", ctypes.c_float), ("eB", ctypes.c_float), ("window_size", ctypes.c_uint32),
                 ("sample_step", ctypes.c_uint32), ("train_passes", ctypes.c_uint32),
-                ("start_full_window", ctypes.c_uint32), ("dictionary_size", ctypes.c_uint32)]
+                ("start_full_window", ctypes.c_uint32), ("dictionary_size", ctypes.c_uint32),
+                ("norm_constraint", ctypes.c_float)]
 
 
 def reference_params(config: Mapping[str, Any], num_antennas: int) -> OracleParams:
@@ -63,6 +64,7 @@ def reference_params(config: Mapping[str, Any], num_antennas: int) -> OraclePara
     p.train_passes = int(config.get("trainPasses", 1))
     p.start_full_window = int(bool(config.get("startWithFullWindow", False)))
     p.dictionary_size = int(config.get("dictionarySize", 685))
+    p.norm_constraint = f32(config.get("normConstraint", 0.0))
     return p
 
 

@@ -54,6 +54,11 @@ CASES = {
     "wG08_detect_oldfast": (dict(seed=107, K=4, N=16, P=200, S=208, modulation="QAM16"),
                             {"otype": "APSM", "windowSize": 40, "gaussianKernelWeight": 0.8,
                              "gaussianKernelVariance": 0.2, "eB": 0.02, "detectVersion": "oldfast"}),
+    # normConstraint (apsm_train.cu:142-145, 190-256): 0.05 is below the unconstrained model's
+    # RKHS norm (0.14), so the coefficients are scaled back after most steps
+    "norm_constraint": (dict(seed=108, K=3, N=8, P=96, S=96, modulation="QAM16"),
+                        {"otype": "APSM", "windowSize": 10, "gaussianKernelVariance": 0.5,
+                         "normConstraint": 0.05}),
 }
 CAPTURED_CFG = {"otype": "APSM", "windowSize": 80}  # the README example's algorithm config
 USER = 1
@@ -79,19 +84,22 @@ def capture() -> None:
     print("wrote", HERE / "captured_qpsk_inputs.npz")
 
 
-def run(out: Path) -> None:
+def run(out: Path, only: set[str] | None = None) -> None:
     from libapsm_b200 import synth
     from oracle import oracle as O
 
     out.mkdir(parents=True, exist_ok=True)
     todo = []
     for name, (fr, cfg) in CASES.items():
+        if only and name not in only:
+            continue
         f = synth.generate_frame(fr["seed"], K=fr["K"], N=fr["N"], P=fr["P"], S=fr["S"], modulation=fr["modulation"],
                                  snr_db=20)
         todo.append((name, cfg, f.rx_train, f.tx_train, f.rx_data, f.tx_data, fr["modulation"]))
     cap = np.load(HERE / "captured_qpsk_inputs.npz")
-    todo.append(("captured_qpsk", CAPTURED_CFG, cap["rx_train"], cap["tx_train"], cap["rx_data"], cap["tx_data"],
-                 "QPSK"))
+    if not only or "captured_qpsk" in only:
+        todo.append(("captured_qpsk", CAPTURED_CFG, cap["rx_train"], cap["tx_train"], cap["rx_data"],
+                     cap["tx_data"], "QPSK"))
     for name, cfg, rxt, txt, rxd, txd, mod in todo:
         r = O.ReferenceDetector(cfg, rxt.shape[0])
         tms = r.train(rxt, txt[USER])
@@ -104,6 +112,8 @@ def run(out: Path) -> None:
                             rx_train=rxt, tx_train=txt[USER], rx_data=rxd, tx_data=txd[USER], est_ref=est,
                             ref_run_to_run=spread, ref_train_ms=tms, ref_detect_ms=dms)
         print(f"{name}: ref train {tms:.3f} ms detect {dms:.3f} ms, run-to-run max |d| {spread:.2e}")
+    if only and "lls" not in only:
+        return
     # LLS reference outputs on one case (the reference's cuBLAS least-squares detector)
     name, cfg, rxt, txt, rxd, txd, mod = todo[2]
     r = O.ReferenceDetector({"otype": "LLS"}, rxt.shape[0])
@@ -128,6 +138,8 @@ HISTORY_CASES = {
                                "trainingShuffle": True}),
     "bpsk_var0": (dict(seed=204, K=2, N=4, P=128, S=64, modulation="BPSK"),
                   {"otype": "APSM", "windowSize": 6, "gaussianKernelVariance": 0.0}),
+    "qam16_norm": (dict(seed=205, K=3, N=8, P=96, S=96, modulation="QAM16"),
+                   {"otype": "APSM", "windowSize": 10, "gaussianKernelVariance": 0.5, "normConstraint": 0.05}),
 }
 # 2P and 2S are multiples of 32 (see the module docstring).  A case with more
 # pilots than the dictionary holds (2P > 2 dictionarySize) is kept apart as
@@ -139,7 +151,7 @@ RACE_CASES = {
 }
 
 
-def history(out: Path) -> None:
+def history(out: Path, only: set[str] | None = None) -> None:
     from libapsm_b200 import synth
     from libapsm_b200.modulation import Modulation
     from oracle import oracle as O
@@ -147,13 +159,18 @@ def history(out: Path) -> None:
     out.mkdir(parents=True, exist_ok=True)
     todo = []
     for name, (fr, cfg) in HISTORY_CASES.items():
+        if only and name not in only:
+            continue
         f = synth.generate_frame(fr["seed"], K=fr["K"], N=fr["N"], P=fr["P"], S=fr["S"], modulation=fr["modulation"],
                                  snr_db=20)
         todo.append((name, cfg, f.rx_train, f.tx_train[USER], f.rx_data, f.tx_data[USER], fr["modulation"]))
     cap = np.load(HERE / "captured_qpsk_inputs.npz")
-    todo.append(("captured_qpsk", CAPTURED_CFG, cap["rx_train"], cap["tx_train"][USER], cap["rx_data"],
-                 cap["tx_data"][USER], "QPSK"))
+    if not only or "captured_qpsk" in only:
+        todo.append(("captured_qpsk", CAPTURED_CFG, cap["rx_train"], cap["tx_train"][USER], cap["rx_data"],
+                     cap["tx_data"][USER], "QPSK"))
     for name, (fr, cfg) in RACE_CASES.items():
+        if only and name not in only:
+            continue
         f = synth.generate_frame(fr["seed"], K=fr["K"], N=fr["N"], P=fr["P"], S=fr["S"], modulation=fr["modulation"],
                                  snr_db=20)
         todo.append(("race:" + name, cfg, f.rx_train, f.tx_train[USER], f.rx_data, f.tx_data[USER],
@@ -174,10 +191,12 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("mode", choices=["capture", "run", "history"])
     ap.add_argument("--out", default=str(HERE))
+    ap.add_argument("--cases", default="", help="comma-separated case names (default: all)")
     a = ap.parse_args()
+    only = set(filter(None, a.cases.split(","))) or None
     if a.mode == "capture":
         capture()
     elif a.mode == "run":
-        run(Path(a.out))
+        run(Path(a.out), only)
     else:
-        history(Path(a.out))
+        history(Path(a.out), only)

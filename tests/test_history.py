@@ -104,6 +104,9 @@ CASES = {
                  {"otype": "APSM", "windowSize": 7, "startWithFullWindow": True}),
     "n64_shuffle": (dict(seed=306, K=4, N=64, P=96, S=64, modulation="QPSK"),
                     {"otype": "APSM", "windowSize": 10, "trainingShuffle": True}),
+    "qam16_norm_evict": (dict(seed=307, K=3, N=8, P=120, S=64, modulation="QAM16"),
+                         {"otype": "APSM", "windowSize": 10, "gaussianKernelVariance": 0.5, "dictionarySize": 50,
+                          "normConstraint": 0.05}),
 }
 
 

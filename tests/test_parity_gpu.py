@@ -81,6 +81,13 @@ CASES = [
     ("N64", dict(BASE, windowSize=16), (13, 4, 64, 100, 70, "QAM16")),
     ("N16-oldfast", dict(BASE, windowSize=40, detectVersion="oldfast"), (14, 4, 16, 300, 200, "QAM64")),
     ("config0", synth.CONFIG0_ALGORITHM, (0, 6, 8, 600, 1800, "QPSK")),
+    # normConstraint: every bound below is active (the unconstrained model's RKHS norm is larger)
+    ("norm", dict(BASE, windowSize=10, normConstraint=0.05), (108, 3, 8, 96, 96, "QAM16")),
+    ("norm-w80", dict(BASE, windowSize=80, normConstraint=0.1), (15, 3, 8, 300, 100, "QAM16")),
+    ("norm-wrap", dict(BASE, dictionarySize=60, normConstraint=0.05), (10, 3, 6, 150, 100, "QAM16")),
+    ("norm-N32", dict(BASE, windowSize=12, normConstraint=0.003), (16, 3, 32, 100, 64, "QAM16")),
+    ("norm-passes2", dict(BASE, windowSize=10, trainPasses=2, dictionarySize=96, normConstraint=0.05),
+     (108, 3, 8, 96, 96, "QAM16")),
 ]
 
 
@@ -109,7 +116,7 @@ def test_product_matches_oracle_fp64_config0(oracle_mod):
 def test_second_train_call_appends(oracle_mod):
     f = synth.generate_frame(20, K=3, N=6, P=150, S=100, modulation="QAM16")
     g = synth.generate_frame(21, K=3, N=6, P=70, S=10, modulation="QAM16")
-    for cfg in (BASE, dict(BASE, dictionarySize=100)):
+    for cfg in (BASE, dict(BASE, dictionarySize=100), dict(BASE, dictionarySize=100, normConstraint=0.05)):
         det = L.NomaDetectorFactory.build(cfg, 6)
         det.train(f.rx_train, f.tx_train[0])
         det.train(g.rx_train, g.tx_train[0])
@@ -131,6 +138,23 @@ def test_reset_state_gives_fresh_detector():
     det.train(f.rx_train, f.tx_train[0])
     e2, _ = det.detect(f.rx_data)
     np.testing.assert_array_equal(e1, e2)  # deterministic
+
+
+def test_norm_constraint_binds_and_multi_user_equals_single():
+    f = synth.generate_frame(108, K=3, N=8, P=96, S=96, modulation="QAM16", snr_db=20)
+    cfg = dict(BASE, windowSize=10, normConstraint=0.05)
+    _, free = run_product(dict(BASE, windowSize=10), f)
+    _, bound = run_product(cfg, f)
+    assert float(np.max(np.abs(free - bound))) > 1e-3  # the bound changes the model
+    _, est = run_product(cfg, f, users=3)
+    for u in range(3):
+        _, e1 = run_product(cfg, f, u=u)
+        np.testing.assert_array_equal(est[u], e1)
+
+
+def test_norm_constraint_with_incremental_sweep_is_refused():
+    with pytest.raises(L.ApsmError, match="exact training sweep"):
+        L.NomaDetectorFactory.build(dict(BASE, normConstraint=0.1, trainVersion="incremental"), 4)
 
 
 def test_multi_user_equals_single_user_runs():
@@ -214,7 +238,10 @@ def test_product_matches_reference_all_users_config1(oracle_mod):
 # instead of re-summing it in the reference's order; the FP32 bar (1e-4
 # relative) applies.
 
-@pytest.mark.parametrize("name,cfg,frame", CASES, ids=[c[0] for c in CASES])
+INC_CASES = [c for c in CASES if "normConstraint" not in c[1]]  # normConstraint: exact sweep only
+
+
+@pytest.mark.parametrize("name,cfg,frame", INC_CASES, ids=[c[0] for c in INC_CASES])
 def test_incremental_sweep_matches_oracle(oracle_mod, name, cfg, frame):
     seed, K, N, P, S, mod = frame
     f = synth.generate_frame(seed, K=K, N=N, P=P, S=S, modulation=mod, snr_db=20)
