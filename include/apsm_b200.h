@@ -238,6 +238,12 @@ uint64_t apsm_pool_bytes_in_use(const apsm_pool* p);
  * columns + sweep) and detection stages; blocks until the batch finished. */
 apsm_status apsm_pool_last_ms(apsm_pool* p, uint32_t lane, float* train_ms, float* detect_ms);
 
+/* Per-stage GPU events of every batch (default on): apsm_pool_last_ms and
+ * apsm_pool_last_sweep_ms report -1 while off.  Off saves six event records
+ * per batch on the latency-critical path (the request server turns it off).
+ * No reference counterpart. */
+apsm_status apsm_pool_set_timing(apsm_pool* pool, int on);
+
 /* GPU time (ms) of the persistent training sweep kernel of the lane's last batch (-1: none). */
 apsm_status apsm_pool_last_sweep_ms(apsm_pool* p, uint32_t lane, float* sweep_ms);
 

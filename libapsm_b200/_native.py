@@ -74,6 +74,7 @@ SIGNATURES = [
     ("apsm_pool_last_error", ctypes.c_char_p, [_P]),
     ("apsm_pool_last_launches", ctypes.c_int, [_P, _U32]),
     ("apsm_pool_last_sweep_ms", ctypes.c_int, [_P, _U32, _F]),
+    ("apsm_pool_set_timing", ctypes.c_int, [_P, ctypes.c_int]),
     # request server (continuous batching over a pool)
     ("apsm_server_create", ctypes.c_int, [_P, _U32, _U32, ctypes.POINTER(_P)]),
     ("apsm_server_destroy", None, [_P]),

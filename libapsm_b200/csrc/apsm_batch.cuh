@@ -36,6 +36,7 @@ struct BatchTrainJob {
     const float* y;      // 2 nP targets (row form: Re x, Im x)
     float* a;            // 2 nP coefficients (row form); in: old rows, out: visible rows
     float* w;            // 2N linear weights (in/out)
+    float* r;            // 2N residual weights r = w - sum_{b visible} a_b x_b (in/out, kept with the detector)
     const float4* Kc;    // combined kernel columns (A + wL r, Bp + wL m, Bm - wL m, 0), pairs n in [n_first, nP)
     const TrainStep* steps;
     int n_steps;
@@ -45,11 +46,35 @@ struct BatchTrainJob {
     long long kc_base;   // column_prefix(n_first)
     float ew;            // -0.5 / (variance * N^2)
     int fresh;           // start from a fresh state (w = 0; the universe holds only the new pilots)
+    // Sums over the old pairs of a call that appends (null otherwise), for every kernel column
+    // n in [n_first, nP), per pass of kKcolRows column entries ([n - n_first][pass], pro_stride
+    // passes), written by launch_batch_kcol: sum_b a_b Kt(b, n) over b in [pro_lo, pro_hi) for
+    // the first window's pairs n < n_first + pro_w (their starting predictions), over
+    // b in [col_begin(n), n_first) for the later pairs (the part of their frozen sums whose
+    // coefficients this call never changes).
+    float2* pro;
+    int pro_w, pro_lo, pro_hi, pro_stride;
 };
+
+// Kernel-column launch shape: columns per block and column entries per pass.
+constexpr int kKcolGroup = 8;
+constexpr int kKcolRows = 128;
 
 // Column n holds pairs [col_begin(n), col_end(n)).
 __host__ __device__ inline int col_begin(int n, int capP) { return n + 1 - capP > 0 ? n + 1 - capP : 0; }
 __host__ __device__ inline int col_end(int n, int qP, int nP) { return n + qP < nP ? n + qP : nP; }
+
+// Range of old pairs summed into the pro sums of column n.
+__host__ __device__ inline void pro_range(const BatchTrainJob& j, int n, int* lo, int* hi)
+{
+    if (n < j.n_first + j.pro_w) {
+        *lo = j.pro_lo;
+        *hi = j.pro_hi;
+    } else {
+        *lo = col_begin(n, j.capP);
+        *hi = j.n_first;
+    }
+}
 
 // Sum of the column lengths of pairs [0, n) (closed form of the clamped ramps).
 __host__ __device__ inline long long column_prefix(long long n, long long qP, long long nP, long long capP)
@@ -64,8 +89,7 @@ __host__ __device__ inline long long column_prefix(long long n, long long qP, lo
 
 // One detection job: S data samples of one detector against its dictionary.
 struct BatchDetectJob {
-    const float2* Ys;   // S x Np data samples
-    const float* nrm_s; // S squared norms
+    const float2* rx;   // N x S received data samples, antenna-major (as the caller holds them)
     const float2* Yd;   // Mp x Np dictionary samples
     const float* nrm_d; // Mp norms
     const float* a;     // 2 Mp coefficients (row form)
@@ -73,6 +97,10 @@ struct BatchDetectJob {
     float2* out;        // S soft estimates (Re = f(row 2s), Im = f(row 2s+1))
     int S, Mp, N, Np;
     float ew;
+    // split launches (parts > 1): per-chunk partial sums [chunk][S] and one
+    // arrival counter per sample tile (zeroed before the launch)
+    float2* part;
+    int* cnt;
 };
 
 // One detection job on the tensor cores (kernels_batch_gram.cu).
@@ -114,17 +142,26 @@ struct BatchCopyJob {
 // max_n: largest antenna count of the jobs (sizes the kernel's shared memory)
 cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s);
 cudaError_t launch_batch_copy(const BatchCopyJob* d_jobs, int n_jobs, int max_pairs, int max_np, cudaStream_t s);
-cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, int n_jobs, int max_cols, int max_n, BatchCommon cm,
-                              cudaStream_t s);
+// row_split: blocks per column group, each taking every row_split-th pass of
+// kColRows column entries (entries are computed alike whatever the split)
+cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, int n_jobs, int max_cols, int max_n, int row_split,
+                              BatchCommon cm, cudaStream_t s);
+int batch_kcol_group(); // columns per block
+int batch_kcol_rows();  // column entries per block pass
 size_t batch_sweep_smem(const BatchCommon& cm);
 int batch_sweep_threads();
 cudaError_t batch_sweep_occupancy(const BatchCommon& cm, int* ctas_per_sm);
 cudaError_t launch_batch_sweep(const BatchTrainJob* d_jobs, int n_jobs, BatchCommon cm, int grid, int* d_counter,
                                int* d_err, cudaStream_t s);
 // Jobs of one antenna class (N <= nmax, nmax in {4, 8, 16, 32, 64}).
-cudaError_t launch_batch_detect(const BatchDetectJob* d_jobs, int n_jobs, int max_tiles, int nmax, float wL, float wG,
-                                cudaStream_t s);
-int batch_detect_tile(); // samples per block of launch_batch_detect
+// parts: blocks that share one tile of samples, each taking a contiguous run of
+// the job's 64-pair dictionary chunks (1: one block per tile).  Results do not
+// depend on parts: every chunk's sum starts from zero and the chunk sums are
+// added in chunk order, by the block itself or by the tile's last block.
+cudaError_t launch_batch_detect(const BatchDetectJob* d_jobs, int n_jobs, int max_tiles, int parts, int nmax, float wL,
+                                float wG, cudaStream_t s);
+int batch_detect_tile();  // samples per block of launch_batch_detect
+int batch_detect_chunk(); // dictionary pairs per chunk of launch_batch_detect
 
 // Tensor-core detection of jobs with Kp <= Kp_max (Kp = 2N rounded up to 8,
 // Kp_max in {8, 16, 32, 64}): operand packing and the Gram kernel, whose CTA

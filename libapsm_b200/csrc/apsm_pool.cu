@@ -13,6 +13,11 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <condition_variable>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -38,6 +43,7 @@ struct PoolDet {
     float* y = nullptr; // cap targets
     float* a = nullptr; // cap coefficients
     float* w = nullptr; // 2N
+    float* r = nullptr; // 2N residual weights of the training sweep (w minus the dictionary's share)
 };
 
 struct Lane {
@@ -57,9 +63,24 @@ struct Lane {
         size_t off, bytes;
     };
     std::vector<CopyOut> pending; // estimates to hand to the caller once the batch finished
+    std::vector<void*> retired;   // outgrown page-locked buffers (freed with the pool)
     int* err = nullptr;           // error flag of the last batch (in the scratch)
+    int* err_host = nullptr;      // its copy in page-locked memory, written by the batch's last copy
+    bool err_copied = false;      // the last batch copies the flag (it has kernels that can set it)
     int launches = 0;             // kernels launched by the last batch
+    // batch timeline (APSM_POOL_TRACE): stream start, inputs copied, packed, kernel columns, swept,
+    // trained (dictionary copied back), detected
+    cudaEvent_t tr[7] = {};
+    double t_run0 = 0, t_run1 = 0;
+    int tr_nT = 0, tr_nD = 0;
+    bool traced = false;
 };
+
+double host_us()
+{
+    using namespace std::chrono;
+    return duration<double, std::micro>(steady_clock::now().time_since_epoch()).count();
+}
 
 // Page-locked host memory (cudaMallocHost or cudaHostRegister): copies need no staging.
 bool is_pinned(const void* p)
@@ -72,23 +93,98 @@ bool is_pinned(const void* p)
     return a.type == cudaMemoryTypeHost;
 }
 
-// Copies the inputs into the pinned staging buffer, on several threads for large batches.
-template <class In> void staged_copy(char* dst, const std::vector<In>& ins)
-{
-    size_t total = 0;
-    for (const auto& in : ins) total += in.bytes;
-    const unsigned nt = total > (size_t(16) << 20) ? std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1u;
-    if (nt <= 1) {
-        for (const auto& in : ins) std::memcpy(dst + in.off, in.src, in.bytes);
-        return;
+// Copies host inputs into a lane's page-locked staging buffer.  Batches of more
+// than kStageSplit bytes are cut into byte ranges shared with persistent helper
+// threads (started on first use), so a request loop does not pay for thread
+// creation and a large batch is not staged at one thread's memcpy bandwidth.
+class Stager {
+public:
+    ~Stager()
+    {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
     }
-    std::vector<std::thread> th;
-    for (unsigned k = 0; k < nt; ++k)
-        th.emplace_back([&, k] {
-            for (size_t i = k; i < ins.size(); i += nt) std::memcpy(dst + ins[i].off, ins[i].src, ins[i].bytes);
-        });
-    for (auto& t : th) t.join();
-}
+
+    struct Range {
+        char* dst;
+        const char* src;
+        size_t bytes;
+    };
+
+    void copy(std::vector<Range>& pieces)
+    {
+        size_t total = 0;
+        for (const auto& r : pieces) total += r.bytes;
+        if (total < kStageSplit) {
+            for (const auto& r : pieces) std::memcpy(r.dst, r.src, r.bytes);
+            return;
+        }
+        start();
+        // cut every input into kStageGrain pieces; helpers and this thread take pieces in turn
+        std::vector<Range> work;
+        for (const auto& r : pieces)
+            for (size_t o = 0; o < r.bytes; o += kStageGrain)
+                work.push_back({r.dst + o, r.src + o, std::min(kStageGrain, r.bytes - o)});
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            work_ = &work;
+            next_.store(0);
+            busy_ = unsigned(th_.size());
+            ++gen_;
+        }
+        cv_.notify_all();
+        drain(work);
+        std::unique_lock<std::mutex> lk(mu_);
+        done_cv_.wait(lk, [&] { return busy_ == 0; });
+        work_ = nullptr;
+    }
+
+private:
+    static constexpr size_t kStageSplit = size_t(1) << 20;
+    static constexpr size_t kStageGrain = size_t(256) << 10;
+
+    void drain(std::vector<Range>& work)
+    {
+        for (size_t i = next_.fetch_add(1); i < work.size(); i = next_.fetch_add(1))
+            std::memcpy(work[i].dst, work[i].src, work[i].bytes);
+    }
+
+    void start()
+    {
+        if (!th_.empty()) return;
+        const unsigned n = std::min(7u, std::max(1u, std::thread::hardware_concurrency() / 2));
+        for (unsigned k = 0; k < n; ++k)
+            th_.emplace_back([this] {
+                uint64_t seen = 0;
+                for (;;) {
+                    std::vector<Range>* w;
+                    {
+                        std::unique_lock<std::mutex> lk(mu_);
+                        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                        if (stop_) return;
+                        seen = gen_;
+                        w = work_;
+                    }
+                    drain(*w);
+                    std::lock_guard<std::mutex> g(mu_);
+                    if (--busy_ == 0) done_cv_.notify_all();
+                }
+            });
+    }
+
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    std::vector<Range>* work_ = nullptr;
+    std::atomic<size_t> next_{0};
+    unsigned busy_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
 
 int detect_class(uint32_t N)
 {
@@ -109,6 +205,10 @@ struct apsm_pool {
     int device = 0, sms = 0, sweep_ctas = 1;
     std::string last_error;
     std::mutex mu;
+    std::FILE* trace = nullptr; // batch timeline lines (env APSM_POOL_TRACE = file path)
+    bool timing = true;         // per-stage GPU events of each batch (apsm_pool_last_ms)
+    cudaMemPool_t mempool = nullptr; // lane scratch (stream-ordered; keeps its memory mapped)
+    Stager stager;                   // host-input staging (helper threads for large batches)
     std::map<uint32_t, std::vector<int>> perms;
 
     ~apsm_pool();
@@ -149,20 +249,26 @@ apsm_pool::~apsm_pool()
         if (l.scratch) cudaFree(l.scratch);
         if (l.pinned) cudaFreeHost(l.pinned);
         if (l.pinned_out) cudaFreeHost(l.pinned_out);
+        for (void* r : l.retired) cudaFreeHost(r);
         for (auto& e : l.ev)
             if (e) cudaEventDestroy(e);
         if (l.done) cudaEventDestroy(l.done);
         if (l.desc_copied) cudaEventDestroy(l.desc_copied);
+        for (auto& e : l.tr)
+            if (e) cudaEventDestroy(e);
+        if (l.err_host) cudaFreeHost(l.err_host);
         if (l.stream) cudaStreamDestroy(l.stream);
     }
     for (auto& d : dets)
         if (d.mem) cudaFree(d.mem);
+    if (mempool) cudaMemPoolDestroy(mempool);
+    if (trace) std::fclose(trace);
 }
 
 namespace {
 
 // Bytes of a detector's resident state and its sub-buffer offsets.
-size_t resident_layout(uint32_t N, uint32_t capP, size_t off[5])
+size_t resident_layout(uint32_t N, uint32_t capP, size_t off[6])
 {
     const uint32_t Np = round_up(N, 2);
     size_t o = 0;
@@ -171,6 +277,7 @@ size_t resident_layout(uint32_t N, uint32_t capP, size_t off[5])
     off[2] = o; o = align_up(o + sizeof(float) * 2 * capP, 256);
     off[3] = o; o = align_up(o + sizeof(float) * 2 * capP, 256);
     off[4] = o; o = align_up(o + sizeof(float) * 2 * N, 256);
+    off[5] = o; o = align_up(o + sizeof(float) * 2 * N, 256);
     return o;
 }
 
@@ -187,6 +294,9 @@ struct TrainPlan {
     const int* perm_dev = nullptr;
     size_t perm_off = 0;
     bool fresh = false;
+    // prologue sums of the first window's pairs over the old pairs (launch_batch_kcol)
+    int pro_n = 0, pro_w = 0, pro_lo = 0, pro_stride = 0; // pro_n: columns with sums
+    size_t off_pro = 0;
 };
 
 struct DetectPlan {
@@ -198,6 +308,7 @@ struct DetectPlan {
     int Kp = 0, tiles = 0, chunks = 0;
     size_t off_rx = 0, off_Y = 0, off_nrm = 0, off_est = 0;
     size_t off_aops = 0, off_bops = 0, off_bx = 0, off_lin = 0;
+    size_t off_part = 0, off_cnt = 0; // split CUDA-core launches: chunk sums, tile counters
 };
 
 int gram_class(int Kp)
@@ -239,6 +350,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     apsm_pool* p = this;
     Lane& L = lanes[lane_id];
     const bool host = mode != APSM_RUN_DEVICE;
+    const double t_run0 = trace ? host_us() : 0.0;
     if (!L.pending.empty()) {
         apsm_status st = finish(lane_id); // the lane's previous host batch
         if (st != APSM_OK) return st;
@@ -291,6 +403,13 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             t.n_first = t.steps.empty() ? t.nP : uint32_t(t.steps[0].hi - t.steps[0].wk) / 2;
             t.kc_base = column_prefix(t.n_first, cm.qP, t.nP, t.det->capP);
             t.n_kc = column_prefix(t.nP, cm.qP, t.nP, t.det->capP) - t.kc_base;
+            if (!t.steps.empty() && t.usedP > 0 && !t.fresh) {
+                const int hiP0 = t.steps[0].hi / 2;
+                t.pro_w = hiP0 - int(t.n_first);
+                t.pro_n = int(t.nP - t.n_first);
+                t.pro_lo = std::max(0, hiP0 - int(t.det->capP));
+                t.pro_stride = (int(t.det->capP) + cm.qP + kKcolGroup - 2 + kKcolRows - 1) / kKcolRows + 1;
+            }
             const uint32_t fhP = uint32_t(t.final_hi) / 2;
             t.usedP_new = std::min(fhP, t.det->capP);
             t.lo_new = fhP - t.usedP_new;
@@ -338,9 +457,25 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         }
 
     const size_t nT = tp.size(), nD = dp.size();
+    // CUDA-core detection: when the batch's sample tiles alone would leave most of the GPU idle
+    // (single requests), the dictionary chunks of each tile are spread over several blocks;
+    // the estimates do not depend on this (launch_batch_detect)
+    int det_parts = 1;
+    {
+        long long tiles_all = 0;
+        int chunks_max = 0;
+        const int tile = batch_detect_tile(), chunk = batch_detect_chunk();
+        for (size_t k = 0; k < nD - nG; ++k) {
+            tiles_all += (dp[k].S + tile - 1) / tile;
+            chunks_max = std::max(chunks_max, int((dp[k].Mp + chunk - 1) / chunk));
+        }
+        const long long target = 4LL * std::max(1, sms);
+        if (tiles_all > 0 && tiles_all < target)
+            det_parts = int(std::min<long long>(std::max(chunks_max, 1), (target + tiles_all - 1) / tiles_all));
+    }
     size_t nCopyIn = 0;
     for (const auto& t : tp) nCopyIn += t.usedP > 0;
-    const size_t nPack = nT + nD;
+    const size_t nPack = nT + nG; // CUDA-core detection reads the samples as the caller holds them
     // descriptor region
     size_t o = 0;
     const size_t off_tj = o; o = align_up(o + sizeof(BatchTrainJob) * nT, 256);
@@ -365,6 +500,19 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             t.perm_off = perm_off[t.P];
         }
     o = align_up(o, 256);
+    // sweep job counter + error flag, and the tile counters of split CUDA-core detection: zeroed
+    // in the host copy of the descriptors, so the one upload clears them
+    const size_t off_counter = o;
+    o = align_up(o + 256, 256);
+    const size_t off_dcnt = o;
+    if (det_parts > 1)
+        for (auto& d : dp)
+            if (!d.gram) {
+                d.off_cnt = o;
+                o += sizeof(int) * ((d.S + batch_detect_tile() - 1) / batch_detect_tile());
+            }
+    o = align_up(o, 256);
+    const size_t dcnt_bytes = o - off_dcnt;
     const size_t desc_only = o; // the descriptors alone
     if (host) { // staged host inputs travel with the descriptors
         for (auto& t : tp) {
@@ -378,7 +526,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         o = align_up(o, 256);
     }
     const size_t desc_bytes = o; // bytes of the one host-to-device copy
-    const size_t off_counter = o; o = align_up(o + 256, 256); // sweep job counter, error flag
     for (auto& t : tp) {
         const PoolDet& d = *t.det;
         t.off_Y = o; o = align_up(o + sizeof(float2) * size_t(t.nP) * d.Np, 256);
@@ -386,10 +533,21 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         t.off_y = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
         t.off_a = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
         t.off_kc = o; o = align_up(o + sizeof(float4) * size_t(std::max<long long>(t.n_kc, 1)), 256);
+        if (t.pro_n > 0) {
+            t.off_pro = o;
+            o = align_up(o + sizeof(float2) * size_t(t.pro_n) * t.pro_stride, 256);
+        }
     }
     for (auto& d : dp) {
-        d.off_Y = o; o = align_up(o + sizeof(float2) * size_t(d.S) * d.det->Np, 256);
-        d.off_nrm = o; o = align_up(o + sizeof(float) * d.S, 256);
+        if (d.gram) {
+            d.off_Y = o; o = align_up(o + sizeof(float2) * size_t(d.S) * d.det->Np, 256);
+            d.off_nrm = o; o = align_up(o + sizeof(float) * d.S, 256);
+        }
+        if (det_parts > 1 && !d.gram) {
+            const size_t chunks = (d.Mp + batch_detect_chunk() - 1) / batch_detect_chunk();
+            d.off_part = o;
+            o = align_up(o + sizeof(float2) * size_t(d.S) * std::max<size_t>(chunks, 1), 256);
+        }
         if (d.gram) {
             d.off_aops = o; o = align_up(o + batch_gram_a_bytes(d.Kp) * d.tiles, 256);
             d.off_bops = o; o = align_up(o + batch_gram_b_bytes(d.Kp) * std::max(d.chunks, 1), 256);
@@ -408,34 +566,38 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     const size_t scratch_need = o;
 
     // ---------- memory ----------
+    // Growth is geometric and never stalls the device: scratch comes from the pool's own
+    // stream-ordered memory pool (the old block is released in stream order behind the lane's
+    // earlier batches), and outgrown page-locked buffers are kept until the pool is destroyed
+    // (freeing page-locked memory can synchronize the device).
     if (scratch_need > L.scratch_bytes) {
         const uint64_t others = in_use() - L.scratch_bytes;
         if (budget && others + scratch_need > budget)
             return fail(APSM_ERR_OUT_OF_MEMORY, "batch needs " + std::to_string(scratch_need) +
                                                     " scratch bytes; the HBM budget leaves " +
                                                     std::to_string(budget > others ? budget - others : 0));
-        POOL_CK(cudaStreamSynchronize(L.stream));
-        if (L.scratch) POOL_CK(cudaFree(L.scratch));
+        size_t want = std::max(scratch_need, 2 * L.scratch_bytes);
+        if (budget && others + want > budget) want = size_t(budget - others);
+        if (L.scratch) POOL_CK(cudaFreeAsync(L.scratch, L.stream));
         L.scratch = nullptr;
         L.scratch_bytes = 0;
-        POOL_CK(cudaMalloc(&L.scratch, scratch_need));
-        L.scratch_bytes = scratch_need;
+        POOL_CK(cudaMallocFromPoolAsync(&L.scratch, want, mempool, L.stream));
+        L.scratch_bytes = want;
     }
     if (desc_bytes > L.pinned_bytes) {
         POOL_CK(cudaEventSynchronize(L.desc_copied));
-        if (L.pinned) POOL_CK(cudaFreeHost(L.pinned));
+        if (L.pinned) L.retired.push_back(L.pinned);
         L.pinned = nullptr;
+        const size_t want = std::max({desc_bytes + desc_bytes / 2, 2 * L.pinned_bytes, size_t(1) << 20});
         L.pinned_bytes = 0;
-        const size_t want = std::max<size_t>(desc_bytes + desc_bytes / 2, 1 << 16);
         POOL_CK(cudaMallocHost(&L.pinned, want));
         L.pinned_bytes = want;
     }
     if (est_bytes > L.pinned_out_bytes) {
-        POOL_CK(cudaStreamSynchronize(L.stream));
-        if (L.pinned_out) POOL_CK(cudaFreeHost(L.pinned_out));
+        if (L.pinned_out) L.retired.push_back(L.pinned_out); // no batch of this lane has results pending
         L.pinned_out = nullptr;
+        const size_t want = std::max({est_bytes + est_bytes / 2, 2 * L.pinned_out_bytes, size_t(1) << 18});
         L.pinned_out_bytes = 0;
-        const size_t want = std::max<size_t>(est_bytes + est_bytes / 2, 1 << 16);
         POOL_CK(cudaMallocHost(&L.pinned_out, want));
         L.pinned_out_bytes = want;
     }
@@ -479,6 +641,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         tj.y = yv;
         tj.a = av;
         tj.w = d.w;
+        tj.r = d.r;
         tj.Kc = reinterpret_cast<const float4*>(D(t.off_kc));
         tj.steps = reinterpret_cast<const TrainStep*>(D(t.off_steps));
         tj.n_steps = int(t.steps.size());
@@ -491,6 +654,11 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         tj.kc_base = t.kc_base;
         tj.ew = d.ew;
         tj.fresh = t.fresh ? 1 : 0;
+        tj.pro = t.pro_n > 0 ? reinterpret_cast<float2*>(D(t.off_pro)) : nullptr;
+        tj.pro_w = t.pro_w;
+        tj.pro_lo = t.pro_lo;
+        tj.pro_hi = int(t.usedP);
+        tj.pro_stride = t.pro_stride;
         h_tj[k] = tj;
         max_cols = std::max(max_cols, int(t.nP - t.n_first));
         h_co[k] = BatchCopyJob{Y + size_t(t.lo_new) * d.Np, nrm + t.lo_new, yv + 2 * t.lo_new, av + 2 * t.lo_new,
@@ -504,14 +672,19 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         PoolDet& d = *q.det;
         const apsm_job& j = jobs[q.job];
         const float2* rx = host ? reinterpret_cast<const float2*>(D(q.off_rx)) : reinterpret_cast<const float2*>(j.rx);
-        auto* Ys = reinterpret_cast<float2*>(D(q.off_Y));
-        auto* ns = reinterpret_cast<float*>(D(q.off_nrm));
-        h_pj[ipack++] = BatchPackJob{rx, nullptr, nullptr, Ys, ns, nullptr, nullptr, int(q.S), int(d.N), int(d.Np)};
-        max_len = std::max(max_len, int(q.S));
-        max_np = std::max(max_np, int(d.Np));
-        max_n = std::max(max_n, int(d.N));
+        auto* Ys = q.gram ? reinterpret_cast<float2*>(D(q.off_Y)) : nullptr;
+        auto* ns = q.gram ? reinterpret_cast<float*>(D(q.off_nrm)) : nullptr;
+        if (q.gram) {
+            h_pj[ipack++] = BatchPackJob{rx, nullptr, nullptr, Ys, ns, nullptr, nullptr, int(q.S), int(d.N), int(d.Np)};
+            max_len = std::max(max_len, int(q.S));
+            max_np = std::max(max_np, int(d.Np));
+            max_n = std::max(max_n, int(d.N));
+        }
         float2* out = host ? reinterpret_cast<float2*>(D(q.off_est)) : reinterpret_cast<float2*>(j.est);
-        h_dj[k] = BatchDetectJob{Ys, ns, d.Y, d.nrm, d.a, d.w, out, int(q.S), int(q.Mp), int(d.N), int(d.Np), d.ew};
+        const bool split = det_parts > 1 && !q.gram;
+        h_dj[k] = BatchDetectJob{rx,       d.Y,       d.nrm, d.a,  d.w, out, int(q.S), int(q.Mp), int(d.N), int(d.Np),
+                                 d.ew,     split ? reinterpret_cast<float2*>(D(q.off_part)) : nullptr,
+                                 split ? reinterpret_cast<int*>(D(q.off_cnt)) : nullptr};
         if (q.gram) {
             BatchGramJob g{};
             g.Ys = Ys;
@@ -581,25 +754,35 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                 direct = false;
                 break;
             }
-        if (!direct) staged_copy(hst, ins);
+        if (!direct) {
+            std::vector<Stager::Range> pieces;
+            pieces.reserve(ins.size());
+            for (const auto& in : ins)
+                pieces.push_back({hst + in.off, static_cast<const char*>(in.src), in.bytes});
+            stager.copy(pieces);
+        }
     }
+    std::memset(hst + off_counter, 0, off_dcnt - off_counter + dcnt_bytes);
+    if (trace) POOL_CK(cudaEventRecord(L.tr[0], s));
     POOL_CK(cudaMemcpyAsync(dev, hst, direct ? desc_only : desc_bytes, cudaMemcpyHostToDevice, s));
     if (direct)
         for (const auto& in : ins) POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, s));
     POOL_CK(cudaEventRecord(L.desc_copied, s));
-    L.have_train = nT > 0;
-    L.have_detect = nD > 0;
+    L.have_train = timing && nT > 0;
+    L.have_detect = timing && nD > 0;
     for (PoolDet* d : resets) {
         POOL_CK(cudaMemsetAsync(d->w, 0, sizeof(float) * 2 * d->N, s));
+        POOL_CK(cudaMemsetAsync(d->r, 0, sizeof(float) * 2 * d->N, s));
         d->used = 0;
     }
     int* d_counter = reinterpret_cast<int*>(D(off_counter));
     int* d_err = d_counter + 4;
-    POOL_CK(cudaMemsetAsync(d_counter, 0, 32, s));
+
     L.err = d_err;
     L.launches = 0;
+    if (trace) POOL_CK(cudaEventRecord(L.tr[1], s));
     if (nT > 0) {
-        POOL_CK(cudaEventRecord(L.ev[0], s));
+        if (timing) POOL_CK(cudaEventRecord(L.ev[0], s));
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_ci)), int(nCopyIn), max_pairs_in, max_np, s));
         L.launches += nCopyIn > 0 && max_pairs_in > 0;
     }
@@ -607,20 +790,36 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)), int(nPack), max_len, max_n, s));
         L.launches += max_len > 0;
     }
+    if (trace) POOL_CK(cudaEventRecord(L.tr[2], s));
     if (nT > 0) {
         const auto* d_tj = reinterpret_cast<const BatchTrainJob*>(D(off_tj));
-        POOL_CK(launch_batch_kcol(d_tj, int(nT), max_cols, max_n, cm, s));
+        // small batches (single train requests): spread each column group's rows over blocks
+        int row_split = 1;
+        {
+            const long long blocks = (long long)nT * ((max_cols + batch_kcol_group() - 1) / batch_kcol_group());
+            const int passes = int((int(cfg.dict_size) + cm.qP + batch_kcol_rows() - 1) / batch_kcol_rows());
+            const long long target = 4LL * std::max(1, sms);
+            if (blocks > 0 && blocks < target)
+                row_split = int(std::min<long long>(std::max(passes, 1), (target + blocks - 1) / blocks));
+        }
+        POOL_CK(launch_batch_kcol(d_tj, int(nT), max_cols, max_n, row_split, cm, s));
+        if (trace) POOL_CK(cudaEventRecord(L.tr[3], s));
         const int grid = int(std::min<size_t>(nT, size_t(sweep_ctas) * sms));
-        POOL_CK(cudaEventRecord(L.ev[4], s));
+        if (timing) POOL_CK(cudaEventRecord(L.ev[4], s));
         POOL_CK(launch_batch_sweep(d_tj, int(nT), cm, grid, d_counter, d_err, s));
-        POOL_CK(cudaEventRecord(L.ev[5], s));
+        if (timing) POOL_CK(cudaEventRecord(L.ev[5], s));
+        if (trace) POOL_CK(cudaEventRecord(L.tr[4], s));
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_co)), int(nT), max_pairs_out, max_np, s));
         L.launches += (max_cols > 0) + 1 + (max_pairs_out > 0);
-        POOL_CK(cudaEventRecord(L.ev[1], s));
+        if (timing) POOL_CK(cudaEventRecord(L.ev[1], s));
         for (const auto& t : tp) t.det->used = 2 * t.usedP_new;
+    } else if (trace) {
+        POOL_CK(cudaEventRecord(L.tr[3], s));
+        POOL_CK(cudaEventRecord(L.tr[4], s));
     }
+    if (trace) POOL_CK(cudaEventRecord(L.tr[5], s));
     if (nD > 0) {
-        POOL_CK(cudaEventRecord(L.ev[2], s));
+        if (timing) POOL_CK(cudaEventRecord(L.ev[2], s));
         const auto* d_dj = reinterpret_cast<const BatchDetectJob*>(D(off_dj));
         size_t k0 = 0;
         const size_t nC = nD - nG; // CUDA-core jobs come first
@@ -631,7 +830,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                 tiles = std::max(tiles, int((dp[k1].S + batch_detect_tile() - 1) / batch_detect_tile()));
                 ++k1;
             }
-            POOL_CK(launch_batch_detect(d_dj + k0, int(k1 - k0), tiles, dp[k0].cls, cfg.wL, cfg.wG, s));
+            POOL_CK(launch_batch_detect(d_dj + k0, int(k1 - k0), tiles, det_parts, dp[k0].cls, cfg.wL, cfg.wG, s));
             L.launches += tiles > 0;
             k0 = k1;
         }
@@ -643,7 +842,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                                       cfg.wG, d_err, s));
             L.launches += (g[4] > 0) + (g[5] > 0) + (g[3] > 0);
         }
-        POOL_CK(cudaEventRecord(L.ev[3], s));
+        if (timing) POOL_CK(cudaEventRecord(L.ev[3], s));
         if (host && est_bytes > 0) {
             bool out_direct = true;
             for (const auto& q : dp)
@@ -661,6 +860,18 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             }
         }
     }
+    // the error flag of kernels with bounded waits (sweep, tensor-core detection) travels back with
+    // the batch: finish() reads it without a synchronous copy
+    L.err_copied = nT > 0 || nG > 0;
+    if (L.err_copied) POOL_CK(cudaMemcpyAsync(L.err_host, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (trace) {
+        POOL_CK(cudaEventRecord(L.tr[6], s));
+        L.traced = true;
+        L.tr_nT = int(nT);
+        L.tr_nD = int(nD);
+        L.t_run0 = t_run0;
+        L.t_run1 = host_us();
+    }
     POOL_CK(cudaEventRecord(L.done, s));
     if (mode == APSM_RUN_HOST) return finish(lane_id);
     return APSM_OK;
@@ -670,19 +881,34 @@ apsm_status apsm_pool::finish(uint32_t lane_id)
 {
     apsm_pool* p = this;
     Lane& L = lanes[lane_id];
+    const double t0 = trace ? host_us() : 0.0;
     POOL_CK(cudaEventSynchronize(L.done));
+    const double t1 = trace ? host_us() : 0.0;
     for (const auto& c : L.pending) std::memcpy(c.dst, static_cast<char*>(L.pinned_out) + c.off, c.bytes);
     L.pending.clear();
-    return check_lane(lane_id);
+    const apsm_status st = check_lane(lane_id);
+    if (trace && L.traced) {
+        // one line per batch: lane, jobs, host run() time, host gap until finish(), finish's wait and rest,
+        // GPU: inputs copied, packed, kernel columns, sweep, dictionary copied back, detected (+ results
+        // copied) -- microseconds
+        float g[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 6; ++k)
+            if (cudaEventElapsedTime(&g[k], L.tr[k], L.tr[k + 1]) != cudaSuccess) g[k] = -1e-3f;
+        cudaGetLastError();
+        std::fprintf(trace, "%u %d %d %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f\n", lane_id, L.tr_nT, L.tr_nD,
+                     L.t_run1 - L.t_run0, t0 - L.t_run1, t1 - t0, host_us() - t1, 1e3 * g[0], 1e3 * g[1], 1e3 * g[2],
+                     1e3 * g[3], 1e3 * g[4], 1e3 * g[5]);
+        L.traced = false;
+    }
+    return st;
 }
 
 apsm_status apsm_pool::check_lane(uint32_t lane_id)
 {
     apsm_pool* p = this;
     Lane& L = lanes[lane_id];
-    if (!L.err) return APSM_OK;
-    int h = 0;
-    POOL_CK(cudaMemcpy(&h, L.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!L.err || !L.err_host || !L.err_copied) return APSM_OK;
+    const int h = *static_cast<volatile int*>(L.err_host); // copied by the batch before its done event
     if (h) return fail(APSM_ERR_CUDA, "a bounded wait in a tensor-core kernel expired (results of the batch are invalid)");
     return APSM_OK;
 }
@@ -761,6 +987,16 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
         return failp("cudaGetDeviceProperties failed", APSM_ERR_CUDA);
     if (prop.major < 10) return failp("an sm_100 (Blackwell) device is required", APSM_ERR_NO_DEVICE);
     p->sms = prop.multiProcessorCount;
+    {
+        cudaMemPoolProps mp = {};
+        mp.allocType = cudaMemAllocationTypePinned;
+        mp.handleTypes = cudaMemHandleTypeNone;
+        mp.location.type = cudaMemLocationTypeDevice;
+        mp.location.id = p->device;
+        if (cudaMemPoolCreate(&p->mempool, &mp) != cudaSuccess) return failp("cudaMemPoolCreate failed", APSM_ERR_CUDA);
+        uint64_t keep = ~0ull; // released memory stays with the pool for the next growth
+        cudaMemPoolSetAttribute(p->mempool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     p->lanes.resize(lanes);
     for (auto& l : p->lanes) {
         if (cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -770,8 +1006,19 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
         if (cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&l.desc_copied, cudaEventDisableTiming) != cudaSuccess)
             return failp("cudaEventCreate failed", APSM_ERR_CUDA);
+        for (auto& e : l.tr)
+            if (cudaEventCreate(&e) != cudaSuccess) return failp("cudaEventCreate failed", APSM_ERR_CUDA);
+        if (cudaMallocHost(reinterpret_cast<void**>(&l.err_host), sizeof(int)) != cudaSuccess)
+            return failp("cudaMallocHost failed", APSM_ERR_CUDA);
+        *l.err_host = 0;
         cudaEventRecord(l.done, l.stream);
         cudaEventRecord(l.desc_copied, l.stream);
+    }
+    if (const char* path = std::getenv("APSM_POOL_TRACE")) {
+        p->trace = std::fopen(path, "w");
+        if (p->trace)
+            std::fprintf(p->trace, "# lane n_train n_detect run_us gap_us fin_wait_us fin_rest_us gpu_inputs_us "
+                                   "gpu_pack_us gpu_kcol_us gpu_sweep_us gpu_copyout_us gpu_detect_us\n");
     }
     if (batch_sweep_occupancy(cm, &p->sweep_ctas) != cudaSuccess || p->sweep_ctas < 1)
         return failp("the training sweep does not fit an SM", APSM_ERR_UNSUPPORTED);
@@ -796,7 +1043,7 @@ extern "C" apsm_status apsm_pool_add(apsm_pool* p, uint32_t num_antennas, uint32
     d.capP = p->cfg.dict_size;
     d.cap = 2 * d.capP;
     d.ew = -0.5f / (p->cfg.variance * float(num_antennas * num_antennas));
-    size_t off[5];
+    size_t off[6];
     d.bytes = resident_layout(d.N, d.capP, off);
     if (p->budget && p->in_use() + d.bytes > p->budget)
         return p->fail(APSM_ERR_OUT_OF_MEMORY, "detector state of " + std::to_string(d.bytes) +
@@ -819,6 +1066,7 @@ extern "C" apsm_status apsm_pool_add(apsm_pool* p, uint32_t num_antennas, uint32
     d.y = reinterpret_cast<float*>(m + off[2]);
     d.a = reinterpret_cast<float*>(m + off[3]);
     d.w = reinterpret_cast<float*>(m + off[4]);
+    d.r = reinterpret_cast<float*>(m + off[5]);
     e = cudaMemset(d.mem, 0, d.bytes);
     if (e != cudaSuccess) {
         cudaFree(d.mem);
@@ -955,6 +1203,14 @@ extern "C" int apsm_pool_last_launches(apsm_pool* p, uint32_t lane)
 {
     if (!p || lane >= p->lanes.size()) return -1;
     return p->lanes[lane].launches;
+}
+
+extern "C" apsm_status apsm_pool_set_timing(apsm_pool* p, int on)
+{
+    if (!p) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    p->timing = on != 0;
+    return APSM_OK;
 }
 
 extern "C" apsm_status apsm_pool_last_sweep_ms(apsm_pool* p, uint32_t lane, float* sweep_ms)

@@ -12,7 +12,11 @@
 //   * a detection request is not put before a training request of the same
 //     detector that arrived earlier (a batch runs its training jobs first);
 //   * the batch is bounded by a request count and by the device scratch the
-//     pool's HBM budget leaves per lane (apsm_pool_job_bytes).
+//     pool's HBM budget leaves per lane (apsm_pool_job_bytes);
+//   * a batch holds one kind of request, that of its oldest admitted request,
+//     so detections never wait behind a training sweep in the same batch
+//     (a detector whose next request is of the other kind waits for a later
+//     batch, keeping its order).
 // Batches on different lanes overlap on the device.  Request times are taken
 // with a monotonic host clock: submission, admission and completion.
 #include "apsm_b200.h"
@@ -97,11 +101,13 @@ bool apsm_server::admit(uint32_t lane)
     std::vector<apsm_job> jobs;
     std::unordered_set<uint32_t> blocked, trained, detected;
     uint64_t bytes = 0;
+    int batch_kind = -1;
     for (auto it = queue.begin(); it != queue.end() && jobs.size() < max_batch;) {
         const uint64_t tk = *it;
         const apsm_job& j = reqs[tk].job;
         const uint32_t d = j.detector;
         bool ok = !busy_dets.count(d) && !blocked.count(d);
+        if (ok && batch_kind >= 0 && int(j.kind) != batch_kind) ok = false;
         if (ok && j.kind == APSM_JOB_TRAIN && (trained.count(d) || detected.count(d))) ok = false;
         const uint64_t b = apsm_pool_job_bytes(pool, &j);
         if (ok && !jobs.empty() && bytes + b > cap) ok = false;
@@ -111,6 +117,7 @@ bool apsm_server::admit(uint32_t lane)
             continue;
         }
         bytes += b;
+        batch_kind = int(j.kind);
         (j.kind == APSM_JOB_TRAIN ? trained : detected).insert(d);
         jobs.push_back(j);
         take.push_back(tk);
@@ -177,6 +184,7 @@ extern "C" apsm_status apsm_server_create(apsm_pool* pool, uint32_t lanes, uint3
     for (uint32_t l = 0; l < lanes; ++l)
         if (!apsm_pool_stream(pool, l)) return APSM_ERR_INVALID_ARGUMENT;
     auto* s = new apsm_server();
+    apsm_pool_set_timing(pool, 0); // per-stage events cost latency; the server reports request times
     s->pool = pool;
     s->n_lanes = lanes;
     s->max_batch = max_batch;

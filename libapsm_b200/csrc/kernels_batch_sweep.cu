@@ -82,6 +82,29 @@ __device__ __forceinline__ void acc_pair(float2 ab, float4 kv, float& g0, float&
     g1 = fmaf(ab.x, kv.y, fmaf(ab.y, kv.x, g1));
 }
 
+// asynchronous global -> shared copies (complete at cp_async_wait_all)
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst))),
+                 "l"(gmem_src)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gmem_src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst))),
+                 "l"(gmem_src)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 __device__ __forceinline__ void warp_sum2(float& a, float& b)
 {
 #pragma unroll
@@ -92,6 +115,41 @@ __device__ __forceinline__ void warp_sum2(float& a, float& b)
 }
 
 } // namespace
+
+#ifdef APSM_SWEEP_PROFILE
+// Profiling builds: globaltimer stamps of block 0's jobs (setup, prologue, each step, end).
+__device__ unsigned long long g_sweep_prof[64][6]; // start, setup, prologue, steps, final w, n_steps
+__device__ unsigned int g_sweep_prof_n;
+#define SWEEP_MARK(k)                                                                                        \
+    do {                                                                                                     \
+        if (blockIdx.x == 0 && tid == 0 && g_sweep_prof_n < 64) {                                           \
+            unsigned long long t_;                                                                           \
+            asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t_));                                           \
+            g_sweep_prof[g_sweep_prof_n][k] = t_;                                                            \
+        }                                                                                                    \
+    } while (0)
+extern "C" void apsm_sweep_prof_read(unsigned long long* out, unsigned int* n)
+{
+    cudaMemcpyFromSymbol(out, g_sweep_prof, sizeof(g_sweep_prof));
+    cudaMemcpyFromSymbol(n, g_sweep_prof_n, sizeof(unsigned int));
+    const unsigned int z = 0;
+    cudaMemcpyToSymbol(g_sweep_prof_n, &z, sizeof(z));
+}
+// per-step phase stamps of block 0's first job (clock64): loop top, phase 1 done, window
+// update done, evictions done, step end
+__device__ long long g_sweep_steps[64][8];
+#define STEP_MARK(k)                                                                                         \
+    do {                                                                                                     \
+        if (blockIdx.x == 0 && tid == 0 && g_sweep_prof_n == 0 && t < 64) g_sweep_steps[t][k] = clock64();  \
+    } while (0)
+extern "C" void apsm_sweep_steps_read(long long* out)
+{
+    cudaMemcpyFromSymbol(out, g_sweep_steps, sizeof(g_sweep_steps));
+}
+#else
+#define SWEEP_MARK(k)
+#define STEP_MARK(k)
+#endif
 
 __global__ void __launch_bounds__(kThreads, 2)
     batch_sweep_kernel(const BatchTrainJob* __restrict__ jobs, int n_jobs, BatchCommon cm, int* counter)
@@ -108,8 +166,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     float* KA = smem;                                        // [XSP][XSPp]
     float* KP = KA + XSP * XSPp;                             // [XSP][XSPp]
     float* KM = KP + XSP * XSPp;                             // [XSP][XSPp]
-    float2* Yw = reinterpret_cast<float2*>(KM + XSP * XSPp); // [XSP][Np]
-    float* hw = reinterpret_cast<float*>(Yw + XSP * cm.Np);  // [2 XSPp] predictions by row slot
+    float2* Yw = reinterpret_cast<float2*>(KM + XSP * XSPp); // [XSP][Np + 1] (odd pitch: row-slot threads
+                                                             // reading one feature each hit distinct banks)
+    // (the region is rounded up to whole 16-byte units: red below takes float4 stores)
+    float* hw = reinterpret_cast<float*>(Yw + round_up(uint32_t(XSP * (cm.Np + 1)), 2u)); // [2 XSPp] predictions
     float* yw = hw + 2 * XSPp;                               // targets
     float* aw = yw + 2 * XSPp;                               // coefficients
     float* cs = aw + 2 * XSPp;                               // corrections of the step (0 when inactive)
@@ -120,6 +180,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     float* wp = dr + kMaxFeatures;                           // [kMaxEnter][kWarps][2] entering partial sums (direct loads)
     float* wpf = wp + 2 * kMaxEnter * kWarps;                // [2][kWarps][2] frozen partial sums by step parity
     float* wpe = wpf + 4 * kWarps;                           // [2][2] window part + linear term (warps 6-7)
+    float2* ev_y = reinterpret_cast<float2*>(wpe + 4);       // [kMaxEnter][Np] pairs evicted at a step
+    float* ev_a = reinterpret_cast<float*>(ev_y + kMaxEnter * cm.Np); // [2 kMaxEnter] their coefficients
+    float* wpr = ev_a + 2 * kMaxEnter;                       // [4][2] old-pair sums of entering pairs (slot tt % 4)
+    float* nws = wpr + 8;                                    // [XSPp] squared norms by pair slot
+    float* ev_n = nws + XSPp;                                // [kMaxEnter] norms of the evicted pairs
 
     for (;;) {
         __syncthreads();
@@ -129,6 +194,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         __syncthreads();
         if (job_s >= n_jobs) break;
+        SWEEP_MARK(0);
         const int N = js.N, Np = js.Np, capP = js.capP, nP = js.nP, n_steps = js.n_steps;
         const int D = 2 * N;
         const float ew = js.ew;
@@ -181,14 +247,17 @@ __global__ void __launch_bounds__(kThreads, 2)
 
         // ---- job state ----
         for (int i = tid; i < 3 * XSP * XSPp; i += kThreads) KA[i] = 0.f;
-        for (int i = tid; i < XSP * Np; i += kThreads) Yw[i] = make_float2(0.f, 0.f);
+        const int YP = Np + 1; // pitch of the window samples
+        for (int i = tid; i < XSP * YP; i += kThreads) Yw[i] = make_float2(0.f, 0.f);
         for (int i = tid; i < 2 * XSPp; i += kThreads) hw[i] = yw[i] = aw[i] = cs[i] = 0.f;
-        for (int i = tid; i < XSPp; i += kThreads) rd[i] = 0.f;
+        for (int i = tid; i < XSPp; i += kThreads) rd[i] = nws[i] = 0.f;
         for (int i = tid; i < kParts * 2 * XSPp; i += kThreads) red[i] = 0.f;
         PairStep pc = pair_step(n_steps > 0 ? steps[0] : make_int4(0, 0, 0, 0), capP);
+        // residual weights as the detector's last sweep left them (0 for a fresh detector), plus the
+        // share of the old pairs [0, loP) that leave the dictionary before this call's first step
         for (int d = tid; d < kMaxFeatures; d += kThreads) {
             float r = 0.f;
-            if (d < D && !js.fresh) r = js.w[d] - (n_steps > 0 ? ax_sum(d, pc.loP, js.used_beforeP) : 0.f);
+            if (d < D && !js.fresh) r = js.r[d] + (n_steps > 0 && pc.loP > 0 ? ax_sum(d, 0, pc.loP) : 0.f);
             r_s[d] = r;
         }
         if (n_steps <= 0) continue; // w unchanged
@@ -198,17 +267,32 @@ __global__ void __launch_bounds__(kThreads, 2)
         int4 st_nn = steps[n_steps > 2 ? 2 : 0];
         int4 st_3 = steps[n_steps > 3 ? 3 : 0];
 
+        SWEEP_MARK(1);
         // ---- prologue: the pairs of the first window enter with direct loads ----
         {
             const int e_lo = pc.sP, e_hi = pc.hiP, top = js.used_beforeP;
             for (int j = e_lo + warp; j < e_hi; j += kWarps) {
                 const int q = j % XSP;
-                for (int k = lane; k < Np; k += 32) Yw[q * Np + k] = Y[size_t(j) * Np + k];
+                for (int k = lane; k < Np; k += 32) Yw[q * YP + k] = Y[size_t(j) * Np + k];
                 float g0 = 0.f, g1 = 0.f;
                 const float4* col = col_ptr(j);
+                if (js.pro && j - e_lo < js.pro_w) {
+                    // the kernel-column launch summed the old pairs per pass of its column group
+                    if (lane == 0) {
+                        const int n0 = js.n_first + (j - js.n_first) / kKcolGroup * kKcolGroup;
+                        const int nc = min(kKcolGroup, nP - n0);
+                        const int b_lo = col_begin(n0, capP), b_hi = col_end(n0 + nc - 1, qP, nP);
+                        const float2* pr = js.pro + size_t(j - js.n_first) * js.pro_stride;
+                        for (int ps = 0; ps < (b_hi - b_lo + kKcolRows - 1) / kKcolRows; ++ps) {
+                            g0 += pr[ps].x;
+                            g1 += pr[ps].y;
+                        }
+                    }
+                } else {
 #pragma unroll 8
-                for (int b = pc.loP + lane; b < top; b += 32)
-                    acc_pair(*reinterpret_cast<const float2*>(ag + 2 * b), __ldg(col + b), g0, g1);
+                    for (int b = pc.loP + lane; b < top; b += 32)
+                        acc_pair(*reinterpret_cast<const float2*>(ag + 2 * b), __ldg(col + b), g0, g1);
+                }
                 for (int d = lane; d < D; d += 32) lin_feature(d, r_s[d], Y[size_t(j) * Np + d % N], g0, g1);
                 warp_sum2(g0, g1);
                 if (lane == 0) {
@@ -219,6 +303,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     aw[2 * q] = ag[2 * j];
                     aw[2 * q + 1] = ag[2 * j + 1];
                     rd[q] = 1.f / fmaf(wL, js.nrm[j], wG);
+                    nws[q] = js.nrm[j];
                 }
                 for (int b = max(e_lo, j - LB + 1) + lane; b <= j; b += 32) fill_band(b % XSP, q, col[b]);
             }
@@ -245,16 +330,38 @@ __global__ void __launch_bounds__(kThreads, 2)
             e_nxt.lo = ps.loP;
             e_nxt.top = pv.hiP;
             e_nxt.F = min(max(F, e_nxt.lo), e_nxt.top);
-            if (ne != 1 || e_nxt.F - e_nxt.lo > kThreads * kPf || e_nxt.top - e_nxt.F > 2 * kEntThreads ||
+            // old pairs below n_first were summed by the kernel-column launch (appending calls)
+            const int fl = js.pro ? min(max(e_nxt.lo, js.n_first), e_nxt.F) : e_nxt.lo;
+            if (ne != 1 || e_nxt.F - fl > kThreads * kPf || e_nxt.top - e_nxt.F > 2 * kEntThreads ||
                 D > 2 * kEntThreads) {
                 e_nxt.slow = 1;
                 return;
             }
             const int n = e_lo;
             const float4* col = col_ptr(n);
+            if (warp == 5) {
+                // the pair's old-pair sums (one per kernel-column pass): lanes take passes, shuffle sum
+                float p0 = 0.f, p1 = 0.f;
+                if (js.pro) {
+                    const int n0 = js.n_first + (n - js.n_first) / kKcolGroup * kKcolGroup;
+                    const int nc = min(kKcolGroup, nP - n0);
+                    const int b_lo = col_begin(n0, capP), b_hi = col_end(n0 + nc - 1, qP, nP);
+                    const float2* pr = js.pro + size_t(n - js.n_first) * js.pro_stride;
+                    const int passes = (b_hi - b_lo + kKcolRows - 1) / kKcolRows;
+                    for (int ps2 = lane; ps2 < passes; ps2 += 32) {
+                        p0 += pr[ps2].x;
+                        p1 += pr[ps2].y;
+                    }
+                }
+                warp_sum2(p0, p1);
+                if (lane == 0) {
+                    wpr[2 * (tt & 3)] = p0;
+                    wpr[2 * (tt & 3) + 1] = p1;
+                }
+            }
 #pragma unroll
             for (int k = 0; k < kPf; ++k) {
-                const int b = e_nxt.lo + tid + k * kThreads;
+                const int b = fl + tid + k * kThreads;
                 const bool ok = b < e_nxt.F;
                 colbuf[k] = ok ? __ldg(col + b) : make_float4(0.f, 0.f, 0.f, 0.f);
                 abuf[k] = ok ? *reinterpret_cast<const float2*>(ag + 2 * b) : make_float2(0.f, 0.f);
@@ -298,6 +405,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         issue(2, st_nn, st_n, pc.sP);
         __syncthreads();
 
+        SWEEP_MARK(2);
         int los = pc.sP % XSP; // slot of the window's first pair
 #pragma unroll 1
         for (int t = 0; t < n_steps; ++t) {
@@ -308,6 +416,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int4 st_4 = t + 4 < n_steps ? steps[t + 4] : st_3;
             const float inv_wk = 1.f / float(pc.wk);
 
+            STEP_MARK(0);
             // ================= phase 1 =================
             // (1a) window rows: fold the last update in; corrections of the active rows
             for (int r = tid; r < 2 * XSP && tid < kRowThreads; r += kRowThreads) {
@@ -349,12 +458,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                     wpe[2 * (warp - kRowThreads / 32)] = g0;
                     wpe[2 * (warp - kRowThreads / 32) + 1] = g1;
                 }
-                if (et < Np) Yw[qn * Np + et] = et < N ? y_cur0 : make_float2(0.f, 0.f);
+                if (et < Np) Yw[qn * YP + et] = et < N ? y_cur0 : make_float2(0.f, 0.f);
                 if (et == 0) {
                     yw[2 * qn] = t_cur0;
                     yw[2 * qn + 1] = t_cur1;
                     aw[2 * qn] = aw[2 * qn + 1] = 0.f;
                     rd[qn] = 1.f / fmaf(wL, n_cur, wG);
+                    nws[qn] = n_cur;
                     fill_diag(qn, n_cur);
                 }
               }
@@ -377,19 +487,32 @@ __global__ void __launch_bounds__(kThreads, 2)
                         wp[(e * kWarps + warp) * 2 + 1] = g1;
                     }
                     for (int b = max(0, n - LB + 1) + tid; b < n; b += kThreads) fill_band(b % XSP, qn, col[b]);
-                    for (int k = tid; k < Np; k += kThreads) Yw[qn * Np + k] = Y[size_t(n) * Np + k];
+                    for (int k = tid; k < Np; k += kThreads) Yw[qn * YP + k] = Y[size_t(n) * Np + k];
                     if (tid == 0) {
                         yw[2 * qn] = js.y[2 * n];
                         yw[2 * qn + 1] = js.y[2 * n + 1];
                         aw[2 * qn] = aw[2 * qn + 1] = 0.f;
                         rd[qn] = 1.f / fmaf(wL, js.nrm[n], wG);
+                        nws[qn] = js.nrm[n];
                         fill_diag(qn, js.nrm[n]);
                     }
                 }
             }
             __syncthreads();
+            STEP_MARK(1);
 
             // ================= phase 2 =================
+            // A single pair leaving the dictionary at t+1: its sample, norm and coefficients are
+            // fetched now and used after the window update, which hides their load latency.
+            const bool evict = has_next && pn.loP > pc.loP;
+            const int nev = evict ? pn.loP - pc.loP : 0;
+            const bool ev1 = nev == 1;
+            const int lons = pn.sP % XSP;
+            if (ev1) { // copied into shared memory in the background
+                if (tid < Np) cp_async8(ev_y + tid, Y + size_t(pc.loP) * Np + tid);
+                if (tid == Np) cp_async8(ev_a, ag + 2 * pc.loP);
+                if (tid == Np + 1) cp_async4(ev_n, js.nrm + pc.loP);
+            }
             // (2a) window update partials: red[part][row] = sum_{p in part} c_p Kt(p, .)
             for (int idx = tid; idx < ncp * kParts; idx += kThreads) {
                 const int cp = idx % ncp, part = idx / ncp;
@@ -411,6 +534,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
                 *reinterpret_cast<float4*>(red + part * 2 * XSPp + 4 * cp) = make_float4(h00, h01, h10, h11);
             }
+            STEP_MARK(2);
             // (2b) coefficients of the active rows (apsm_train.cu:407)
             for (int r = tid; r < 2 * XSP; r += kThreads) {
                 int d = (r >> 1) - los;
@@ -422,37 +546,73 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
             }
             // (2c) evicted pairs: dr = sum a_b x_b joins r; their Gaussian terms leave the rows that stay
-            const bool evict = has_next && pn.loP > pc.loP;
             if (evict) {
+                // the evicted pairs' samples and coefficients, staged once for all window rows
+                const bool staged = nev <= kMaxEnter;
+                if (ev1) {
+                    cp_async_commit_wait_all();
+                    STEP_MARK(5);
+                    __syncthreads();
+                    STEP_MARK(6);
+                } else if (staged) {
+                    for (int i = tid; i < nev * Np; i += kThreads) ev_y[i] = Y[size_t(pc.loP) * Np + i];
+                    for (int i = tid; i < 2 * nev; i += kThreads) ev_a[i] = ag[2 * pc.loP + i];
+                    for (int i = tid; i < nev; i += kThreads) ev_n[i] = js.nrm[pc.loP + i];
+                    __syncthreads();
+                }
                 for (int d = tid; d < kMaxFeatures; d += kThreads) {
-                    const float v = d < D ? ax_sum(d, pc.loP, pn.loP) : 0.f;
+                    float v = 0.f;
+                    if (d < D) {
+                        if (staged) {
+                            const int k = d < N ? d : d - N;
+                            for (int e = 0; e < nev; ++e) {
+                                const float2 ab = make_float2(ev_a[2 * e], ev_a[2 * e + 1]);
+                                const float2 yv = ev_y[e * Np + k];
+                                v = d < N ? fmaf(ab.x, yv.x, fmaf(ab.y, yv.y, v)) : fmaf(ab.x, yv.y, fmaf(-ab.y, yv.x, v));
+                            }
+                        } else {
+                            v = ax_sum(d, pc.loP, pn.loP);
+                        }
+                    }
                     dr[d] = v;
                     r_s[d] += v;
                 }
-                const int lons = pn.sP % XSP;
                 for (int q = tid; q < XSP; q += kThreads) {
                     int dd = q - lons;
                     if (dd < 0) dd += XSP;
                     const int p = pn.sP + dd;
                     if (p >= pc.hiP) continue;
-                    const float4* col = col_ptr(p);
                     float g0 = 0.f, g1 = 0.f;
-                    for (int b = pc.loP; b < pn.loP; ++b) {
+                    // the Gaussian kernel of pair b against the row's pair, from y_b^H y_p and the norms
+                    // (the expressions of the kernel columns)
+                    auto evict_term = [&](const float2* yrow, float nb, float2 ab) {
                         float re = 0.f, im = 0.f;
+#pragma unroll 4
                         for (int k = 0; k < N; ++k) {
-                            const float2 yb = Y[size_t(b) * Np + k], yj = Yw[q * Np + k];
+                            const float2 yb = yrow[k], yj = Yw[q * YP + k];
                             re = fmaf(yb.x, yj.x, fmaf(yb.y, yj.y, re));
                             im = fmaf(yb.x, yj.y, fmaf(-yb.y, yj.x, im));
                         }
-                        const float4 kt = col[b]; // Kt = K + wL <x_b, x_p>: subtract the linear part
-                        const float4 kg = make_float4(fmaf(-wL, re, kt.x), fmaf(-wL, im, kt.y), fmaf(wL, im, kt.z), 0.f);
-                        acc_pair(*reinterpret_cast<const float2*>(ag + 2 * b), kg, g0, g1);
+                        const float sn = nb + nws[q];
+                        const float4 kg = make_float4(wG * expf(ew * fmaxf(fmaf(-2.f, re, sn), 0.f)),
+                                                      wG * expf(ew * fmaxf(fmaf(-2.f, im, sn), 0.f)),
+                                                      wG * expf(ew * fmaxf(fmaf(2.f, im, sn), 0.f)), 0.f);
+                        acc_pair(ab, kg, g0, g1);
+                    };
+                    if (staged) {
+                        for (int e = 0; e < nev; ++e)
+                            evict_term(ev_y + e * Np, ev_n[e], make_float2(ev_a[2 * e], ev_a[2 * e + 1]));
+                    } else {
+                        for (int b = pc.loP; b < pn.loP; ++b)
+                            evict_term(Y + size_t(b) * Np, js.nrm[b], *reinterpret_cast<const float2*>(ag + 2 * b));
                     }
                     hw[2 * q] -= g0;
                     hw[2 * q + 1] -= g1;
                 }
+                STEP_MARK(7);
                 __syncthreads();
             }
+            STEP_MARK(3);
             // (2d) entering pairs: predictions start from the reduced partial sums (plus wL <x_n, dr>
             //      after an eviction: their partial sums used r from before it)
             for (int i = kThreads - 1 - tid; i < 2 * min(ne, kMaxEnter) && i >= 0; i += kThreads) {
@@ -461,6 +621,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if (fast) {
                     const int fb = (t + 1) & 1; // frozen partials of the pair entering at t+1
                     for (int w2 = 0; w2 < kWarps; ++w2) s += wpf[(fb * kWarps + w2) * 2 + row];
+                    s += wpr[2 * ((t + 1) & 3) + row];
                     s += wpe[row] + wpe[2 + row];
                 } else {
                     for (int w2 = 0; w2 < kWarps; ++w2) s += wp[(e * kWarps + w2) * 2 + row];
@@ -468,13 +629,14 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if (evict) {
                     float l = 0.f;
                     for (int k = 0; k < N; ++k) {
-                        const float2 v = Yw[qn * Np + k];
+                        const float2 v = Yw[qn * YP + k];
                         l = row == 0 ? fmaf(dr[k], v.x, fmaf(dr[N + k], v.y, l)) : fmaf(dr[k], v.y, fmaf(-dr[N + k], v.x, l));
                     }
                     s = fmaf(wL, l, s);
                 }
                 hw[2 * qn + row] = s;
             }
+            STEP_MARK(4);
             // (2e) pipeline: frozen part of the pair entering at t+2, loads for t+3
             advance(t & 1); // the pair entering at t+2: parity (t + 2) & 1
             issue(t + 3, st_3, st_nn, pc.sP);
@@ -486,8 +648,45 @@ __global__ void __launch_bounds__(kThreads, 2)
             st_3 = st_4;
             __syncthreads();
         }
-        // w = r + sum over the visible pairs of a_b x_b
-        for (int d = tid; d < D; d += kThreads) js.w[d] = r_s[d] + ax_sum(d, pc.loP, pc.hiP);
+        SWEEP_MARK(3);
+        // w = r + sum over the visible pairs of a_b x_b: warp w2 sums pairs lo + w2 + 8 i, lane k
+        // features k and N + k; the warps' sums are added in warp order (the window kernel's
+        // shared memory is free now).  r stays with the detector for its next sweep.
+        {
+            float* part = KA; // [kWarps][kMaxFeatures]
+            for (int k = lane; k < kMaxFeatures / 2; k += 32) {
+                float s0 = 0.f, s1 = 0.f;
+                if (k < N) {
+#pragma unroll 4
+                    for (int b = pc.loP + warp; b < pc.hiP; b += kWarps) {
+                        const float2 ab = *reinterpret_cast<const float2*>(ag + 2 * b);
+                        const float2 v = Y[size_t(b) * Np + k];
+                        s0 = fmaf(ab.x, v.x, fmaf(ab.y, v.y, s0));
+                        s1 = fmaf(ab.x, v.y, fmaf(-ab.y, v.x, s1));
+                    }
+                }
+                part[warp * kMaxFeatures + k] = s0;
+                part[warp * kMaxFeatures + kMaxFeatures / 2 + k] = s1;
+            }
+            __syncthreads();
+            for (int d = tid; d < D; d += kThreads) {
+                const int idx = d < N ? d : kMaxFeatures / 2 + (d - N);
+                float acc = 0.f;
+                for (int w2 = 0; w2 < kWarps; ++w2) acc += part[w2 * kMaxFeatures + idx];
+                js.w[d] = r_s[d] + acc;
+                js.r[d] = r_s[d];
+            }
+        }
+#ifdef APSM_SWEEP_PROFILE
+        __syncthreads();
+        if (blockIdx.x == 0 && tid == 0 && g_sweep_prof_n < 64) {
+            unsigned long long t_;
+            asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t_));
+            g_sweep_prof[g_sweep_prof_n][4] = t_;
+            g_sweep_prof[g_sweep_prof_n][5] = (unsigned long long)n_steps;
+            ++g_sweep_prof_n;
+        }
+#endif
     }
 }
 
@@ -495,8 +694,10 @@ int batch_sweep_threads() { return kThreads; }
 
 size_t batch_sweep_smem(const BatchCommon& cm)
 {
-    const size_t f = 3 * size_t(cm.XSP) * cm.XSPp + 2 * size_t(cm.XSP) * cm.Np + 8 * size_t(cm.XSPp) + cm.XSPp +
-                     size_t(kParts) * 2 * cm.XSPp + 2 * kMaxFeatures + 2 * kMaxEnter * kWarps + 4 * kWarps + 4;
+    const size_t f = 3 * size_t(cm.XSP) * cm.XSPp + 2 * size_t(round_up(uint32_t(cm.XSP * (cm.Np + 1)), 2u)) +
+                     8 * size_t(cm.XSPp) + cm.XSPp +
+                     size_t(kParts) * 2 * cm.XSPp + 2 * kMaxFeatures + 2 * kMaxEnter * kWarps + 4 * kWarps + 4 +
+                     2 * size_t(kMaxEnter) * cm.Np + 2 * kMaxEnter + 8 + cm.XSPp + kMaxEnter;
     return sizeof(float) * f;
 }
 

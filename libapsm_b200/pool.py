@@ -185,6 +185,10 @@ class DetectorPool:
         self._check(self._lib.apsm_pool_last_ms(self._h, int(lane), ctypes.byref(t), ctypes.byref(d)))
         return t.value, d.value
 
+    def set_timing(self, on: bool) -> None:
+        """Per-stage GPU events of each batch (default on; needed by last_ms / last_sweep_ms)."""
+        self._check(self._lib.apsm_pool_set_timing(self._h, 1 if on else 0))
+
     def last_sweep_ms(self, lane: int = 0) -> float:
         """GPU time of the last batch's training sweep kernel."""
         v = ctypes.c_float()
