@@ -748,12 +748,17 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             ins.push_back({j.tx, t.off_tx, sizeof(float2) * t.P});
         }
         for (const auto& q : dp) ins.push_back({jobs[q.job].rx, q.off_rx, sizeof(float2) * size_t(q.det->N) * q.S});
-        direct = !ins.empty();
-        for (const auto& in : ins)
-            if (!is_pinned(in.src)) {
-                direct = false;
-                break;
-            }
+        // small batches travel in the one descriptor upload even from page-locked buffers: a
+        // host memcpy of a few KB costs less than a copy command per input
+        size_t in_bytes = 0;
+        for (const auto& in : ins) in_bytes += in.bytes;
+        direct = !ins.empty() && in_bytes >= (size_t(256) << 10);
+        if (direct)
+            for (const auto& in : ins)
+                if (!is_pinned(in.src)) {
+                    direct = false;
+                    break;
+                }
         if (!direct) {
             std::vector<Stager::Range> pieces;
             pieces.reserve(ins.size());
@@ -860,9 +865,9 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             }
         }
     }
-    // the error flag of kernels with bounded waits (sweep, tensor-core detection) travels back with
-    // the batch: finish() reads it without a synchronous copy
-    L.err_copied = nT > 0 || nG > 0;
+    // the error flag of kernels with bounded waits (tensor-core detection) travels back with the
+    // batch: finish() reads it without a synchronous copy
+    L.err_copied = nG > 0; // only the tensor-core kernels wait on barriers (bounded, flagging expiry)
     if (L.err_copied) POOL_CK(cudaMemcpyAsync(L.err_host, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (trace) {
         POOL_CK(cudaEventRecord(L.tr[6], s));
