@@ -449,6 +449,8 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain and serving measurements")
+    ap.add_argument("--trace-serving", default="",
+                    help="file for the serving pool's batch timeline (APSM_POOL_TRACE; tracing adds latency)")
     ap.add_argument("--detectors", type=int, default=N_DET,
                     help="detectors of the batched workload (the first ones of the same seeded draw; 512 is the "
                          "benchmark, fewer only for profiling captures)")
@@ -474,7 +476,10 @@ def main():
     line = run_batched(args, rank, world)
     if line is not None and not args.no_extras:
         line["plain"] = run_plain()
+        if args.trace_serving:
+            os.environ["APSM_POOL_TRACE"] = args.trace_serving
         line["serving"] = run_serving()
+        os.environ.pop("APSM_POOL_TRACE", None)
     if line is not None and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if world > 1:
