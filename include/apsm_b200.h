@@ -95,6 +95,23 @@ apsm_status apsm_train_history(apsm_detector* h, const float* rx, const float* t
                                const float* tx_val, uint32_t S, uint32_t bits_per_symbol, float modulation_scale,
                                float* history, uint32_t max_steps, uint32_t* n_steps, float* ms);
 
+/*
+ * The effective Gaussian variance of the model (apsm_parameters::
+ * gaussianKernelVariance after the constructor's N^2 scaling,
+ * apsm_noma_detector.cu:79-80, or, for a configured 0, the heuristic's value
+ * once training ran: computeGaussianVarianceHeuristic, :193-218, which the
+ * reference prints).  0 before a heuristic detector's first training call.
+ */
+apsm_status apsm_gaussian_variance(const apsm_detector* h, float* variance);
+
+/*
+ * ApsmNomaDetector::computeNormRatio (apsm_noma_detector.cu:220-311): the
+ * ratio wL |w|^2 / (wG sum_ij a_i a_j k(d_i, d_j)) of the linear to the
+ * Gaussian share of user `user`'s model, over the current dictionary.
+ * APSM detectors only (APSM_ERR_UNSUPPORTED for LLS).  Synchronous.
+ */
+apsm_status apsm_norm_ratio(apsm_detector* h, uint32_t user, float* ratio);
+
 /* Training steps (history rows per user) a train call with P pilots runs on
  * the detector's current state; 0 for LLS detectors.  No reference
  * counterpart (its history vectors grow as they are filled). */

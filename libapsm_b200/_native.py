@@ -44,6 +44,8 @@ SIGNATURES = [
     ("apsm_train_history", ctypes.c_int, [_P, _P, _P, _U32, _P, _P, _U32, _U32, ctypes.c_float, _P, _U32,
                                           ctypes.POINTER(_U32), _F]),
     ("apsm_train_steps", _U32, [_P, _U32]),
+    ("apsm_norm_ratio", ctypes.c_int, [_P, _U32, _F]),
+    ("apsm_gaussian_variance", ctypes.c_int, [_P, _F]),
     ("apsm_detect", ctypes.c_int, [_P, _P, _U32, _P, _F]),
     ("apsm_reset", ctypes.c_int, [_P]),
     ("apsm_train_device", ctypes.c_int, [_P, _P, _P, _U32, _P]),

@@ -150,31 +150,6 @@ std::vector<TrainStep> build_schedule(const Config& c, uint32_t used_before, uin
     return steps;
 }
 
-// computeGaussianVarianceHeuristic (apsm_noma_detector.cu:193-218): host
-// code in the reference too; used only when gaussianKernelVariance == 0.
-float variance_heuristic(const float2* rx, uint32_t N, uint32_t P)
-{
-    std::vector<float> nd;
-    nd.reserve(size_t(P) * (P > 0 ? P - 1 : 0) / 2);
-    for (uint32_t i = 0; i < P; ++i)
-        for (uint32_t j = i + 1; j < P; ++j) {
-            float dist = 0;
-            for (uint32_t k = 0; k < N; ++k) {
-                std::complex<float> a(rx[size_t(k) * P + i].x, rx[size_t(k) * P + i].y);
-                std::complex<float> b(rx[size_t(k) * P + j].x, rx[size_t(k) * P + j].y);
-                dist += std::abs(a - b);
-            }
-            nd.push_back(std::sqrt(dist));
-        }
-    if (nd.empty()) return 0.f;
-    std::sort(nd.begin(), nd.end());
-    const float p = 0.7f;
-    const float q = 5;
-    float variance = nd[size_t(nd.size() * p)] * std::pow(double(P), -1. / q);
-    variance = variance * variance;
-    return variance;
-}
-
 // NomaDetector::shuffleData (noma_detector.cu:59-74): mt19937 seeded with
 // {1,...,8}; rx rows and tx are shuffled with identical copies of the engine,
 // i.e. by one permutation.  Returns perm with shuffled[i] = original[perm[i]].
@@ -316,6 +291,20 @@ extern "C" apsm_status apsm_train_history(apsm_detector* h, const float* rx, con
 }
 
 extern "C" uint32_t apsm_train_steps(const apsm_detector* h, uint32_t P) { return h ? h->train_steps(P) : 0; }
+
+extern "C" apsm_status apsm_gaussian_variance(const apsm_detector* h, float* variance)
+{
+    if (!h || !variance) return APSM_ERR_INVALID_ARGUMENT;
+    *variance = h->gaussian_variance();
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_norm_ratio(apsm_detector* h, uint32_t user, float* ratio)
+{
+    if (!h) return APSM_ERR_INVALID_ARGUMENT;
+    if (!ratio) return fail(h, APSM_ERR_INVALID_ARGUMENT, "norm ratio: null output");
+    return h->norm_ratio(user, ratio);
+}
 
 extern "C" apsm_status apsm_detect(apsm_detector* h, const float* rx, uint32_t S, float* est, float* ms)
 {

@@ -143,17 +143,17 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         APSM_CK(cudaMemcpyAsync(w.p, lls_weights(this), sizeof(float) * size_t(U) * D, cudaMemcpyDeviceToDevice, s));
     }
     if (variance_eff == 0.f) {
-        // the reference computes the heuristic on the host from the pilots
-        std::vector<float2> h_rx(size_t(N) * P);
-        APSM_CK(cudaMemcpyAsync(h_rx.data(), d_rx, sizeof(float2) * h_rx.size(), cudaMemcpyDeviceToHost, s));
-        APSM_CK(cudaStreamSynchronize(s));
-        std::vector<float2> shuffled = h_rx;
-        if (cfg.shuffle) {
-            std::vector<int> pm = shuffle_permutation(P);
-            for (uint32_t a = 0; a < N; ++a)
-                for (uint32_t i = 0; i < P; ++i) shuffled[size_t(a) * P + i] = h_rx[size_t(a) * P + pm[i]];
+        // computeGaussianVarianceHeuristic of the pilots (on the GPU; the multiset of pair
+        // distances, hence the result, does not depend on the training shuffle)
+        const size_t M = size_t(P) * (P - 1) / 2;
+        APSM_CK(vh_nd.ensure(std::max<size_t>(M, 1)));
+        APSM_CK(vh_hist.ensure(256));
+        std::string err;
+        apsm_status st = variance_heuristic_gpu(d_rx, N, P, vh_nd.p, vh_hist.p, s, &variance_eff, &err);
+        if (st != APSM_OK) {
+            last_error = err;
+            return st;
         }
-        variance_eff = variance_heuristic(shuffled.data(), N, P);
         if (!(variance_eff > 0.f)) {
             last_error = "Gaussian variance heuristic produced a non-positive variance";
             return APSM_ERR_INVALID_ARGUMENT;
@@ -542,6 +542,25 @@ apsm_status apsm_detector::train_host(const float2* rx, const float2* tx, uint32
     st = check_train_error();
     if (st != APSM_OK) return st;
     if (ms) *ms = t;
+    return APSM_OK;
+}
+
+apsm_status apsm_detector::norm_ratio(uint32_t user, float* ratio)
+{
+    if (is_lls) {
+        last_error = "the norm ratio belongs to APSM detectors";
+        return APSM_ERR_UNSUPPORTED;
+    }
+    if (user >= U) {
+        last_error = "user " + std::to_string(user) + " of a detector with " + std::to_string(U) + " users";
+        return APSM_ERR_INVALID_ARGUMENT;
+    }
+    APSM_CK(nr_scratch.ensure(size_t(used) + 1));
+    const ModelParams mp = model_params();
+    APSM_CK(launch_norm_ratio(dict_X.p, int(Dp), int(D), int(used), dict_a.p + size_t(user) * cap, w.p + size_t(user) * D,
+                              mp.ew, mp.wL, mp.wG, nr_scratch.p + 1, nr_scratch.p, stream));
+    APSM_CK(cudaMemcpyAsync(ratio, nr_scratch.p, sizeof(float), cudaMemcpyDeviceToHost, stream));
+    APSM_CK(cudaStreamSynchronize(stream));
     return APSM_OK;
 }
 

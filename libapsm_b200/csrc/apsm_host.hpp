@@ -35,7 +35,6 @@ struct Config {
 
 Config parse_config(const std::string& json_text);
 std::vector<TrainStep> build_schedule(const Config& c, uint32_t used_before, uint32_t P, uint32_t cap, int* final_hi);
-float variance_heuristic(const float2* rx, uint32_t N, uint32_t P);
 std::vector<int> shuffle_permutation(uint32_t P);
 
 // Growable device buffer.
@@ -110,6 +109,9 @@ struct apsm_detector {
     // per-step coefficients, evaluation rows / targets, partial sums, output
     apsm::DevBuf<float> h_snap_a, h_snap_w, h_snap_scale, h_a0, h_A, h_E, h_Ey, h_part, h_out;
     apsm::DevBuf<float2> h_rx, h_tx;
+    apsm::DevBuf<float> nr_scratch; // norm ratio: row sums and the result
+    apsm::DevBuf<float> vh_nd;      // variance heuristic: pair distances
+    apsm::DevBuf<unsigned long long> vh_hist;
     apsm::GramWorkspace* gram = nullptr;
     apsm::LlsWorkspace* lls = nullptr; // least-squares detector / llsInitialization
     bool is_lls = false;               // "otype": "LLS"
@@ -129,6 +131,8 @@ struct apsm_detector {
                                    const float2* tx_val, uint32_t S, uint32_t bps, float mod_scale, float* history,
                                    uint32_t max_steps, uint32_t* n_steps, float* ms);
     uint32_t train_steps(uint32_t P) const;
+    apsm_status norm_ratio(uint32_t user, float* ratio);
+    float gaussian_variance() const { return variance_eff; }
     apsm_status detect(const float2* d_rx, uint32_t S, float2* d_est, cudaStream_t s);
     apsm_status train_host(const float2* rx, const float2* tx, uint32_t P, float* ms);
     apsm_status detect_host(const float2* rx, uint32_t S, float2* est, float* ms);

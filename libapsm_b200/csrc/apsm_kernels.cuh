@@ -1,7 +1,10 @@
 // Kernel declarations and launch-argument structs of the B200 APSM library.
 #pragma once
 
+#include "apsm_b200.h"
 #include "apsm_common.cuh"
+
+#include <string>
 
 namespace apsm {
 
@@ -74,6 +77,16 @@ struct HistoryArgs {
 size_t history_eval_smem(int D);
 int history_tiles(int nE);
 cudaError_t launch_history(const HistoryArgs& h, cudaStream_t s);
+
+// ApsmNomaDetector::computeNormRatio (kernels_norm_ratio.cu): out[0] = wL |w|^2 / (wG a^T K a)
+// over the M dictionary rows X (pitch Dp); row_sums: M floats of scratch.
+cudaError_t launch_norm_ratio(const float* X, int Dp, int D, int M, const float* a, const float* w, float ew, float wL,
+                              float wG, float* row_sums, float* out, cudaStream_t s);
+
+// computeGaussianVarianceHeuristic on the GPU (kernels_variance.cu): rx N x P antenna-major
+// on the device; scratch d_nd of P (P - 1) / 2 floats and d_hist of 256 counters.
+apsm_status variance_heuristic_gpu(const float2* d_rx, uint32_t N, uint32_t P, float* d_nd,
+                                   unsigned long long* d_hist, cudaStream_t s, float* variance, std::string* err);
 
 constexpr int kProfSteps = 4096;
 constexpr int kProfMarks = 8;

@@ -175,6 +175,19 @@ class NomaDetector:
     def stream(self) -> int:
         return int(self._lib.apsm_stream(self._h) or 0)
 
+    @property
+    def gaussian_variance(self) -> float:
+        """Effective Gaussian variance (N^2-scaled, or the heuristic's value after training)."""
+        v = ctypes.c_float(0.0)
+        self._check(self._lib.apsm_gaussian_variance(self._h, ctypes.byref(v)))
+        return float(v.value)
+
+    def compute_norm_ratio(self, user: int = 0) -> float:
+        """ApsmNomaDetector::computeNormRatio: wL |w|^2 / (wG a^T K a) of the user's model."""
+        r = ctypes.c_float(0.0)
+        self._check(self._lib.apsm_norm_ratio(self._h, int(user), ctypes.byref(r)))
+        return float(r.value)
+
     # -- model snapshot ---------------------------------------------------
     def rows(self) -> int:
         return int(self._lib.apsm_rows(self._h))

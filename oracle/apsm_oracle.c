@@ -314,6 +314,36 @@ static void adapt_coeffs_f64(apsm_oracle* o)
     }
 }
 
+/* computeNormRatio (apsm_noma_detector.cu:220-311): wL |w|^2 / (wG a^T K a), the
+ * Gaussian sum as kernel_norm_ratio adds it -- row i by LANES lanes, lane l over
+ * j = l, l+LANES, ... ((k a_i) fused with a_j into the lane sum), lanes in order,
+ * rows in order -- and the linear sum in order (fma-contracted). */
+float apsm_oracle_norm_ratio(const apsm_oracle* o)
+{
+    const apsm_oracle_params* p = &o->par;
+    const float ew = -0.5f / p->gaussian_variance;
+    const uint32_t M = o->used, D = o->D;
+    float g = 0.f;
+    for (uint32_t i = 0; i < M; ++i) {
+        const uint32_t ri = phys(o, i);
+        float lane[LANES];
+        memset(lane, 0, sizeof(lane));
+        for (uint32_t j = 0; j < M; ++j) {
+            const uint32_t rj = phys(o, j);
+            const float k = kern_f32(&o->Xf[(size_t)ri * D], &o->Xf[(size_t)rj * D], D, ew);
+            lane[j % LANES] = fmaf(k * o->Af[ri], o->Af[rj], lane[j % LANES]);
+        }
+        float r = 0.f;
+        for (uint32_t l = 0; l < LANES && l < M; ++l) r = r + lane[l];
+        g = g + r;
+    }
+    g = g * p->gaussian_weight;
+    float lin = 0.f;
+    for (uint32_t d = 0; d < D; ++d) lin = fmaf(o->Wf[d], o->Wf[d], lin);
+    lin = lin * p->linear_weight;
+    return lin / g;
+}
+
 /* ---------------------------------------------------------------- FP64 -- */
 
 static double predict_f64(const apsm_oracle* o, const double* x)

@@ -61,6 +61,8 @@ int apsm_oracle_train(apsm_oracle* o, const float* rx, const float* tx, uint32_t
 int apsm_oracle_train_history(apsm_oracle* o, const float* rx, const float* tx, uint32_t P, const float* rx_val,
                               const float* tx_val, uint32_t S, uint32_t bps, float mod_scale, float* history,
                               uint32_t max_steps, uint32_t* n_steps);
+/* computeNormRatio of the current model (F32 oracles). */
+float apsm_oracle_norm_ratio(const apsm_oracle* o);
 /* est: S complex (re,im). */
 int apsm_oracle_detect(apsm_oracle* o, const float* rx, uint32_t S, float* est);
 

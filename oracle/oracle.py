@@ -93,6 +93,8 @@ def _load_oracle() -> ctypes.CDLL:
         lib.apsm_oracle_train_history.argtypes = [P, P, P, ctypes.c_uint32, P, P, ctypes.c_uint32, ctypes.c_uint32,
                                                   ctypes.c_float, P, ctypes.c_uint32, P]
         lib.apsm_oracle_train_history.restype = ctypes.c_int
+        lib.apsm_oracle_norm_ratio.argtypes = [P]
+        lib.apsm_oracle_norm_ratio.restype = ctypes.c_float
         lib.apsm_oracle_detect.argtypes = [P, P, ctypes.c_uint32, P]
         lib.apsm_oracle_detect.restype = ctypes.c_int
         lib.apsm_oracle_rows.argtypes = [P]
@@ -230,6 +232,10 @@ class OracleDetector:
     def rows(self) -> int:
         return int(self._lib.apsm_oracle_rows(self._h))
 
+    def norm_ratio(self) -> float:
+        """computeNormRatio (apsm_noma_detector.cu:220-311) of the current model."""
+        return float(self._lib.apsm_oracle_norm_ratio(self._h))
+
     def get_state(self) -> dict[str, np.ndarray]:
         r = self.rows()
         D = 2 * self.N
@@ -269,6 +275,8 @@ def _load_ref() -> ctypes.CDLL:
                                           ctypes.c_uint32, ctypes.c_float, P, ctypes.c_uint32, P,
                                           ctypes.POINTER(ctypes.c_float)]
         lib.ref_train_history.restype = ctypes.c_int
+        lib.ref_norm_ratio.argtypes = [P, ctypes.POINTER(ctypes.c_float)]
+        lib.ref_norm_ratio.restype = ctypes.c_int
         lib.ref_reset.argtypes = [P]
         lib.ref_destroy.argtypes = [P]
         lib.ref_run_users_threaded.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, P, P,
@@ -330,6 +338,13 @@ class ReferenceDetector:
         if self._lib.ref_detect(self._h, rx.ctypes.data, self.N, S, est.ctypes.data, ctypes.byref(ms)):
             raise RuntimeError("reference detect failed")
         return est, ms.value
+
+    def norm_ratio(self) -> float:
+        """ApsmNomaDetector::computeNormRatio of the reference detector."""
+        v = ctypes.c_float()
+        if self._lib.ref_norm_ratio(self._h, ctypes.byref(v)):
+            raise RuntimeError("reference norm ratio failed")
+        return v.value
 
     def reset_state(self):
         self._lib.ref_reset(self._h)

@@ -26,6 +26,8 @@
 
 #include "noma/noma_detector_factory.cuh"
 #include "noma/noma_train_history.cuh"
+#include "apsm/apsm_versions.cuh"
+#include "apsm/apsm_noma_detector.cuh"
 
 namespace {
 
@@ -116,6 +118,19 @@ int ref_train_history(ref_handle* h, const float* rx, const float* tx, uint32_t 
         std::memcpy(out + 6 * i, row, sizeof(row));
     }
     return n > max_steps ? 3 : 0;
+}
+
+// ApsmNomaDetector::computeNormRatio (apsm_noma_detector.cuh:92), whichever detect version
+// the factory built.
+int ref_norm_ratio(ref_handle* h, float* out)
+{
+    NomaDetector* d = h->det.get();
+    if (auto* x = dynamic_cast<ApsmNomaDetector<apsm_versions::APSM_DETECT_BALANCED>*>(d)) *out = x->computeNormRatio();
+    else if (auto* x = dynamic_cast<ApsmNomaDetector<apsm_versions::APSM_DETECT_ORIGINAL>*>(d)) *out = x->computeNormRatio();
+    else if (auto* x = dynamic_cast<ApsmNomaDetector<apsm_versions::APSM_DETECT_OLDFAST>*>(d)) *out = x->computeNormRatio();
+    else if (auto* x = dynamic_cast<ApsmNomaDetector<apsm_versions::APSM_DETECT_SHMEM>*>(d)) *out = x->computeNormRatio();
+    else return 1;
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
 }
 
 void ref_reset(ref_handle* h) { h->det->resetState(); }

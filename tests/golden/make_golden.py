@@ -14,6 +14,9 @@ train -> detect) on a B200.
   python tests/golden/make_golden.py run --out DIR
       (on a GPU box) runs the reference library on every case and writes
       DIR/golden_<case>.npz: inputs, config and the reference's estimates.
+  python tests/golden/make_golden.py normratio --out DIR
+      (on a GPU box) trains the reference on every golden_<case>.npz and
+      writes DIR/golden_norm_ratio.npz: its computeNormRatio per case.
   python tests/golden/make_golden.py history --out DIR
       (on a GPU box) trains the reference with a validation set and writes
       DIR/golden_history_<case>.npz: inputs, config, the per-step history.
@@ -187,9 +190,27 @@ def history(out: Path, only: set[str] | None = None) -> None:
         print(f"history {name}: {hist.shape[0]} steps, ref train {tms:.3f} ms, last {hist[-1]}")
 
 
+def norm_ratio(out: Path) -> None:
+    """computeNormRatio of the reference after training on each golden_<case>.npz."""
+    from oracle import oracle as O
+
+    vals = {}
+    for f in sorted(HERE.glob("golden_*.npz")):
+        name = f.stem[len("golden_"):]
+        if name.startswith(("lls", "history", "norm_ratio")):
+            continue
+        d = np.load(f)
+        cfg = json.loads(str(d["config"]))
+        r = O.ReferenceDetector(cfg, d["rx_train"].shape[0])
+        r.train(d["rx_train"], d["tx_train"])
+        vals[name] = np.float32(r.norm_ratio())
+        print(f"norm ratio {name}: {vals[name]}")
+    np.savez(out / "golden_norm_ratio.npz", **vals)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("mode", choices=["capture", "run", "history"])
+    ap.add_argument("mode", choices=["capture", "run", "history", "normratio"])
     ap.add_argument("--out", default=str(HERE))
     ap.add_argument("--cases", default="", help="comma-separated case names (default: all)")
     a = ap.parse_args()
@@ -198,5 +219,7 @@ if __name__ == "__main__":
         capture()
     elif a.mode == "run":
         run(Path(a.out), only)
+    elif a.mode == "normratio":
+        norm_ratio(Path(a.out))
     else:
         history(Path(a.out), only)
