@@ -288,6 +288,101 @@ def run_plain(steps: int = 5, warmup: int = 3) -> dict:
                         "(exact FP32 sweep + BALANCED-order detect)"}
 
 
+# ------------------------------------------------- large-detect precision --
+PRECISION_FORMS = ("balanced", "gram_tf32", "gram_bf16x3", "gram_bf16")
+
+
+def model_fp64(state: dict, variance: float, wL: float, wG: float, rx: np.ndarray) -> np.ndarray:
+    """Soft outputs of a trained model (float32 state) evaluated in float64:
+    est_u(s) = f_u(x_2s) + i f_u(x_2s+1) with the Dedup rows x_2s = [Re; Im],
+    x_2s+1 = [Im; -Re] and f_u(x) = wL <w_u, x> + wG sum_b a_ub exp(-||d_b - x||^2 / (2 variance))."""
+    d = state["dictionary"].astype(np.float64)
+    a = state["a"].astype(np.float64)
+    w = state["w"].astype(np.float64)
+    re, im = rx.real.astype(np.float64).T, rx.imag.astype(np.float64).T
+    out = np.empty((a.shape[0], rx.shape[1]), dtype=np.complex128)
+    dn = (d * d).sum(1)
+    for part, x in enumerate((np.hstack([re, im]), np.hstack([im, -re]))):
+        for s0 in range(0, x.shape[0], 512):
+            xs = x[s0:s0 + 512]
+            dist = np.maximum((xs * xs).sum(1)[:, None] + dn[None, :] - 2.0 * xs @ d.T, 0.0)
+            f = wL * xs @ w.T + wG * np.exp(-0.5 / variance * dist) @ a.T  # (rows, users)
+            if part == 0:
+                out[:, s0:s0 + 512] = f.T
+            else:
+                out[:, s0:s0 + 512] += 1j * f.T
+    return out
+
+
+def run_precision_study(reps: int = 3, sample: int = 2048) -> dict:
+    """Large detection in every precision: N=64 antennas (128 real features),
+    16 16QAM users at 15 dB behind a Rapp PA (p=3), a dictionary of 8192
+    entries filled by 8192 pilots (exact FP32 sweep, all users in one
+    launch), 65536 data symbols detected by one trained model in each form
+    (the model copied into one detector per form).  Soft outputs and
+    decisions against a float64 evaluation of the same model on the first
+    `sample` symbols; symbol error rates on all symbols."""
+    import torch
+
+    import libapsm_b200 as L
+    from libapsm_b200 import synth
+
+    K, N, P, S = 16, 64, 8192, 65536
+    f = synth.generate_frame(3, K=K, N=N, P=P, S=S, modulation="QAM16", snr_db=15.0, rapp_p=3.0)
+    cfg = dict(synth.CONFIG0_ALGORITHM, dictionarySize=8192)
+    dets = {m: L.NomaDetectorFactory.build(dict(cfg, detectVersion=m), N, num_users=K) for m in PRECISION_FORMS}
+    base = dets["balanced"]
+    rx, tx, rxd = (torch.from_numpy(a).cuda() for a in (f.rx_train, f.tx_train, f.rx_data))
+    stream = torch.cuda.ExternalStream(base.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    base.train_device(rx, tx)
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    base.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    state = base.get_state()
+    ref = model_fp64(state, base.gaussian_variance, 0.5, 0.5, f.rx_data[:, :sample])
+    mod = f.modulation
+    ref_dec = mod.hard_decode_int(ref)
+    true_dec = mod.hard_decode_int(f.tx_data)
+    forms = {}
+    for m, det in dets.items():
+        if det is not base:
+            det.copy_state_from(base)
+        est = torch.empty((K, S), dtype=torch.complex64, device="cuda")
+        st = torch.cuda.ExternalStream(det.stream)
+        det.detect_device(rxd, est)  # warm-up (workspace allocation)
+        det.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for a, b in ev:
+            with torch.cuda.stream(st):
+                a.record(st)
+            det.detect_device(rxd, est)
+            with torch.cuda.stream(st):
+                b.record(st)
+        det.synchronize()
+        ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+        e = est.cpu().numpy()
+        es = e[:, :sample].astype(np.complex128)
+        err = np.abs(es - ref)
+        forms[m] = {
+            "detect_ms": round(ms, 3),
+            "symbols_per_s": K * S / (ms * 1e-3),
+            "soft_max_err_rel": float(err.max() / np.abs(ref).max()),
+            "soft_rms_err_rel": float(np.sqrt(np.mean(err ** 2) / np.mean(np.abs(ref) ** 2))),
+            "decisions_differing_from_fp64": float(np.mean(mod.hard_decode_int(es) != ref_dec)),
+            "ser": float(np.mean(mod.hard_decode_int(e) != true_dec)),
+        }
+    for det in dets.values():
+        det.close()
+    return {"workload": f"16QAM K={K} users N={N} P={P} S={S} 15 dB Rapp p=3, window 80, dictionary 8192, "
+                        "variance 0.5 N^2, one model detected in each form",
+            "train_ms": round(train_ms, 3), "fp64_sample_symbols": sample,
+            "ser_fp64_model": float(np.mean(ref_dec != true_dec[:, :sample])), "forms": forms}
+
+
 # ------------------------------------------------------------ serving form --
 def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = N_DET, lanes: int = 8,
                 max_batch: int = 16) -> dict:
@@ -454,7 +549,12 @@ def main():
     ap.add_argument("--detectors", type=int, default=N_DET,
                     help="detectors of the batched workload (the first ones of the same seeded draw; 512 is the "
                          "benchmark, fewer only for profiling captures)")
+    ap.add_argument("--precision-only", action="store_true",
+                    help="run only the large-detect precision study (N=64, dictionary 8192) and print it")
     args = ap.parse_args()
+    if args.precision_only:
+        print(json.dumps({"precision": run_precision_study()}), flush=True)
+        return
     if args.warmup < 3:
         args.warmup = 3
 
@@ -480,6 +580,7 @@ def main():
             os.environ["APSM_POOL_TRACE"] = args.trace_serving
         line["serving"] = run_serving()
         os.environ.pop("APSM_POOL_TRACE", None)
+        line["precision"] = run_precision_study()
     if line is not None and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     if world > 1:

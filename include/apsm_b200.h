@@ -165,6 +165,19 @@ uint32_t apsm_rows(const apsm_detector* h);
 apsm_status apsm_get_state(apsm_detector* h, float* dict, float* a, float* w);
 
 /*
+ * Copies the whole trained state of src (dictionary rows, their targets and
+ * coefficients, linear weights, the kernel variance a heuristic chose) into
+ * dst, on the device.  Both are APSM detectors on one device with the same
+ * antennas, users, dictionarySize and kernel weights; dst's configured
+ * gaussianKernelVariance must be 0 (heuristic) or equal src's.  dst's
+ * detection form (detectVersion) is its own, so one trained model can be
+ * evaluated in several precisions.  Waits for src's stream; the copies are
+ * ordered on dst's stream.  No reference counterpart (the reference's detector
+ * state is private, apsm_noma_detector.cuh:93 only reads it).
+ */
+apsm_status apsm_copy_state(apsm_detector* dst, const apsm_detector* src);
+
+/*
  * GPU time (CUDA events, ms) of the last training sweep kernel and of the last
  * detection kernel of this handle; -1 when that stage has not run.  Blocks
  * until those kernels finished.  Replaces nothing in the reference (its

@@ -55,6 +55,7 @@ SIGNATURES = [
     ("apsm_synchronize", ctypes.c_int, [_P]),
     ("apsm_rows", _U32, [_P]),
     ("apsm_get_state", ctypes.c_int, [_P, _P, _P, _P]),
+    ("apsm_copy_state", ctypes.c_int, [_P, _P]),
     ("apsm_last_kernel_ms", ctypes.c_int, [_P, _F, _F]),
     ("apsm_last_error", ctypes.c_char_p, [_P]),
     # detector pool (batched many-detector form)

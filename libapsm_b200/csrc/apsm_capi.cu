@@ -323,6 +323,13 @@ extern "C" apsm_status apsm_get_state(apsm_detector* h, float* dict, float* a, f
     return h->get_state(dict, a, w);
 }
 
+extern "C" apsm_status apsm_copy_state(apsm_detector* dst, const apsm_detector* src)
+{
+    if (!dst || !src) return APSM_ERR_INVALID_ARGUMENT;
+    if (dst == src) return APSM_OK;
+    return dst->copy_state_from(*src);
+}
+
 extern "C" apsm_status apsm_last_kernel_ms(apsm_detector* h, float* sweep_ms, float* detect_ms)
 {
     if (!h) return APSM_ERR_INVALID_ARGUMENT;

@@ -99,6 +99,7 @@ apsm_status apsm_detector::init(const Config& c, uint32_t num_antennas, uint32_t
     APSM_CK(train_err.ensure(1));
     APSM_CK(cudaMemset(train_err.p, 0, sizeof(int)));
     cluster = env_int("APSM_TRAIN_CLUSTER", 16);
+    force_glob_a = env_int("APSM_TRAIN_GLOBAL_RING", 0) != 0;
     return reset();
 }
 
@@ -289,6 +290,7 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         ta.snap_a = hist_nE > 0 ? h_snap_a.p : nullptr;
         ta.snap_w = hist_nE > 0 ? h_snap_w.p : nullptr;
         ta.norm_c = cfg.norm_constraint;
+        ta.a_glob = nullptr;
         ta.snap_scale = hist_nE > 0 && cfg.norm_constraint > 0.f ? h_snap_scale.p : nullptr;
 
         ta.XP = int(Dp) + 4; // padded window-row pitch (conflict-free column reads)
@@ -343,6 +345,7 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
                     stage_valid[0] = true;
                     last_train_cluster = bestC;
                     last_train_staged = false;
+                    last_train_glob_a = false;
                     goto sweep_done;
                 }
             }
@@ -351,48 +354,53 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
 
         // launch shape: the largest cluster (<= 16 CTAs) that holds its kernel
         // columns in shared memory and of which every user gets one at once
-        auto shape = [&](int C, bool staged, int* nwarps_out, int* ns_out) -> size_t {
+        // glob_a: the coefficient ring lives in global memory (one private copy per CTA)
+        auto shape = [&](int C, bool staged, bool glob_a, int* nwarps_out, int* ns_out) -> size_t {
             int nwarps = std::max({(int(q2) + C - 1) / C, (int(D) * kWGroups + 31) / 32, 4});
             int ns = staged ? ta.XW / C + 2 : 0;
             *nwarps_out = nwarps;
             *ns_out = ns;
-            return sizeof(float) * (size_t(ta.XW) * ta.XP + size_t(ns) * Lk + size_t(ta.A_ring) + kMaxFeatures +
-                                    2 * q2 + size_t(nwarps) * 32 + 2 * size_t(ta.XW) + 64) +
+            return sizeof(float) * (size_t(ta.XW) * ta.XP + size_t(ns) * Lk + (glob_a ? 0 : size_t(ta.A_ring)) +
+                                    kMaxFeatures + 2 * q2 + size_t(nwarps) * 32 + 2 * size_t(ta.XW) + 64) +
                    48;
         };
         const size_t smem_limit = 227 * 1024;
         struct Choice {
             int C = 0, nwarps = 0, ns = 0, clusters = 0;
-            bool staged = false;
+            bool staged = false, glob_a = false;
             size_t smem = 0;
         } best;
         const int cmax = cluster > 0 ? std::min(16, cluster) : 16;
-        for (int C = cmax; C >= 1; C /= 2) {
-            for (int st = 1; st >= 0; --st) {
-                int nw = 0, ns = 0;
-                size_t sm = shape(C, st == 1, &nw, &ns);
-                if (sm > smem_limit || nw > 32) continue;
-                int mc = 0;
-                if (query_train_clusters(st == 1, C, nw * 32, sm, int(U), &mc) != cudaSuccess) {
-                    cudaGetLastError();
-                    continue;
+        // shared-memory coefficient ring first; a global one only when no shape holds it
+        for (int ga = force_glob_a ? 1 : 0; ga < 2 && best.C == 0; ++ga) {
+            for (int C = cmax; C >= 1; C /= 2) {
+                for (int st = 1; st >= 0; --st) {
+                    int nw = 0, ns = 0;
+                    size_t sm = shape(C, st == 1, ga == 1, &nw, &ns);
+                    if (sm > smem_limit || nw > 32) continue;
+                    int mc = 0;
+                    if (query_train_clusters(st == 1, ga == 1, C, nw * 32, sm, int(U), &mc) != cudaSuccess) {
+                        cudaGetLastError();
+                        continue;
+                    }
+                    if (mc < 1) continue;
+                    // prefer: all users concurrent, then staged columns, then larger clusters
+                    auto score = [&](int clusters, bool staged, int c) {
+                        return (clusters >= int(U) ? 4 : 0) + (staged ? 2 : 0) + (c >= 8 ? 1 : 0);
+                    };
+                    if (best.C == 0 || score(mc, st == 1, C) > score(best.clusters, best.staged, best.C)) {
+                        best.C = C;
+                        best.nwarps = nw;
+                        best.ns = ns;
+                        best.clusters = mc;
+                        best.staged = st == 1;
+                        best.glob_a = ga == 1;
+                        best.smem = sm;
+                    }
+                    break; // staged preferred at this cluster size
                 }
-                if (mc < 1) continue;
-                // prefer: all users concurrent, then staged columns, then larger clusters
-                auto score = [&](int clusters, bool staged, int c) {
-                    return (clusters >= int(U) ? 4 : 0) + (staged ? 2 : 0) + (c >= 8 ? 1 : 0);
-                };
-                if (best.C == 0 || score(mc, st == 1, C) > score(best.clusters, best.staged, best.C)) {
-                    best.C = C;
-                    best.nwarps = nw;
-                    best.ns = ns;
-                    best.clusters = mc;
-                    best.staged = st == 1;
-                    best.smem = sm;
-                }
-                break; // staged preferred at this cluster size
+                if (best.C != 0 && best.clusters >= int(U) && best.staged) break;
             }
-            if (best.C != 0 && best.clusters >= int(U) && best.staged) break;
         }
         if (best.C == 0) {
             last_error = "training kernel does not fit one cluster (window " + std::to_string(q2) +
@@ -402,6 +410,10 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         ta.NS = best.ns;
         ta.users = int(U);
         ta.prof = prof_buffer;
+        if (best.glob_a) {
+            APSM_CK(a_rings.ensure(size_t(U) * best.C * ta.A_ring));
+            ta.a_glob = a_rings.p;
+        }
         int max_clusters = 0;
         APSM_CK(cudaMemsetAsync(train_err.p, 0, sizeof(int), s));
         APSM_CK(cudaEventRecord(stage_ev[0], s));
@@ -414,6 +426,7 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         }
         last_train_cluster = best.C;
         last_train_staged = best.staged;
+        last_train_glob_a = best.glob_a;
     }
 sweep_done:
     if (hist_nE > 0) {
@@ -637,6 +650,36 @@ apsm_status apsm_detector::get_state(float* dict, float* a_out, float* w_out)
         APSM_CK(cudaMemcpy2D(a_out, sizeof(float) * used, dict_a.p, sizeof(float) * cap, sizeof(float) * used, U,
                              cudaMemcpyDeviceToHost));
     if (w_out) APSM_CK(cudaMemcpy(w_out, w.p, sizeof(float) * size_t(U) * D, cudaMemcpyDeviceToHost));
+    return APSM_OK;
+}
+
+apsm_status apsm_detector::copy_state_from(const apsm_detector& src)
+{
+    if (is_lls || src.is_lls) {
+        last_error = "state copies need two APSM detectors";
+        return APSM_ERR_UNSUPPORTED;
+    }
+    if (src.device != device || src.N != N || src.U != U || src.cap != cap) {
+        last_error = "state copy between detectors of different device, antennas, users or dictionarySize";
+        return APSM_ERR_INVALID_ARGUMENT;
+    }
+    if (src.cfg.wL != cfg.wL || src.cfg.wG != cfg.wG) {
+        last_error = "state copy between detectors of different kernel weights";
+        return APSM_ERR_INVALID_ARGUMENT;
+    }
+    if (cfg.variance != 0.f && src.variance_eff != variance_eff) {
+        last_error = "state copy between detectors of different gaussianKernelVariance";
+        return APSM_ERR_INVALID_ARGUMENT;
+    }
+    APSM_CK(cudaStreamSynchronize(src.stream));
+    const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+    APSM_CK(cudaMemcpyAsync(dict_X.p, src.dict_X.p, sizeof(float) * size_t(cap) * Dp, k, stream));
+    APSM_CK(cudaMemcpyAsync(dict_nrm.p, src.dict_nrm.p, sizeof(float) * cap, k, stream));
+    APSM_CK(cudaMemcpyAsync(dict_y.p, src.dict_y.p, sizeof(float) * size_t(U) * cap, k, stream));
+    APSM_CK(cudaMemcpyAsync(dict_a.p, src.dict_a.p, sizeof(float) * size_t(U) * cap, k, stream));
+    APSM_CK(cudaMemcpyAsync(w.p, src.w.p, sizeof(float) * size_t(U) * D, k, stream));
+    used = src.used;
+    if (src.variance_eff != 0.f) variance_eff = src.variance_eff;
     return APSM_OK;
 }
 

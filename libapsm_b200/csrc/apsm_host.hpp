@@ -101,6 +101,7 @@ struct apsm_detector {
 
     // per-call scratch
     apsm::DevBuf<float> uX, unrm, uy, ua, K, xs;
+    apsm::DevBuf<float> a_rings; // exact sweep: per-CTA coefficient rings of large dictionaries
     apsm::DevBuf<apsm::TrainStep> steps;
     apsm::DevBuf<int> train_err; // set by the sweep when a bounded wait expired
     apsm::DevBuf<int> perm;
@@ -120,6 +121,8 @@ struct apsm_detector {
     int cluster = 0;
     int last_train_cluster = 0;
     bool last_train_staged = false;
+    bool last_train_glob_a = false; // the last exact sweep kept its coefficient rings in global memory
+    bool force_glob_a = false;      // APSM_TRAIN_GLOBAL_RING=1: global rings for every exact sweep
     unsigned long long* prof_buffer = nullptr; // device timestamps of profiling builds
 
     ~apsm_detector();
@@ -137,6 +140,7 @@ struct apsm_detector {
     apsm_status train_host(const float2* rx, const float2* tx, uint32_t P, float* ms);
     apsm_status detect_host(const float2* rx, uint32_t S, float2* est, float* ms);
     apsm_status get_state(float* dict, float* a, float* w_out);
+    apsm_status copy_state_from(const apsm_detector& src);
     apsm_status stage_ms(float* sweep_ms, float* detect_ms);
     apsm_status check_train_error();
     apsm::ModelParams model_params() const;

@@ -46,6 +46,7 @@ struct TrainArgs {
     float* snap_w;            // users x n_steps x D: the linear weights after each step
     float* snap_scale;        // users x n_steps: the normConstraint factor of each step (1: none)
     float norm_c;             // normConstraint: bound of ||f_G|| after every step (0: off; exact sweep only)
+    float* a_glob;            // exact sweep: per-CTA coefficient rings in global memory (nullptr: shared memory)
 };
 
 // Training history (kernels_history.cu): every step's model evaluated on the
@@ -106,7 +107,8 @@ __global__ void gram_columns_kernel(const float* __restrict__ X, int Dp, int D, 
 cudaError_t launch_train_exact(bool staged, int cluster, int threads, size_t smem, cudaStream_t stream,
                                const TrainArgs& args, int* max_clusters);
 // Clusters of this shape that fit the device at once.
-cudaError_t query_train_clusters(bool staged, int cluster, int threads, size_t smem, int users, int* max_clusters);
+cudaError_t query_train_clusters(bool staged, bool glob_a, int cluster, int threads, size_t smem, int users,
+                                 int* max_clusters);
 
 // Incremental sweep (kernels_sweep_inc.cu): one cluster of `cluster` CTAs per user.
 int incremental_threads();

@@ -127,7 +127,11 @@ __device__ __forceinline__ void st_async_f32(const float* local, const uint64_t*
 //   yw, nw [XW]       targets and squared norms of the window rows
 //   nbuf   [2][16]    normConstraint: the CTAs' partial sums of ||f_G||^2 (st.async)
 //   npart  [32]       normConstraint: warp partials
-template <bool kStaged>
+// kGlobA: dictionaries whose coefficient ring does not fit shared memory keep it
+// in global memory instead, one private copy per CTA (args.a_glob, A_ring floats
+// per CTA): every CTA still applies every correction to its own copy, so no
+// copy is read by another CTA.
+template <bool kStaged, bool kGlobA>
 __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
 {
     cg::cluster_group cluster = cg::this_cluster();
@@ -141,8 +145,9 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
     extern __shared__ __align__(16) float smem[];
     float* xw = smem;
     float* kcol = xw + size_t(args.XW) * XP;
-    float* a_ring = kcol + (kStaged ? size_t(args.NS) * args.Lc : 0);
-    float* w_s = a_ring + args.A_ring;
+    float* a_smem = kcol + (kStaged ? size_t(args.NS) * args.Lc : 0);
+    float* a_ring = kGlobA ? args.a_glob + size_t(blockIdx.x) * args.A_ring : a_smem;
+    float* w_s = a_smem + (kGlobA ? 0 : args.A_ring);
     float* cbuf = w_s + kMaxFeatures;
     float* red = cbuf + 2 * q2;
     float* yw = red + nwarps * 32;
@@ -404,10 +409,19 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
     }
 }
 
+namespace {
+using SweepKernel = void (*)(TrainArgs);
+SweepKernel sweep_kernel(bool staged, bool glob_a)
+{
+    if (glob_a) return staged ? train_sweep_kernel<true, true> : train_sweep_kernel<false, true>;
+    return staged ? train_sweep_kernel<true, false> : train_sweep_kernel<false, false>;
+}
+} // namespace
+
 cudaError_t launch_train_exact(bool staged, int cluster, int threads, size_t smem, cudaStream_t stream,
                                const TrainArgs& args, int* max_clusters)
 {
-    auto kern = staged ? train_sweep_kernel<true> : train_sweep_kernel<false>;
+    auto kern = sweep_kernel(staged, args.a_glob != nullptr);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     if (cluster > 8) {
@@ -432,9 +446,10 @@ cudaError_t launch_train_exact(bool staged, int cluster, int threads, size_t sme
     return cudaLaunchKernelEx(&lc, kern, args);
 }
 
-cudaError_t query_train_clusters(bool staged, int cluster, int threads, size_t smem, int users, int* max_clusters)
+cudaError_t query_train_clusters(bool staged, bool glob_a, int cluster, int threads, size_t smem, int users,
+                                 int* max_clusters)
 {
-    auto kern = staged ? train_sweep_kernel<true> : train_sweep_kernel<false>;
+    auto kern = sweep_kernel(staged, glob_a);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     if (cluster > 8) {

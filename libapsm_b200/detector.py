@@ -203,6 +203,11 @@ class NomaDetector:
                                              a.ctypes.data if rows else None, w.ctypes.data))
         return {"dictionary": dic, "a": a, "w": w}
 
+    def copy_state_from(self, other: "NomaDetector") -> None:
+        """Take over the trained state of another detector of the same sizes
+        (apsm_copy_state): one model, evaluated in this detector's detection form."""
+        self._check(self._lib.apsm_copy_state(self._h, other._h))
+
 
 class NomaDetectorFactory:
     """NomaDetectorFactory::build (cpp/lib/noma/noma_detector_factory.cu:57-65)."""

@@ -275,3 +275,56 @@ def test_incremental_sweep_config1_all_users(oracle_mod):
         _, eo = run_oracle(oracle_mod, cfg, f, u=u)
         assert_soft_close(est[u], eo)
         assert_hard_equal(est[u], eo, f.modulation)
+
+
+# ------------------------------------------- coefficient rings in global memory --
+# Dictionaries whose coefficient ring does not fit the exact sweep's shared
+# memory (N = 64 with dictionarySize 8192: a 32768-entry ring beside 256 window
+# rows of 132 floats) keep one private ring per CTA in global memory.  The
+# summation order is unchanged, so the FP32 bar is the exact sweep's own.
+# APSM_TRAIN_GLOBAL_RING=1 selects that form for any size, so the eviction,
+# multi-pass and normConstraint paths are covered at sizes the oracle finishes.
+
+GLOBAL_RING_CASES = [c for c in CASES if c[0] in ("wrap", "passes2", "sfw", "window>P", "N64", "norm-wrap",
+                                                   "norm-passes2", "config0")]
+
+
+@pytest.mark.parametrize("name,cfg,frame", GLOBAL_RING_CASES, ids=[c[0] for c in GLOBAL_RING_CASES])
+def test_global_coefficient_ring_matches_oracle(oracle_mod, monkeypatch, name, cfg, frame):
+    monkeypatch.setenv("APSM_TRAIN_GLOBAL_RING", "1")
+    seed, K, N, P, S, mod = frame
+    f = synth.generate_frame(seed, K=K, N=N, P=P, S=S, modulation=mod, snr_db=20)
+    det, est = run_product(cfg, f)
+    o, eo = run_oracle(oracle_mod, cfg, f)
+    assert det.rows() == o.rows()
+    assert_soft_close(est, eo, rtol=1e-5)
+    assert_hard_equal(est, eo, f.modulation)
+    assert_soft_close(det.get_state()["a"][0], o.get_state()["a"], rtol=1e-5)
+
+
+def test_global_coefficient_ring_users_and_append(oracle_mod, monkeypatch):
+    monkeypatch.setenv("APSM_TRAIN_GLOBAL_RING", "1")
+    f = synth.generate_frame(20, K=3, N=6, P=150, S=100, modulation="QAM16")
+    g = synth.generate_frame(21, K=3, N=6, P=70, S=10, modulation="QAM16")
+    cfg = dict(BASE, dictionarySize=100)
+    det = L.NomaDetectorFactory.build(cfg, 6, num_users=3)
+    det.train(f.rx_train, f.tx_train)
+    det.train(g.rx_train, g.tx_train)
+    est, _ = det.detect(f.rx_data)
+    for u in range(3):
+        o = oracle_mod.OracleDetector(cfg, 6, oracle_mod.F32)
+        o.train(f.rx_train, f.tx_train[u])
+        o.train(g.rx_train, g.tx_train[u])
+        assert_soft_close(est[u], o.detect(f.rx_data), rtol=1e-5)
+
+
+def test_large_dictionary_n64_matches_oracle(oracle_mod):
+    # precision-study sizes (N = 64, dictionarySize 8192) with a short pilot
+    # sequence: the shape search itself falls back to global rings here
+    cfg = dict(BASE, windowSize=80, dictionarySize=8192)
+    f = synth.generate_frame(31, K=4, N=64, P=240, S=200, modulation="QAM16", snr_db=15)
+    det, est = run_product(cfg, f, users=4)
+    for u in (0, 3):
+        _, eo = run_oracle(oracle_mod, cfg, f, u=u)
+        assert_soft_close(est[u], eo, rtol=1e-5)
+        assert_hard_equal(est[u], eo, f.modulation)
