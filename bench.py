@@ -19,6 +19,10 @@ detection in TF32 hi/lo form, FP32-accurate).  Seeded synthetic frames
   serving  Poisson per-TTI requests (train-append 16-64 pilots / detect
            500-4000 symbols) against 512 resident detectors through the
            request server: p50 / p99 latency and detected symbols/s
+  precision  large detection (N=64, dictionary 8192, 16 users, 65536
+           symbols) in the exact form and every tensor-core form: time,
+           symbols/s, soft-output and decision error against a float64
+           evaluation of the same trained model, SER
 
 ``--impl reference`` times the reference algorithm on the host cores (the
 reference has no CPU implementation of APSM: this is the repository's FP32 C
@@ -289,7 +293,7 @@ def run_plain(steps: int = 5, warmup: int = 3) -> dict:
 
 
 # ------------------------------------------------- large-detect precision --
-PRECISION_FORMS = ("balanced", "gram_tf32", "gram_bf16x3", "gram_bf16")
+PRECISION_FORMS = ("balanced", "gram_tf32x3", "gram_tf32", "gram_bf16x3", "gram_bf16")
 
 
 def model_fp64(state: dict, variance: float, wL: float, wG: float, rx: np.ndarray) -> np.ndarray:
@@ -319,9 +323,12 @@ def run_precision_study(reps: int = 3, sample: int = 2048) -> dict:
     16 16QAM users at 15 dB behind a Rapp PA (p=3), a dictionary of 8192
     entries filled by 8192 pilots (exact FP32 sweep, all users in one
     launch), 65536 data symbols detected by one trained model in each form
-    (the model copied into one detector per form).  Soft outputs and
-    decisions against a float64 evaluation of the same model on the first
-    `sample` symbols; symbol error rates on all symbols."""
+    (the model copied into one detector per form).  Two kernel widths: the
+    config-0 width (gaussianKernelVariance 0.5, scaled by N^2: a wide kernel,
+    the linear part dominates) and the reference's default 0.05 (exponents of
+    a few units: the Gaussian part carries the model).  Soft outputs and decisions
+    against a float64 evaluation of the same model on the first `sample`
+    symbols; symbol error rates on all symbols."""
     import torch
 
     import libapsm_b200 as L
@@ -329,58 +336,61 @@ def run_precision_study(reps: int = 3, sample: int = 2048) -> dict:
 
     K, N, P, S = 16, 64, 8192, 65536
     f = synth.generate_frame(3, K=K, N=N, P=P, S=S, modulation="QAM16", snr_db=15.0, rapp_p=3.0)
-    cfg = dict(synth.CONFIG0_ALGORITHM, dictionarySize=8192)
-    dets = {m: L.NomaDetectorFactory.build(dict(cfg, detectVersion=m), N, num_users=K) for m in PRECISION_FORMS}
-    base = dets["balanced"]
     rx, tx, rxd = (torch.from_numpy(a).cuda() for a in (f.rx_train, f.tx_train, f.rx_data))
-    stream = torch.cuda.ExternalStream(base.stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-    base.train_device(rx, tx)
-    with torch.cuda.stream(stream):
-        e1.record(stream)
-    base.synchronize()
-    train_ms = e0.elapsed_time(e1)
-    state = base.get_state()
-    ref = model_fp64(state, base.gaussian_variance, 0.5, 0.5, f.rx_data[:, :sample])
+    est = torch.empty((K, S), dtype=torch.complex64, device="cuda")
     mod = f.modulation
-    ref_dec = mod.hard_decode_int(ref)
     true_dec = mod.hard_decode_int(f.tx_data)
-    forms = {}
-    for m, det in dets.items():
-        if det is not base:
-            det.copy_state_from(base)
-        est = torch.empty((K, S), dtype=torch.complex64, device="cuda")
-        st = torch.cuda.ExternalStream(det.stream)
-        det.detect_device(rxd, est)  # warm-up (workspace allocation)
-        det.synchronize()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
-        for a, b in ev:
-            with torch.cuda.stream(st):
-                a.record(st)
-            det.detect_device(rxd, est)
-            with torch.cuda.stream(st):
-                b.record(st)
-        det.synchronize()
-        ms = statistics.median(a.elapsed_time(b) for a, b in ev)
-        e = est.cpu().numpy()
-        es = e[:, :sample].astype(np.complex128)
-        err = np.abs(es - ref)
-        forms[m] = {
-            "detect_ms": round(ms, 3),
-            "symbols_per_s": K * S / (ms * 1e-3),
-            "soft_max_err_rel": float(err.max() / np.abs(ref).max()),
-            "soft_rms_err_rel": float(np.sqrt(np.mean(err ** 2) / np.mean(np.abs(ref) ** 2))),
-            "decisions_differing_from_fp64": float(np.mean(mod.hard_decode_int(es) != ref_dec)),
-            "ser": float(np.mean(mod.hard_decode_int(e) != true_dec)),
-        }
-    for det in dets.values():
-        det.close()
+    models = []
+    for label, variance in (("0.5 N^2", 0.5), ("0.05 N^2", 0.05)):
+        cfg = dict(synth.CONFIG0_ALGORITHM, dictionarySize=8192, gaussianKernelVariance=variance)
+        dets = {m: L.NomaDetectorFactory.build(dict(cfg, detectVersion=m), N, num_users=K) for m in PRECISION_FORMS}
+        base = dets["balanced"]
+        stream = torch.cuda.ExternalStream(base.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        base.train_device(rx, tx)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        base.synchronize()
+        train_ms = e0.elapsed_time(e1)
+        state = base.get_state()
+        ref = model_fp64(state, base.gaussian_variance, 0.5, 0.5, f.rx_data[:, :sample])
+        ref_dec = mod.hard_decode_int(ref)
+        forms = {}
+        for m, det in dets.items():
+            if det is not base:
+                det.copy_state_from(base)
+            st = torch.cuda.ExternalStream(det.stream)
+            det.detect_device(rxd, est)  # warm-up (workspace allocation)
+            det.synchronize()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+            for a, b in ev:
+                with torch.cuda.stream(st):
+                    a.record(st)
+                det.detect_device(rxd, est)
+                with torch.cuda.stream(st):
+                    b.record(st)
+            det.synchronize()
+            ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+            e = est.cpu().numpy()
+            es = e[:, :sample].astype(np.complex128)
+            err = np.abs(es - ref)
+            forms[m] = {
+                "detect_ms": round(ms, 3),
+                "symbols_per_s": K * S / (ms * 1e-3),
+                "soft_max_err_rel": float(err.max() / np.abs(ref).max()),
+                "soft_rms_err_rel": float(np.sqrt(np.mean(err ** 2) / np.mean(np.abs(ref) ** 2))),
+                "decisions_differing_from_fp64": float(np.mean(mod.hard_decode_int(es) != ref_dec)),
+                "ser": float(np.mean(mod.hard_decode_int(e) != true_dec)),
+            }
+        models.append({"variance": label, "variance_value": base.gaussian_variance, "train_ms": round(train_ms, 3),
+                       "ser_fp64_model": float(np.mean(ref_dec != true_dec[:, :sample])), "forms": forms})
+        for det in dets.values():
+            det.close()
     return {"workload": f"16QAM K={K} users N={N} P={P} S={S} 15 dB Rapp p=3, window 80, dictionary 8192, "
-                        "variance 0.5 N^2, one model detected in each form",
-            "train_ms": round(train_ms, 3), "fp64_sample_symbols": sample,
-            "ser_fp64_model": float(np.mean(ref_dec != true_dec[:, :sample])), "forms": forms}
+                        "one model per kernel width detected in each form",
+            "fp64_sample_symbols": sample, "models": models}
 
 
 # ------------------------------------------------------------ serving form --

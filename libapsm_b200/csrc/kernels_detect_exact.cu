@@ -9,10 +9,10 @@
 // the shuffle-down tree.  Given the same coefficients the soft outputs are
 // bit-identical to the reference's.
 //
-// B200 layout, up to 32 features: the data rows and every feature of the
+// B200 layout, up to 16 features: the data rows and every feature of the
 // warp's samples live in registers, dictionary tiles are staged feature-major
 // in shared memory so a warp's 32 rows are read without bank conflicts.
-// 64 and 128 features (detect_exact_wide_kernel): the block's samples sit in
+// 32 to 128 features (detect_exact_wide_kernel): the block's samples sit in
 // shared memory and are read as broadcast float4s, dictionary tiles arrive
 // row-major by asynchronous copies (double-buffered) and each lane works on
 // two rows for four samples at once, so eight independent distance chains
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(kWarps * 32) detect_exact_kernel(DetectArgs ar
     }
 }
 
-// ---------------------------------------------------------------- 64 / 128 features --
+// ----------------------------------------------------------- 32 to 128 features --
 constexpr int kWideRows = 64;  // dictionary rows per tile: two per lane
 constexpr int kWideSpw = 4;    // samples per warp
 constexpr int kWideUsers = 16; // users per pass
@@ -306,7 +306,7 @@ void launch_detect_exact(const DetectArgs& args, cudaStream_t stream)
     if (args.n_samples <= 0) return;
     if (args.D <= 8) launch_dp<8, 4>(args, stream);
     else if (args.D <= 16) launch_dp<16, 4>(args, stream);
-    else if (args.D <= 32) launch_dp<32, 2>(args, stream);
+    else if (args.D <= 32) launch_wide<32>(args, stream);
     else if (args.D <= 64) launch_wide<64>(args, stream);
     else launch_wide<128>(args, stream);
 }

@@ -36,7 +36,7 @@
 namespace apsm {
 
 constexpr int kTileM = 128;       // data rows per CTA tile (UMMA M)
-constexpr int kStages = 3;        // dictionary chunk ring
+constexpr int kMaxStages = 3;     // dictionary chunk ring (2 where 3 stages do not fit)
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = (kEpiWarps + 2) * 32;
 constexpr int kMaxUsers = 16;
@@ -137,8 +137,37 @@ struct GramArgs {
     int* err;
     int n_samples, Mpad, users, Kp, N;
     int chunks_per_split, n_chunks;
+    int stages; // dictionary chunks in flight (<= kMaxStages)
     float ewl2; // ew * log2(e)
 };
+
+// NC accumulator columns of one data row: squared distance from the cross term
+// and the norms, Gaussian value, contraction with every user's coefficients.
+// xs: the stage's norms (xs[0 .. NC)) and coefficient rows (xs[(1 + u) N + ...]).
+template <int NC, int NU>
+__device__ __forceinline__ void epilogue_columns(const float* gv, const float* xs, int N, float xn, float ewl2,
+                                                 int users, float* acc)
+{
+#pragma unroll
+    for (int j = 0; j < NC; j += 4) {
+        const float4 dn4 = *reinterpret_cast<const float4*>(xs + j);
+        float kv[4];
+        kv[0] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + 0], xn + dn4.x), 0.f));
+        kv[1] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + 1], xn + dn4.y), 0.f));
+        kv[2] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + 2], xn + dn4.z), 0.f));
+        kv[3] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + 3], xn + dn4.w), 0.f));
+#pragma unroll
+        for (int u = 0; u < NU; ++u) {
+            if (u < users) {
+                const float4 a4 = *reinterpret_cast<const float4*>(xs + (1 + u) * N + j);
+                acc[u] = fmaf(a4.x, kv[0], acc[u]);
+                acc[u] = fmaf(a4.y, kv[1], acc[u]);
+                acc[u] = fmaf(a4.z, kv[2], acc[u]);
+                acc[u] = fmaf(a4.w, kv[3], acc[u]);
+            }
+        }
+    }
+}
 
 template <int MODE, int NU>
 __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
@@ -151,11 +180,12 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
     const uint32_t x_bytes = uint32_t(g.N) * 4 * (1 + g.users); // dn + aw rows
     uint8_t* sA = smem;
     uint8_t* sB = sA + a_bytes;
-    float* sX = reinterpret_cast<float*>(sB + size_t(kStages) * b_bytes); // [stage][1 + users][N]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(sX) + size_t(kStages) * x_bytes);
-    uint64_t* full = bars;                 // [kStages]
-    uint64_t* empty = bars + kStages;      // [kStages]
-    uint64_t* tfull = bars + 2 * kStages;  // [2]
+    const int NS = g.stages;
+    float* sX = reinterpret_cast<float*>(sB + size_t(NS) * b_bytes); // [stage][1 + users][N]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(sX) + size_t(NS) * x_bytes);
+    uint64_t* full = bars;            // [NS]
+    uint64_t* empty = bars + NS;      // [NS]
+    uint64_t* tfull = bars + 2 * NS;  // [2]
     uint64_t* tempty = tfull + 2;          // [2]
     uint64_t* afull = tempty + 2;          // [1]
     uint64_t* done = afull + 1;            // [1] all MMAs of the CTA completed
@@ -172,7 +202,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
     const uint32_t ncols = uint32_t(2 * N);
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) {
+        for (int s = 0; s < NS; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1 + kEpiWarps);
         }
@@ -202,8 +232,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
             bulk_g2s(sA, g.a_ops + size_t(tile) * a_bytes, a_bytes, afull);
             int issued = 0;
             for (int i = 0; i < nch; ++i) {
-                const int s = i % kStages;
-                if (i >= kStages && !mbar_wait(&empty[s], ((i / kStages) - 1) & 1, abort_flag)) break;
+                const int s = i % NS;
+                if (i >= NS && !mbar_wait(&empty[s], ((i / NS) - 1) & 1, abort_flag)) break;
                 ++issued;
                 const int c = c0 + i;
                 mbar_expect_tx(&full[s], b_bytes + x_bytes);
@@ -215,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
             }
             // no bulk copy may still be writing shared memory when the CTA exits
             mbar_drain(afull, 0);
-            for (int i = max(0, issued - kStages); i < issued; ++i) mbar_drain(&full[i % kStages], (i / kStages) & 1);
+            for (int i = max(0, issued - NS); i < issued; ++i) mbar_drain(&full[i % NS], (i / NS) & 1);
         }
     } else if (warp == kEpiWarps + 1) {
         // ---------------- MMA issuer ----------------
@@ -225,8 +255,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
             const int ksteps = g.Kp / T::kStepK;
             const int lo_off = g.Kp / T::kChunk; // K chunks to the lo half
             for (int i = 0; i < nch; ++i) {
-                const int s = i % kStages, buf = i & 1;
-                if (!mbar_wait(&full[s], (i / kStages) & 1, abort_flag)) break;
+                const int s = i % NS, buf = i & 1;
+                if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag)) break;
                 if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag)) break;
                 tc_fence_after();
                 const uint8_t* b = sB + size_t(s) * b_bytes;
@@ -263,35 +293,25 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
         for (int u = 0; u < NU; ++u) acc[u] = 0.f;
         const int half = N / 2;
         for (int i = 0; i < nch; ++i) {
-            const int s = i % kStages, buf = i & 1;
+            const int s = i % NS, buf = i & 1;
             // the stage's norms / coefficients (bulk copies) and the accumulator
-            if (!mbar_wait(&full[s], (i / kStages) & 1, abort_flag)) break;
+            if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag)) break;
             if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag)) break;
             tc_fence_after();
             const float* xs = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(sX) + size_t(s) * x_bytes);
-            for (int cb = 0; cb < half; cb += 32) {
-                const int col = h * half + cb;
-                float gv[32];
-                tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * N + col), gv);
-#pragma unroll
-                for (int j = 0; j < 32; j += 4) {
-                    const float4 dn4 = *reinterpret_cast<const float4*>(xs + col + j);
-                    float kv[4];
-                    kv[0] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j + 0], xn + dn4.x), 0.f));
-                    kv[1] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j + 1], xn + dn4.y), 0.f));
-                    kv[2] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j + 2], xn + dn4.z), 0.f));
-                    kv[3] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j + 3], xn + dn4.w), 0.f));
-#pragma unroll
-                    for (int u = 0; u < NU; ++u) {
-                        if (u < g.users) {
-                            const float4 a4 = *reinterpret_cast<const float4*>(xs + (1 + u) * N + col + j);
-                            acc[u] = fmaf(a4.x, kv[0], acc[u]);
-                            acc[u] = fmaf(a4.y, kv[1], acc[u]);
-                            acc[u] = fmaf(a4.z, kv[2], acc[u]);
-                            acc[u] = fmaf(a4.w, kv[3], acc[u]);
-                        }
-                    }
+            const uint32_t trow = tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * N);
+            if (half >= 32) {
+                for (int cb = 0; cb < half; cb += 32) {
+                    const int col = h * half + cb;
+                    float gv[32];
+                    tmem_ld32(trow + uint32_t(col), gv);
+                    epilogue_columns<32, NU>(gv, xs + col, N, xn, g.ewl2, g.users, acc);
                 }
+            } else { // 32-column chunks: 16 columns per half
+                const int col = h * half;
+                float gv[16];
+                tmem_ld16(trow + uint32_t(col), gv);
+                epilogue_columns<16, NU>(gv, xs + col, N, xn, g.ewl2, g.users, acc);
             }
             tc_fence_before();
             __syncwarp();
@@ -364,14 +384,17 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     }
     const int Kp = int(round_up(uint32_t(D), uint32_t(T::kStepK)));
     const int KE = T::kSplit ? 2 * Kp : Kp;
-    // dictionary chunk width: keep the data tile and 3 stages within shared memory
-    int N = 256;
-    auto smem_for = [&](int n) {
-        return size_t(kTileM) * KE * T::kElem + size_t(kStages) * (size_t(n) * KE * T::kElem + size_t(n) * 4 * (1 + U)) +
-               (2 * kStages + 6) * 8 + 16 + size_t(4 * 32) * U * 4;
+    // dictionary chunk width and stages: the data tile and the chunk ring within shared memory
+    // (chunks of 256 down to 64 columns in 3 stages, then 32 columns in 3 or 2 stages)
+    int N = 256, stages = kMaxStages;
+    auto smem_for = [&](int n, int st) {
+        return size_t(kTileM) * KE * T::kElem + size_t(st) * (size_t(n) * KE * T::kElem + size_t(n) * 4 * (1 + U)) +
+               (2 * st + 6) * 8 + 16 + size_t(4 * 32) * U * 4;
     };
-    while (N > 64 && smem_for(N) > 220 * 1024) N /= 2;
-    if (smem_for(N) > 220 * 1024) {
+    const size_t limit = 220 * 1024;
+    while (N > 32 && smem_for(N, stages) > limit) N /= 2;
+    if (smem_for(N, stages) > limit) stages = 2;
+    if (smem_for(N, stages) > limit) {
         h->last_error = "Gram detection operands do not fit shared memory";
         return APSM_ERR_UNSUPPORTED;
     }
@@ -423,9 +446,10 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     ga.N = N;
     ga.chunks_per_split = cps;
     ga.n_chunks = n_chunks;
+    ga.stages = stages;
     ga.ewl2 = h->model_params().ew * 1.4426950408889634f;
     // >= 120 KB keeps one CTA per SM, so the 2N tensor-memory columns of a CTA never wait for another's
-    const size_t smem = std::max<size_t>(smem_for(N) + 1024, 120 * 1024);
+    const size_t smem = std::max<size_t>(smem_for(N, stages) + 1024, 120 * 1024);
     if (U <= 1) launch_gram<MODE, 1>(ga, n_tiles, splits, smem, s, &e);
     else if (U <= 2) launch_gram<MODE, 2>(ga, n_tiles, splits, smem, s, &e);
     else if (U <= 4) launch_gram<MODE, 4>(ga, n_tiles, splits, smem, s, &e);
