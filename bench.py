@@ -395,10 +395,12 @@ def run_precision_study(reps: int = 3, sample: int = 2048) -> dict:
 
 # ------------------------------------------------------------ serving form --
 def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = N_DET, lanes: int = 8,
-                max_batch: int = 16) -> dict:
+                max_batch: int = 16, detect_version: str = "balanced") -> dict:
     """Poisson per-TTI requests against resident detectors through the
     request server (continuous batching over `lanes` streams, at most
-    `max_batch` requests of one kind per batch).  Request samples sit in
+    `max_batch` requests of one kind per batch), detection in the FP32
+    CUDA-core pair form ("balanced") or a tensor-core form ("gram_bf16" ...).
+    Request samples sit in
     page-locked host buffers, as a radio front end's DMA buffers would; the
     latency of a request runs from its submission to its completion as the
     server's clock sees them (host samples in, estimates back in host memory)."""
@@ -411,7 +413,7 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
     pop = synth.config4_population(n_det)
     reqs = synth.config4_requests(pop, rate_hz, duration_s)
     warm_reqs = synth.config4_requests(pop, rate_hz, 0.05, seed=9)
-    cfg = dict(synth.CONFIG2_ALGORITHM)
+    cfg = dict(synth.CONFIG2_ALGORITHM, detectVersion=detect_version)
     pool = L.DetectorPool(cfg, lanes=lanes)
     ids = [pool.add(p.frame.N) for p in pop]
     pool.run([L.PoolJob(i, p.frame.rx_train, p.frame.tx_train) for i, p in zip(ids, pop)])
@@ -466,7 +468,8 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
             "deadline_500us_met": float(np.mean(lat_us <= 500.0)), "symbols_per_s": syms / (max(done) - start),
             "requests": len(reqs), "rate_hz": rate_hz, "duration_s": duration_s, "batches": int(b - b0),
             "avg_batch": float((jb - j0) / max(1, b - b0)), "lanes": lanes, "max_batch": max_batch,
-            "detect": "FP32 CUDA-core pair form",
+            "detect": "FP32 CUDA-core pair form" if detect_version == "balanced" else
+                      f"{detect_version} tensor-core pair form",
             "workload": "512 resident detectors (config-2 sizes, dictionarySize 2000); requests alternate "
                         "train-append (16-64 pilots) and detect (500-4000 symbols) per detector; Poisson arrivals; "
                         "request samples in page-locked host buffers"}
@@ -561,9 +564,15 @@ def main():
                          "benchmark, fewer only for profiling captures)")
     ap.add_argument("--precision-only", action="store_true",
                     help="run only the large-detect precision study (N=64, dictionary 8192) and print it")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="run only the served form (FP32 pair form and BF16 Gram detection) and print it")
     args = ap.parse_args()
     if args.precision_only:
         print(json.dumps({"precision": run_precision_study()}), flush=True)
+        return
+    if args.serving_only:
+        print(json.dumps({"serving": run_serving(), "serving_gram_bf16": run_serving(detect_version="gram_bf16")}),
+              flush=True)
         return
     if args.warmup < 3:
         args.warmup = 3
@@ -590,6 +599,7 @@ def main():
             os.environ["APSM_POOL_TRACE"] = args.trace_serving
         line["serving"] = run_serving()
         os.environ.pop("APSM_POOL_TRACE", None)
+        line["serving_gram_bf16"] = run_serving(detect_version="gram_bf16")
         line["precision"] = run_precision_study()
     if line is not None and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()

@@ -109,11 +109,11 @@ struct BatchGramJob {
     const float* nrm_s; // S norms
     const float* w;     // 2N linear weights
     float2* lin;        // S: wL <w, x_2s>, wL <w, x_2s+1>
-    uint8_t* a_ops;     // ceil(S / 128) sample tiles, UMMA canonical layout, TF32 hi | lo
+    uint8_t* a_ops;     // ceil(S / 128) sample tiles, UMMA canonical layout (hi [| lo] of the Gram form)
     const float2* Yd;   // Mp x Np dictionary samples
     const float* nrm_d; // Mp norms
     const float* a;     // 2 Mp coefficients
-    uint8_t* b_ops;     // n_chunks dictionary chunks (64 pairs = 128 rows), TF32 hi | lo
+    uint8_t* b_ops;     // n_chunks dictionary chunks (64 pairs = 128 rows), same layout
     float* bx;          // n_chunks x (128 a*wG + 64 norms)
     float2* out;        // S soft estimates
     int S, N, Np, Kp, Mp, n_chunks;
@@ -163,15 +163,18 @@ cudaError_t launch_batch_detect(const BatchDetectJob* d_jobs, int n_jobs, int ma
 int batch_detect_tile();  // samples per block of launch_batch_detect
 int batch_detect_chunk(); // dictionary pairs per chunk of launch_batch_detect
 
-// Tensor-core detection of jobs with Kp <= Kp_max (Kp = 2N rounded up to 8,
-// Kp_max in {8, 16, 32, 64}): operand packing and the Gram kernel, whose CTA
-// t works on tile t - tile_prefix[j] of job j.
+// Tensor-core detection of jobs with Kp <= Kp_max in one Gram form `mode`
+// (GramMode: kBF16, kBF16x3, kTF32, kTF32x3).  Kp = 2N rounded up to the K of
+// one UMMA (8 TF32 or 16 BF16 elements), Kp_max in {8, 16, 32, 64}: operand
+// packing and the Gram kernel, whose CTA t works on tile t - tile_prefix[j]
+// of job j.
 int batch_gram_tile();        // samples per tile
 int batch_gram_chunk_pairs(); // dictionary pairs per chunk
-size_t batch_gram_a_bytes(int Kp);
-size_t batch_gram_b_bytes(int Kp);
+int batch_gram_kp(int mode, int N);
+size_t batch_gram_a_bytes(int mode, int Kp);
+size_t batch_gram_b_bytes(int mode, int Kp);
 size_t batch_gram_bx_floats();
-cudaError_t launch_batch_gram(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
+cudaError_t launch_batch_gram(int mode, const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
                               const int* d_tile_prefix, int total_tiles, int Kp_max, float wL, float wG, int* d_err,
                               cudaStream_t s);
 

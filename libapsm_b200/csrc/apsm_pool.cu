@@ -10,6 +10,7 @@
 // detection launches (one per antenna class).
 #include "apsm_batch.cuh"
 #include "apsm_host.hpp"
+#include "apsm_tc.cuh"
 
 #include <algorithm>
 #include <array>
@@ -197,6 +198,7 @@ int detect_class(uint32_t N)
 
 struct apsm_pool {
     Config cfg;
+    int gram_mode = kTF32x3; // GramMode of tensor-core detection (cfg.detect_mode != Exact)
     BatchCommon cm{};
     uint64_t budget = 0;
     uint64_t resident = 0;
@@ -435,9 +437,9 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             d.det = &dets[jobs[i].detector];
             d.S = jobs[i].length;
             d.Mp = used_after[jobs[i].detector] / 2;
-            d.gram = cfg.detect_mode == DetectMode::GramTF32x3 && d.det->N <= 32;
+            d.gram = cfg.detect_mode != DetectMode::Exact && d.det->N <= 32;
             if (d.gram) {
-                d.Kp = int(round_up(2 * d.det->N, 8));
+                d.Kp = batch_gram_kp(gram_mode, int(d.det->N));
                 d.cls = gram_class(d.Kp);
                 d.tiles = int((d.S + batch_gram_tile() - 1) / batch_gram_tile());
                 d.chunks = int((d.Mp + batch_gram_chunk_pairs() - 1) / batch_gram_chunk_pairs());
@@ -549,8 +551,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             o = align_up(o + sizeof(float2) * size_t(d.S) * std::max<size_t>(chunks, 1), 256);
         }
         if (d.gram) {
-            d.off_aops = o; o = align_up(o + batch_gram_a_bytes(d.Kp) * d.tiles, 256);
-            d.off_bops = o; o = align_up(o + batch_gram_b_bytes(d.Kp) * std::max(d.chunks, 1), 256);
+            d.off_aops = o; o = align_up(o + batch_gram_a_bytes(gram_mode, d.Kp) * d.tiles, 256);
+            d.off_bops = o; o = align_up(o + batch_gram_b_bytes(gram_mode, d.Kp) * std::max(d.chunks, 1), 256);
             d.off_bx = o; o = align_up(o + sizeof(float) * batch_gram_bx_floats() * std::max(d.chunks, 1), 256);
             d.off_lin = o; o = align_up(o + sizeof(float2) * d.S, 256);
         }
@@ -843,7 +845,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         const int* d_gp = reinterpret_cast<const int*>(D(off_gp));
         for (const auto& g : gseg) {
             const size_t base = size_t(g[0]) - nC;
-            POOL_CK(launch_batch_gram(d_gj + base, g[1] - g[0], g[4], g[5], d_gp + g[2], g[3], dp[g[0]].cls, cfg.wL,
+            POOL_CK(launch_batch_gram(gram_mode, d_gj + base, g[1] - g[0], g[4], g[5], d_gp + g[2], g[3], dp[g[0]].cls, cfg.wL,
                                       cfg.wG, d_err, s));
             L.launches += (g[4] > 0) + (g[5] > 0) + (g[3] > 0);
         }
@@ -957,8 +959,6 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
     else if (cfg.step % 2 != 0 || cfg.step == 0 || cfg.step > 8) why = "the detector pool needs an even sampleStep <= 8";
     else if (cfg.dict_size < cfg.window + cfg.step / 2) why = "the detector pool needs dictionarySize >= windowSize + sampleStep / 2";
     else if (cfg.window == 0) why = "windowSize must be >= 1";
-    else if (cfg.detect_mode != DetectMode::Exact && cfg.detect_mode != DetectMode::GramTF32x3)
-        why = "the detector pool implements detectVersion gram_tf32x3 (tensor cores) and the FP32 CUDA-core form";
     if (!why.empty()) {
         copy_err(err, errlen, why);
         return APSM_ERR_UNSUPPORTED;
@@ -971,6 +971,12 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
     }
     auto* p = new apsm_pool();
     p->cfg = cfg;
+    switch (cfg.detect_mode) {
+    case DetectMode::GramBF16: p->gram_mode = kBF16; break;
+    case DetectMode::GramBF16x3: p->gram_mode = kBF16x3; break;
+    case DetectMode::GramTF32: p->gram_mode = kTF32; break;
+    default: p->gram_mode = kTF32x3; break;
+    }
     p->budget = hbm_budget_bytes;
     BatchCommon& cm = p->cm;
     cm.wL = cfg.wL;

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 namespace apsm {
@@ -10,6 +11,39 @@ namespace apsm {
 enum GramMode : int { kBF16 = 0, kBF16x3 = 1, kTF32 = 2, kTF32x3 = 3 };
 
 namespace tc {
+
+// Operand format of a Gram mode: element type and the K extent of one UMMA
+// (32 bytes); split modes carry a lo half after the hi half along K.
+template <int MODE> struct OpTraits {
+    static constexpr bool kTF = (MODE == kTF32 || MODE == kTF32x3);
+    static constexpr bool kSplit = (MODE == kBF16x3 || MODE == kTF32x3);
+    static constexpr int kElem = kTF ? 4 : 2;     // bytes per operand element
+    static constexpr int kChunk = 16 / kElem;     // elements per 16-byte K chunk
+    static constexpr int kStepK = 2 * kChunk;     // K per UMMA instruction (32 bytes)
+};
+
+// x = hi + lo with hi in the operand format (round to nearest) and lo the FP32 rest
+template <int MODE> __device__ __forceinline__ void split_operand(float x, float* hi, float* lo)
+{
+    if constexpr (OpTraits<MODE>::kTF) {
+        uint32_t h;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+        *hi = __uint_as_float(h);
+    } else {
+        *hi = __bfloat162float(__float2bfloat16_rn(x));
+    }
+    *lo = x - *hi;
+}
+
+// element (r, k) of a tile of R rows in the canonical K-major no-swizzle layout:
+// byte (k / kc) * R * 16 + (r / 8) * 128 + (r % 8) * 16 + (k % kc) * elem
+template <int MODE> __device__ __forceinline__ void put_operand(uint8_t* tile, int R, int r, int k, float v)
+{
+    using T = OpTraits<MODE>;
+    uint8_t* p = tile + size_t(k / T::kChunk) * (R * 16) + (r >> 3) * 128 + (r & 7) * 16 + (k % T::kChunk) * T::kElem;
+    if constexpr (T::kTF) *reinterpret_cast<float*>(p) = v;
+    else *reinterpret_cast<__nv_bfloat16*>(p) = __float2bfloat16_rn(v);
+}
 
 constexpr unsigned long long kWaitLimitNs = 2000000000ull; // bounded mbarrier waits (error instead of a hang)
 

@@ -1,5 +1,7 @@
-// Batched tensor-core detection in pair form (tcgen05, TF32 operands split
-// hi + lo, three UMMAs per K step: FP32-accurate Gram products).
+// Batched tensor-core detection in pair form (tcgen05).  Operands in one of
+// the four Gram forms of the single detector: BF16 or TF32 (one UMMA per K
+// step), or split hi + lo (three UMMAs per K step: bf16x3 ~2^-16 relative,
+// tf32x3 FP32-accurate Gram products).
 //
 // For data sample s and dictionary pair b (complex y_b) the detector needs
 // r = Re(y_b^H x_s) and m = Im(y_b^H x_s) (kernel values of the four row
@@ -35,27 +37,21 @@ constexpr int kEpiWarps = 8;
 constexpr int kThreads = (kEpiWarps + 2) * 32;
 constexpr int kBx = 2 * kChunkPairs + kChunkPairs; // per chunk: a*wG (128, column order) then pair norms (64)
 
-__device__ __forceinline__ uint32_t tf32_bits(float x)
+// bytes of one operand tile of R rows at K extent Kp (hi [+ lo])
+template <int MODE> __host__ __device__ constexpr size_t tile_bytes(int R, int Kp)
 {
-    uint32_t h;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-    return h;
+    return size_t(R) * (OpTraits<MODE>::kSplit ? 2 * Kp : Kp) * OpTraits<MODE>::kElem;
 }
 
-// canonical K-major, no-swizzle byte offset of element (r, k) in a tile of R rows (4-byte elements)
-__device__ __forceinline__ size_t canon_off(int r, int k, int R)
-{
-    return size_t(k >> 2) * (R * 16) + (r >> 3) * 128 + (r & 7) * 16 + (k & 3) * 4;
-}
-
-// A operand tiles (hi then lo halves along K), the samples' linear terms wL <w, x>.
+// A operand tiles (hi [then lo] halves along K), the samples' linear terms wL <w, x>.
+template <int MODE>
 __global__ void __launch_bounds__(256) batch_gram_pack_a_kernel(const BatchGramJob* __restrict__ jobs, float wL)
 {
     const BatchGramJob& jb = jobs[blockIdx.y];
     const int t = blockIdx.x;
     if (t * kTileM >= jb.S) return;
-    const int N = jb.N, Np = jb.Np, Kp = jb.Kp, KE = 2 * Kp;
-    uint8_t* tile = jb.a_ops + size_t(t) * kTileM * KE * 4;
+    const int N = jb.N, Np = jb.Np, Kp = jb.Kp;
+    uint8_t* tile = jb.a_ops + size_t(t) * tile_bytes<MODE>(kTileM, Kp);
     for (int idx = threadIdx.x; idx < kTileM * Kp; idx += blockDim.x) {
         const int r = idx / Kp, k = idx % Kp;
         const int s = t * kTileM + r;
@@ -64,9 +60,10 @@ __global__ void __launch_bounds__(256) batch_gram_pack_a_kernel(const BatchGramJ
             const float2 v = jb.Ys[size_t(s) * Np + (k < N ? k : k - N)];
             x = k < N ? v.x : v.y;
         }
-        const float hi = __uint_as_float(tf32_bits(x));
-        *reinterpret_cast<float*>(tile + canon_off(r, k, kTileM)) = hi;
-        *reinterpret_cast<float*>(tile + canon_off(r, Kp + k, kTileM)) = x - hi;
+        float hi, lo;
+        split_operand<MODE>(x, &hi, &lo);
+        put_operand<MODE>(tile, kTileM, r, k, hi);
+        if constexpr (OpTraits<MODE>::kSplit) put_operand<MODE>(tile, kTileM, r, Kp + k, lo);
     }
     for (int r = threadIdx.x; r < kTileM; r += blockDim.x) {
         const int s = t * kTileM + r;
@@ -84,13 +81,14 @@ __global__ void __launch_bounds__(256) batch_gram_pack_a_kernel(const BatchGramJ
 
 // B operand chunks of the job's dictionary (two rows per pair) and per chunk
 // the coefficients a*wG and the pair norms.
+template <int MODE>
 __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJob* __restrict__ jobs, float wG)
 {
     const BatchGramJob& jb = jobs[blockIdx.y];
     const int c = blockIdx.x;
     if (c >= jb.n_chunks) return;
-    const int N = jb.N, Np = jb.Np, Kp = jb.Kp, KE = 2 * Kp;
-    uint8_t* chunk = jb.b_ops + size_t(c) * kChunkN * KE * 4;
+    const int N = jb.N, Np = jb.Np, Kp = jb.Kp;
+    uint8_t* chunk = jb.b_ops + size_t(c) * tile_bytes<MODE>(kChunkN, Kp);
     for (int idx = threadIdx.x; idx < kChunkN * Kp; idx += blockDim.x) {
         const int r = idx / Kp, k = idx % Kp;
         const int b = c * kChunkPairs + (r >> 1);
@@ -100,9 +98,10 @@ __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJ
             // row 2j: [Re y; Im y]; row 2j+1: [-Im y; Re y]
             x = (r & 1) == 0 ? (k < N ? v.x : v.y) : (k < N ? -v.y : v.x);
         }
-        const float hi = __uint_as_float(tf32_bits(x));
-        *reinterpret_cast<float*>(chunk + canon_off(r, k, kChunkN)) = hi;
-        *reinterpret_cast<float*>(chunk + canon_off(r, Kp + k, kChunkN)) = x - hi;
+        float hi, lo;
+        split_operand<MODE>(x, &hi, &lo);
+        put_operand<MODE>(chunk, kChunkN, r, k, hi);
+        if constexpr (OpTraits<MODE>::kSplit) put_operand<MODE>(chunk, kChunkN, r, Kp + k, lo);
     }
     float* bx = jb.bx + size_t(c) * kBx;
     for (int i = threadIdx.x; i < kBx; i += blockDim.x) {
@@ -118,10 +117,12 @@ __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJ
     }
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
-    batch_gram_kernel(const BatchGramJob* __restrict__ jobs, int n_jobs, const int* __restrict__ tile_prefix, int KEmax,
+    batch_gram_kernel(const BatchGramJob* __restrict__ jobs, int n_jobs, const int* __restrict__ tile_prefix, int Kpmax,
                       int stages, int* err)
 {
+    using T = OpTraits<MODE>;
     // job of this CTA: tile_prefix[j] <= blockIdx.x < tile_prefix[j + 1]
     int lo = 0, hi = n_jobs;
     while (hi - lo > 1) {
@@ -131,15 +132,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     const BatchGramJob& jb = jobs[lo];
     const int tile = int(blockIdx.x) - tile_prefix[lo];
-    const int KE = 2 * jb.Kp;
     const int nch = jb.n_chunks;
 
     extern __shared__ __align__(1024) uint8_t smem[];
-    const uint32_t a_bytes = uint32_t(kTileM) * KE * 4;
-    const uint32_t b_bytes = uint32_t(kChunkN) * KE * 4;
-    const uint32_t b_stride = uint32_t(kChunkN) * KEmax * 4;
+    const uint32_t a_bytes = uint32_t(tile_bytes<MODE>(kTileM, jb.Kp));
+    const uint32_t b_bytes = uint32_t(tile_bytes<MODE>(kChunkN, jb.Kp));
+    const uint32_t b_stride = uint32_t(tile_bytes<MODE>(kChunkN, Kpmax));
     uint8_t* sA = smem;
-    uint8_t* sB = sA + size_t(kTileM) * KEmax * 4;
+    uint8_t* sB = sA + tile_bytes<MODE>(kTileM, Kpmax);
     float* sX = reinterpret_cast<float*>(sB + size_t(stages) * b_stride); // [stages][kBx]
     uint64_t* bars = reinterpret_cast<uint64_t*>(sX + size_t(stages) * kBx);
     uint64_t* full = bars;                // [stages]
@@ -199,10 +199,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp == kEpiWarps + 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0 && nch > 0 && mbar_wait(afull, 0, abort_flag)) {
-            const uint32_t idesc = instr_desc<kTF32x3>(kTileM, kChunkN);
+            const uint32_t idesc = instr_desc<MODE>(kTileM, kChunkN);
             const uint32_t lbo_a = kTileM * 16, lbo_b = kChunkN * 16;
-            const int ksteps = jb.Kp / 8; // 8 TF32 elements (32 bytes) per UMMA K step
-            const int lo_off = jb.Kp / 4; // 16-byte K chunks to the lo half
+            const int ksteps = jb.Kp / T::kStepK; // 32 bytes of K per UMMA
+            const int lo_off = jb.Kp / T::kChunk; // 16-byte K chunks to the lo half
             for (int i = 0; i < nch; ++i) {
                 const int s = i % stages, buf = i & 1;
                 if (!mbar_wait(&full[s], (i / stages) & 1, abort_flag)) break;
@@ -213,11 +213,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int kk = 0; kk < ksteps; ++kk) {
                     const uint64_t ah = smem_desc(sA + size_t(2 * kk) * lbo_a, lbo_a, 128);
                     const uint64_t bh = smem_desc(b + size_t(2 * kk) * lbo_b, lbo_b, 128);
-                    const uint64_t al = smem_desc(sA + size_t(lo_off + 2 * kk) * lbo_a, lbo_a, 128);
-                    const uint64_t bl = smem_desc(b + size_t(lo_off + 2 * kk) * lbo_b, lbo_b, 128);
-                    umma<kTF32x3>(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
-                    umma<kTF32x3>(d, ah, bl, idesc, 1u);
-                    umma<kTF32x3>(d, al, bh, idesc, 1u);
+                    umma<MODE>(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
+                    if constexpr (T::kSplit) {
+                        const uint64_t al = smem_desc(sA + size_t(lo_off + 2 * kk) * lbo_a, lbo_a, 128);
+                        const uint64_t bl = smem_desc(b + size_t(lo_off + 2 * kk) * lbo_b, lbo_b, 128);
+                        umma<MODE>(d, ah, bl, idesc, 1u);
+                        umma<MODE>(d, al, bh, idesc, 1u);
+                    }
                 }
                 umma_commit(&tfull[buf]);
                 umma_commit(&empty[s]);
@@ -294,40 +296,72 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (threadIdx.x == 0 && *abort_flag) atomicExch(err, 1);
 }
 
-size_t gram_smem(int KEmax, int stages)
+template <int MODE> size_t gram_smem(int Kpmax, int stages)
 {
-    return size_t(kTileM) * KEmax * 4 + size_t(stages) * kChunkN * KEmax * 4 + size_t(stages) * kBx * 4 +
-           sizeof(uint64_t) * (2 * stages + 6) + 16 + sizeof(float2) * kTileM + 1024;
+    return tile_bytes<MODE>(kTileM, Kpmax) + size_t(stages) * tile_bytes<MODE>(kChunkN, Kpmax) +
+           size_t(stages) * kBx * 4 + sizeof(uint64_t) * (2 * stages + 6) + 16 + sizeof(float2) * kTileM + 1024;
+}
+
+template <int MODE>
+cudaError_t launch_mode(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
+                        const int* d_tile_prefix, int total_tiles, int Kp, float wL, float wG, int* d_err,
+                        cudaStream_t s)
+{
+    if (Kp % OpTraits<MODE>::kStepK != 0 || Kp > 64) return cudaErrorInvalidValue;
+    if (max_tiles > 0) batch_gram_pack_a_kernel<MODE><<<dim3(max_tiles, n_jobs), 256, 0, s>>>(d_jobs, wL);
+    if (max_chunks > 0) batch_gram_pack_b_kernel<MODE><<<dim3(max_chunks, n_jobs), 256, 0, s>>>(d_jobs, wG);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || total_tiles <= 0) return e;
+    // two pipeline stages when that lets two CTAs share an SM, else three if they fit
+    int stages = (2 * gram_smem<MODE>(Kp, 3) > 227 * 1024) ? 2 : 3;
+    // every CTA holds 256 TMEM columns: at most two CTAs per SM (512 columns), so
+    // shared memory is padded to more than a third of the SM's
+    const size_t smem = std::max<size_t>(gram_smem<MODE>(Kp, stages), 80 * 1024);
+    e = cudaFuncSetAttribute(batch_gram_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    batch_gram_kernel<MODE><<<total_tiles, kThreads, smem, s>>>(d_jobs, n_jobs, d_tile_prefix, Kp, stages, d_err);
+    return cudaGetLastError();
 }
 
 } // namespace
 
 int batch_gram_tile() { return kTileM; }
 int batch_gram_chunk_pairs() { return kChunkPairs; }
-size_t batch_gram_a_bytes(int Kp) { return size_t(kTileM) * 2 * Kp * 4; }
-size_t batch_gram_b_bytes(int Kp) { return size_t(kChunkN) * 2 * Kp * 4; }
+int batch_gram_kp(int mode, int N)
+{
+    const int step = (mode == kTF32 || mode == kTF32x3) ? tc::OpTraits<kTF32>::kStepK : tc::OpTraits<kBF16>::kStepK;
+    return int(round_up(uint32_t(2 * N), uint32_t(step)));
+}
+size_t batch_gram_a_bytes(int mode, int Kp)
+{
+    return size_t(kTileM) * ((mode == kBF16x3 || mode == kTF32x3) ? 2 * Kp : Kp) *
+           ((mode == kTF32 || mode == kTF32x3) ? 4 : 2);
+}
+size_t batch_gram_b_bytes(int mode, int Kp)
+{
+    return batch_gram_a_bytes(mode, Kp) / kTileM * kChunkN;
+}
 size_t batch_gram_bx_floats() { return kBx; }
 
-cudaError_t launch_batch_gram(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
+cudaError_t launch_batch_gram(int mode, const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
                               const int* d_tile_prefix, int total_tiles, int Kp, float wL, float wG, int* d_err,
                               cudaStream_t s)
 {
     if (n_jobs <= 0) return cudaSuccess;
-    if (Kp % 8 != 0 || Kp > 64) return cudaErrorInvalidValue;
-    if (max_tiles > 0) batch_gram_pack_a_kernel<<<dim3(max_tiles, n_jobs), 256, 0, s>>>(d_jobs, wL);
-    if (max_chunks > 0) batch_gram_pack_b_kernel<<<dim3(max_chunks, n_jobs), 256, 0, s>>>(d_jobs, wG);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || total_tiles <= 0) return e;
-    const int KE = 2 * Kp;
-    // two pipeline stages when that lets two CTAs share an SM, else three if they fit
-    int stages = (2 * gram_smem(KE, 3) > 227 * 1024) ? 2 : 3;
-    // every CTA holds 256 TMEM columns: at most two CTAs per SM (512 columns), so
-    // shared memory is padded to more than a third of the SM's
-    const size_t smem = std::max<size_t>(gram_smem(KE, stages), 80 * 1024);
-    e = cudaFuncSetAttribute(batch_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    batch_gram_kernel<<<total_tiles, kThreads, smem, s>>>(d_jobs, n_jobs, d_tile_prefix, KE, stages, d_err);
-    return cudaGetLastError();
+    switch (mode) {
+    case kBF16:
+        return launch_mode<kBF16>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err, s);
+    case kBF16x3:
+        return launch_mode<kBF16x3>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err,
+                                    s);
+    case kTF32:
+        return launch_mode<kTF32>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err, s);
+    case kTF32x3:
+        return launch_mode<kTF32x3>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err,
+                                    s);
+    default:
+        return cudaErrorInvalidValue;
+    }
 }
 
 } // namespace apsm

@@ -59,14 +59,6 @@ namespace {
 
 using namespace tc;
 
-template <int MODE> struct OpTraits {
-    static constexpr bool kTF = (MODE == kTF32 || MODE == kTF32x3);
-    static constexpr bool kSplit = (MODE == kBF16x3 || MODE == kTF32x3);
-    static constexpr int kElem = kTF ? 4 : 2;     // bytes per operand element
-    static constexpr int kChunk = 16 / kElem;     // elements per 16-byte K chunk
-    static constexpr int kStepK = 2 * kChunk;     // K per UMMA instruction (32 bytes)
-};
-
 // ------------------------------------------------------ operand packing --
 
 // rows: n x Dp fp32.  Writes tiles of R rows: element (r, k) of tile t at byte
@@ -87,23 +79,10 @@ __global__ void gram_pack_kernel(const float* __restrict__ rows, int n, int Dp, 
         const int row = t * R + r;
         const float x = (row < n && k < D) ? rows[size_t(row) * Dp + k] : 0.f;
         float hi, lo;
-        if constexpr (T::kTF) {
-            uint32_t h;
-            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-            hi = __uint_as_float(h);
-            lo = x - hi;
-        } else {
-            hi = __bfloat162float(__float2bfloat16_rn(x));
-            lo = x - hi;
-        }
+        split_operand<MODE>(x, &hi, &lo);
         uint8_t* tile = ops + size_t(t) * R * KE * T::kElem;
-        auto put = [&](int kk, float v) {
-            uint8_t* p = tile + size_t(kk / T::kChunk) * (R * 16) + (r / 8) * 128 + (r % 8) * 16 + (kk % T::kChunk) * T::kElem;
-            if constexpr (T::kTF) *reinterpret_cast<float*>(p) = v;
-            else *reinterpret_cast<__nv_bfloat16*>(p) = __float2bfloat16_rn(v);
-        };
-        put(k, hi);
-        if constexpr (T::kSplit) put(Kp + k, lo);
+        put_operand<MODE>(tile, R, r, k, hi);
+        if constexpr (T::kSplit) put_operand<MODE>(tile, R, r, Kp + k, lo);
     }
     if (norms) {
         for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {

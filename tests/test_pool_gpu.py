@@ -72,6 +72,35 @@ def test_pool_matches_oracle_per_detector(native_lib, oracle_mod, cfg):
         assert _rel(est, ref) < TOL, (k, N, _rel(est, ref))
 
 
+# Operand precision of the pool's other tensor-core forms: the cross term y^H x
+# carries ~2^-8 (bf16), ~2^-11 (tf32) or ~2^-16 (bf16x3) relative error of
+# |y||x|, which reaches each Gaussian term scaled by |ew|.
+GRAM_TOL = {"gram_bf16": 1e-2, "gram_tf32": 2e-3, "gram_bf16x3": 1e-4}
+
+
+@pytest.mark.parametrize("narrow", [False, True], ids=["wide", "narrow"])
+@pytest.mark.parametrize("dv", sorted(GRAM_TOL))
+def test_pool_gram_forms_match_oracle(native_lib, oracle_mod, dv, narrow):
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    cfg = dict(CFG, detectVersion=dv)
+    if narrow:
+        cfg.update(windowSize=80, dictionarySize=2000, gaussianKernelVariance=0.05, eB=0.001)
+    pool = DetectorPool(cfg)
+    specs = [(3, 120, 200), (4, 300, 96), (8, 60, 50), (16, 250, 300), (2, 31, 17), (32, 150, 128)]
+    dets, frames = [], []
+    for i, (N, P, S) in enumerate(specs):
+        dets.append(pool.add(N))
+        frames.append((N,) + _frame(300 + i, N, P, S, "QAM16"))
+    jobs = [PoolJob(d, f[1], f[2]) for d, f in zip(dets, frames)] + [PoolJob(d, f[3]) for d, f in zip(dets, frames)]
+    outs = pool.run(jobs)
+    for k, (N, rx, tx, rxd) in enumerate(frames):
+        ref = _oracle_run(oracle_mod, cfg, N, [(rx, tx)], rxd)
+        err = _rel(outs[len(specs) + k], ref)
+        print(f"{dv} {'narrow' if narrow else 'wide'} N={N}: {err:.3e}")
+        assert err < GRAM_TOL[dv], (k, N, err)
+
+
 def test_pool_train_append_and_eviction(native_lib, oracle_mod):
     """Pilots appended to the resident dictionary over several batches; the
     dictionary (200 entries) fills and evicts its oldest entries."""
@@ -95,7 +124,7 @@ def test_pool_train_append_and_eviction(native_lib, oracle_mod):
     assert rows == 2 * 200
 
 
-@pytest.mark.parametrize("dv", ["balanced", "gram_tf32x3"])
+@pytest.mark.parametrize("dv", ["balanced", "gram_tf32x3", "gram_bf16"])
 def test_pool_alone_equals_in_mix(native_lib, dv):
     from libapsm_b200 import DetectorPool, PoolJob
 
