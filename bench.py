@@ -53,6 +53,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "detected symbols/s (batched APSM train + detect, 512 heterogeneous detectors)"
 UNIT = "symbols/s"
 N_DET = 512
+# DRAM bytes per algorithmic byte of the batched sweep (ncu capture of the first
+# 32 detectors: 367.8 MB read + 4.6 MB written for 361.3 MB algorithmic)
+SWEEP_TRAFFIC_PER_ALG_BYTE = (367.794176 + 4.560128) / 361.273728
 WORKLOAD = {"workload": "512 detectors: N~U{4,8,16,32}, P~U[200,2000], S~U[1000,16000], SNR~U[10,25] dB, "
                         "QPSK/16QAM, window 80, dictionary 2000, fresh train + detect per step",
             "detectors": N_DET, "window": 80, "dictionary": 2000, "detect": "gram_tf32x3 (FP32-accurate)",
@@ -243,7 +246,11 @@ def run_batched(args, rank: int, world: int) -> dict | None:
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "batch_sweep_kernel (training sweep, all 512 jobs)",
                      "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
-                     "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_ms": sweep,
+                     "traffic": alg * SWEEP_TRAFFIC_PER_ALG_BYTE, "algorithmic_bytes_per_launch": alg,
+                     "launch_ms": sweep,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of the "
+                                       "32-detector case (372.4 MB for 361.3 MB algorithmic), scaled to this "
+                                       "launch by its algorithmic bytes",
                      "note": "a chain of P dependent steps per detector: latency / shared-memory bound, "
                              "not HBM; see profiles/",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},

@@ -52,6 +52,10 @@ struct Lane {
     cudaEvent_t ev[6] = {};     // train start/end, detect start/end, sweep start/end
     cudaEvent_t done = nullptr;                                // end of the last batch
     cudaEvent_t desc_copied = nullptr;                         // the pinned descriptors were consumed
+    // detection inputs copied while the batch trains: a second stream, ordered after the
+    // lane's earlier work (ev_start) and joined before the detections (ev_inputs)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_inputs = nullptr;
     bool have_train = false, have_detect = false;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -73,6 +77,7 @@ struct Lane {
     // trained (dictionary copied back), detected
     cudaEvent_t tr[7] = {};
     double t_run0 = 0, t_run1 = 0;
+    double t_mark[3] = {0, 0, 0}; // run(): planned, descriptors written, inputs staged
     int tr_nT = 0, tr_nD = 0;
     bool traced = false;
 };
@@ -116,8 +121,17 @@ public:
         size_t bytes;
     };
 
-    void copy(std::vector<Range>& pieces)
+    void copy(const std::vector<Range>& pieces)
     {
+        begin(pieces);
+        wait();
+    }
+
+    // Starts the copies (small totals: done here and now) and returns; wait() joins them,
+    // the calling thread taking pieces too.
+    void begin(const std::vector<Range>& pieces)
+    {
+        wait();
         size_t total = 0;
         for (const auto& r : pieces) total += r.bytes;
         if (total < kStageSplit) {
@@ -125,23 +139,30 @@ public:
             return;
         }
         start();
-        // cut every input into kStageGrain pieces; helpers and this thread take pieces in turn
-        std::vector<Range> work;
+        // cut every input into kStageGrain pieces; helpers and the waiting thread take pieces in turn
+        work_own_.clear();
         for (const auto& r : pieces)
             for (size_t o = 0; o < r.bytes; o += kStageGrain)
-                work.push_back({r.dst + o, r.src + o, std::min(kStageGrain, r.bytes - o)});
+                work_own_.push_back({r.dst + o, r.src + o, std::min(kStageGrain, r.bytes - o)});
         {
             std::lock_guard<std::mutex> g(mu_);
-            work_ = &work;
+            work_ = &work_own_;
             next_.store(0);
             busy_ = unsigned(th_.size());
             ++gen_;
         }
+        active_ = true;
         cv_.notify_all();
-        drain(work);
+    }
+
+    void wait()
+    {
+        if (!active_) return;
+        drain(work_own_);
         std::unique_lock<std::mutex> lk(mu_);
         done_cv_.wait(lk, [&] { return busy_ == 0; });
         work_ = nullptr;
+        active_ = false;
     }
 
 private:
@@ -178,6 +199,8 @@ private:
     }
 
     std::vector<std::thread> th_;
+    std::vector<Range> work_own_; // pieces of the copies in flight
+    bool active_ = false;         // begin() started copies that wait() has not joined
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;
     std::vector<Range>* work_ = nullptr;
@@ -186,6 +209,8 @@ private:
     uint64_t gen_ = 0;
     bool stop_ = false;
 };
+
+constexpr size_t kDirectOutJobs = 16; // detection jobs whose estimates are copied to the caller one by one
 
 int detect_class(uint32_t N)
 {
@@ -212,6 +237,24 @@ struct apsm_pool {
     cudaMemPool_t mempool = nullptr; // lane scratch (stream-ordered; keeps its memory mapped)
     Stager stager;                   // host-input staging (helper threads for large batches)
     std::map<uint32_t, std::vector<int>> perms;
+    // training schedules by (rows before the call, pilots): the same request shapes recur
+    // from batch to batch, and a batch of 512 detectors would rebuild ~600 k steps each time
+    struct Schedule {
+        std::vector<TrainStep> steps;
+        int final_hi = 0;
+    };
+    std::map<std::pair<uint32_t, uint32_t>, Schedule> schedules;
+    const std::vector<TrainStep>& schedule(uint32_t used_before, uint32_t P, int* final_hi)
+    {
+        auto it = schedules.find({used_before, P});
+        if (it == schedules.end()) {
+            Schedule sc;
+            sc.steps = build_schedule(cfg, used_before, P, 2 * cfg.dict_size, &sc.final_hi);
+            it = schedules.emplace(std::make_pair(used_before, P), std::move(sc)).first;
+        }
+        *final_hi = it->second.final_hi;
+        return it->second.steps;
+    }
 
     ~apsm_pool();
     apsm_status fail(apsm_status st, const std::string& msg)
@@ -256,6 +299,10 @@ apsm_pool::~apsm_pool()
             if (e) cudaEventDestroy(e);
         if (l.done) cudaEventDestroy(l.done);
         if (l.desc_copied) cudaEventDestroy(l.desc_copied);
+        if (l.copy_stream) cudaStreamSynchronize(l.copy_stream);
+        if (l.ev_start) cudaEventDestroy(l.ev_start);
+        if (l.ev_inputs) cudaEventDestroy(l.ev_inputs);
+        if (l.copy_stream) cudaStreamDestroy(l.copy_stream);
         for (auto& e : l.tr)
             if (e) cudaEventDestroy(e);
         if (l.err_host) cudaFreeHost(l.err_host);
@@ -286,7 +333,7 @@ size_t resident_layout(uint32_t N, uint32_t capP, size_t off[6])
 struct TrainPlan {
     uint32_t job = 0; // index in the caller's list
     PoolDet* det = nullptr;
-    std::vector<TrainStep> steps;
+    const std::vector<TrainStep>* steps = nullptr; // the pool's cached schedule for (rows before, P)
     int final_hi = 0;
     uint32_t P = 0, usedP = 0, nP = 0, n_first = 0;
     long long kc_base = 0, n_kc = 0;
@@ -358,6 +405,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         if (st != APSM_OK) return st;
     }
     const uint32_t cap = 2 * cfg.dict_size;
+    if (schedules.size() > 16384) schedules.clear(); // bounded; no plan holds a pointer between batches
 
     // ---------- validate ----------
     std::vector<char> trained(dets.size(), 0);
@@ -399,14 +447,14 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             t.P = jobs[i].length;
             t.fresh = (jobs[i].flags & APSM_JOB_FRESH) != 0;
             const uint32_t used0 = t.fresh ? 0u : t.det->used;
-            t.steps = build_schedule(cfg, used0, t.P, cap, &t.final_hi);
+            t.steps = &schedule(used0, t.P, &t.final_hi);
             t.usedP = used0 / 2;
             t.nP = t.usedP + t.P;
-            t.n_first = t.steps.empty() ? t.nP : uint32_t(t.steps[0].hi - t.steps[0].wk) / 2;
+            t.n_first = t.steps->empty() ? t.nP : uint32_t((*t.steps)[0].hi - (*t.steps)[0].wk) / 2;
             t.kc_base = column_prefix(t.n_first, cm.qP, t.nP, t.det->capP);
             t.n_kc = column_prefix(t.nP, cm.qP, t.nP, t.det->capP) - t.kc_base;
-            if (!t.steps.empty() && t.usedP > 0 && !t.fresh) {
-                const int hiP0 = t.steps[0].hi / 2;
+            if (!t.steps->empty() && t.usedP > 0 && !t.fresh) {
+                const int hiP0 = (*t.steps)[0].hi / 2;
                 t.pro_w = hiP0 - int(t.n_first);
                 t.pro_n = int(t.nP - t.n_first);
                 t.pro_lo = std::max(0, hiP0 - int(t.det->capP));
@@ -419,7 +467,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         }
     // longest sweeps first (the persistent kernel takes jobs in this order)
     std::stable_sort(tp.begin(), tp.end(),
-                     [](const TrainPlan& x, const TrainPlan& y) { return x.steps.size() > y.steps.size(); });
+                     [](const TrainPlan& x, const TrainPlan& y) { return x.steps->size() > y.steps->size(); });
     // dictionary sizes after this batch's training, for the detection jobs
     std::vector<uint32_t> used_after(dets.size());
     for (size_t d = 0; d < dets.size(); ++d) used_after[d] = dets[d].used;
@@ -489,7 +537,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     const size_t off_gp = o; o = align_up(o + sizeof(int) * (nG + nGcls), 256);
     for (auto& t : tp) {
         t.off_steps = o;
-        o = align_up(o + sizeof(TrainStep) * t.steps.size(), 16);
+        o = align_up(o + sizeof(TrainStep) * t.steps->size(), 16);
     }
     std::map<uint32_t, size_t> perm_off;
     if (cfg.shuffle)
@@ -515,7 +563,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             }
     o = align_up(o, 256);
     const size_t dcnt_bytes = o - off_dcnt;
-    const size_t desc_only = o; // the descriptors alone
     if (host) { // staged host inputs travel with the descriptors
         for (auto& t : tp) {
             t.off_rx = o; o = align_up(o + sizeof(float2) * size_t(t.det->N) * t.P, 16);
@@ -528,6 +575,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         o = align_up(o, 256);
     }
     const size_t desc_bytes = o; // bytes of the one host-to-device copy
+    const size_t off_det_in = host && nD > 0 ? dp[0].off_rx : desc_bytes; // detection samples from here
     for (auto& t : tp) {
         const PoolDet& d = *t.det;
         t.off_Y = o; o = align_up(o + sizeof(float2) * size_t(t.nP) * d.Np, 256);
@@ -567,6 +615,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     o = align_up(o, 256);
     const size_t scratch_need = o;
 
+    const double t_plan = trace ? host_us() : 0.0;
     // ---------- memory ----------
     // Growth is geometric and never stalls the device: scratch comes from the pool's own
     // stream-ordered memory pool (the old block is released in stream order behind the lane's
@@ -608,6 +657,43 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     char* hst = static_cast<char*>(L.pinned);
     auto D = [&](size_t off) { return dev + off; };
 
+    // host inputs: copied straight from the caller's buffers when they are page-locked,
+    // else staged through the lane's pinned buffer (one copy together with the descriptors)
+    struct HostIn {
+        const void* src;
+        size_t off, bytes;
+        bool detect; // a detection job's samples
+    };
+    std::vector<HostIn> ins;
+    bool direct = false;
+    if (host) {
+        for (const auto& t : tp) {
+            const apsm_job& j = jobs[t.job];
+            ins.push_back({j.rx, t.off_rx, sizeof(float2) * size_t(t.det->N) * t.P, false});
+            ins.push_back({j.tx, t.off_tx, sizeof(float2) * t.P, false});
+        }
+        for (const auto& q : dp)
+            ins.push_back({jobs[q.job].rx, q.off_rx, sizeof(float2) * size_t(q.det->N) * q.S, true});
+        // small batches travel in the one descriptor upload even from page-locked buffers: a
+        // host memcpy of a few KB costs less than a copy command per input
+        size_t in_bytes = 0;
+        for (const auto& in : ins) in_bytes += in.bytes;
+        direct = !ins.empty() && in_bytes >= (size_t(256) << 10);
+        if (direct)
+            for (const auto& in : ins)
+                if (in.detect && !is_pinned(in.src)) {
+                    direct = false;
+                    break;
+                }
+        // staged: every input (no direct copies), or the training inputs of a direct batch --
+        // many small copies cost more per byte than helper threads' memcpy plus one upload
+        std::vector<Stager::Range> pieces;
+        pieces.reserve(ins.size());
+        for (const auto& in : ins)
+            if (!direct || !in.detect) pieces.push_back({hst + in.off, static_cast<const char*>(in.src), in.bytes});
+        stager.begin(pieces); // joined before the upload; the descriptors are written meanwhile
+    }
+
     // ---------- descriptors ----------
     auto* h_tj = reinterpret_cast<BatchTrainJob*>(hst + off_tj);
     auto* h_dj = reinterpret_cast<BatchDetectJob*>(hst + off_dj);
@@ -616,11 +702,12 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     auto* h_co = reinterpret_cast<BatchCopyJob*>(hst + off_co);
     size_t ipack = 0, icopy = 0;
     int max_len = 0, max_np = 1, max_cols = 0, max_n = 1, max_pairs_in = 0, max_pairs_out = 0;
+    int max_len_d = 0, max_n_d = 1; // packing of the tensor-core detection jobs' samples
     for (size_t k = 0; k < nT; ++k) {
         TrainPlan& t = tp[k];
         PoolDet& d = *t.det;
         const apsm_job& j = jobs[t.job];
-        std::memcpy(hst + t.off_steps, t.steps.data(), sizeof(TrainStep) * t.steps.size());
+        std::memcpy(hst + t.off_steps, t.steps->data(), sizeof(TrainStep) * t.steps->size());
         const float2* rx = host ? reinterpret_cast<const float2*>(D(t.off_rx)) : reinterpret_cast<const float2*>(j.rx);
         const float2* tx = host ? reinterpret_cast<const float2*>(D(t.off_tx)) : reinterpret_cast<const float2*>(j.tx);
         auto* Y = reinterpret_cast<float2*>(D(t.off_Y));
@@ -646,7 +733,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         tj.r = d.r;
         tj.Kc = reinterpret_cast<const float4*>(D(t.off_kc));
         tj.steps = reinterpret_cast<const TrainStep*>(D(t.off_steps));
-        tj.n_steps = int(t.steps.size());
+        tj.n_steps = int(t.steps->size());
         tj.nP = int(t.nP);
         tj.N = int(d.N);
         tj.Np = int(d.Np);
@@ -678,9 +765,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         auto* ns = q.gram ? reinterpret_cast<float*>(D(q.off_nrm)) : nullptr;
         if (q.gram) {
             h_pj[ipack++] = BatchPackJob{rx, nullptr, nullptr, Ys, ns, nullptr, nullptr, int(q.S), int(d.N), int(d.Np)};
-            max_len = std::max(max_len, int(q.S));
-            max_np = std::max(max_np, int(d.Np));
-            max_n = std::max(max_n, int(d.N));
+            max_len_d = std::max(max_len_d, int(q.S));
+            max_n_d = std::max(max_n_d, int(d.N));
         }
         float2* out = host ? reinterpret_cast<float2*>(D(q.off_est)) : reinterpret_cast<float2*>(j.est);
         const bool split = det_parts > 1 && !q.gram;
@@ -731,49 +817,32 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             k = k1;
         }
     }
-    (void)pack_train;
 
+    const double t_desc = trace ? host_us() : 0.0;
     // ---------- enqueue ----------
     cudaStream_t s = L.stream;
-    // host inputs: copied straight from the caller's buffers when they are page-locked,
-    // else staged through the lane's pinned buffer (one copy together with the descriptors)
-    struct HostIn {
-        const void* src;
-        size_t off, bytes;
-    };
-    std::vector<HostIn> ins;
-    bool direct = false;
-    if (host) {
-        for (const auto& t : tp) {
-            const apsm_job& j = jobs[t.job];
-            ins.push_back({j.rx, t.off_rx, sizeof(float2) * size_t(t.det->N) * t.P});
-            ins.push_back({j.tx, t.off_tx, sizeof(float2) * t.P});
-        }
-        for (const auto& q : dp) ins.push_back({jobs[q.job].rx, q.off_rx, sizeof(float2) * size_t(q.det->N) * q.S});
-        // small batches travel in the one descriptor upload even from page-locked buffers: a
-        // host memcpy of a few KB costs less than a copy command per input
-        size_t in_bytes = 0;
-        for (const auto& in : ins) in_bytes += in.bytes;
-        direct = !ins.empty() && in_bytes >= (size_t(256) << 10);
-        if (direct)
-            for (const auto& in : ins)
-                if (!is_pinned(in.src)) {
-                    direct = false;
-                    break;
-                }
-        if (!direct) {
-            std::vector<Stager::Range> pieces;
-            pieces.reserve(ins.size());
-            for (const auto& in : ins)
-                pieces.push_back({hst + in.off, static_cast<const char*>(in.src), in.bytes});
-            stager.copy(pieces);
-        }
-    }
     std::memset(hst + off_counter, 0, off_dcnt - off_counter + dcnt_bytes);
+    stager.wait();
+    const double t_stage = trace ? host_us() : 0.0;
     if (trace) POOL_CK(cudaEventRecord(L.tr[0], s));
-    POOL_CK(cudaMemcpyAsync(dev, hst, direct ? desc_only : desc_bytes, cudaMemcpyHostToDevice, s));
-    if (direct)
-        for (const auto& in : ins) POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, s));
+    // a batch that trains and detects from page-locked buffers copies the detection samples
+    // on the lane's copy stream while it trains: after the upload of the descriptors and
+    // training inputs (which would otherwise share the link with them and delay the
+    // training) and after the lane's earlier work (the scratch is free); the detections
+    // wait for them
+    const bool overlap = direct && nT > 0 && nD > 0;
+    POOL_CK(cudaMemcpyAsync(dev, hst, direct ? off_det_in : desc_bytes, cudaMemcpyHostToDevice, s));
+    if (direct && !overlap)
+        for (const auto& in : ins)
+            if (in.detect) POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, s));
+    if (overlap) {
+        POOL_CK(cudaEventRecord(L.ev_start, s));
+        POOL_CK(cudaStreamWaitEvent(L.copy_stream, L.ev_start, 0));
+        for (const auto& in : ins)
+            if (in.detect)
+                POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, L.copy_stream));
+        POOL_CK(cudaEventRecord(L.ev_inputs, L.copy_stream));
+    }
     POOL_CK(cudaEventRecord(L.desc_copied, s));
     L.have_train = timing && nT > 0;
     L.have_detect = timing && nD > 0;
@@ -793,8 +862,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_ci)), int(nCopyIn), max_pairs_in, max_np, s));
         L.launches += nCopyIn > 0 && max_pairs_in > 0;
     }
-    if (nPack > 0) {
-        POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)), int(nPack), max_len, max_n, s));
+    if (pack_train > 0) { // training samples (the detection jobs' are packed when they are needed)
+        POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)), int(pack_train), max_len, max_n, s));
         L.launches += max_len > 0;
     }
     if (trace) POOL_CK(cudaEventRecord(L.tr[2], s));
@@ -826,7 +895,13 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     }
     if (trace) POOL_CK(cudaEventRecord(L.tr[5], s));
     if (nD > 0) {
+        if (overlap) POOL_CK(cudaStreamWaitEvent(s, L.ev_inputs, 0));
         if (timing) POOL_CK(cudaEventRecord(L.ev[2], s));
+        if (nPack > pack_train) {
+            POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)) + pack_train,
+                                      int(nPack - pack_train), max_len_d, max_n_d, s));
+            L.launches += max_len_d > 0;
+        }
         const auto* d_dj = reinterpret_cast<const BatchDetectJob*>(D(off_dj));
         size_t k0 = 0;
         const size_t nC = nD - nG; // CUDA-core jobs come first
@@ -851,9 +926,11 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         }
         if (timing) POOL_CK(cudaEventRecord(L.ev[3], s));
         if (host && est_bytes > 0) {
-            bool out_direct = true;
+            // page-locked outputs of a few jobs: one copy each; of many jobs: one copy of all
+            // estimates, scattered by finish() (per-copy cost exceeds a host memcpy then)
+            bool out_direct = dp.size() <= kDirectOutJobs;
             for (const auto& q : dp)
-                if (!is_pinned(jobs[q.job].est)) {
+                if (out_direct && !is_pinned(jobs[q.job].est)) {
                     out_direct = false;
                     break;
                 }
@@ -878,6 +955,9 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         L.tr_nD = int(nD);
         L.t_run0 = t_run0;
         L.t_run1 = host_us();
+        L.t_mark[0] = t_plan - t_run0;
+        L.t_mark[1] = t_desc - t_run0;
+        L.t_mark[2] = t_stage - t_run0;
     }
     POOL_CK(cudaEventRecord(L.done, s));
     if (mode == APSM_RUN_HOST) return finish(lane_id);
@@ -891,7 +971,13 @@ apsm_status apsm_pool::finish(uint32_t lane_id)
     const double t0 = trace ? host_us() : 0.0;
     POOL_CK(cudaEventSynchronize(L.done));
     const double t1 = trace ? host_us() : 0.0;
-    for (const auto& c : L.pending) std::memcpy(c.dst, static_cast<char*>(L.pinned_out) + c.off, c.bytes);
+    {
+        std::vector<Stager::Range> pieces;
+        pieces.reserve(L.pending.size());
+        for (const auto& c : L.pending)
+            pieces.push_back({static_cast<char*>(c.dst), static_cast<const char*>(L.pinned_out) + c.off, c.bytes});
+        stager.copy(pieces);
+    }
     L.pending.clear();
     const apsm_status st = check_lane(lane_id);
     if (trace && L.traced) {
@@ -902,9 +988,9 @@ apsm_status apsm_pool::finish(uint32_t lane_id)
         for (int k = 0; k < 6; ++k)
             if (cudaEventElapsedTime(&g[k], L.tr[k], L.tr[k + 1]) != cudaSuccess) g[k] = -1e-3f;
         cudaGetLastError();
-        std::fprintf(trace, "%u %d %d %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f\n", lane_id, L.tr_nT, L.tr_nD,
-                     L.t_run1 - L.t_run0, t0 - L.t_run1, t1 - t0, host_us() - t1, 1e3 * g[0], 1e3 * g[1], 1e3 * g[2],
-                     1e3 * g[3], 1e3 * g[4], 1e3 * g[5]);
+        std::fprintf(trace, "%u %d %d %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f\n", lane_id,
+                     L.tr_nT, L.tr_nD, L.t_run1 - L.t_run0, t0 - L.t_run1, t1 - t0, host_us() - t1, 1e3 * g[0],
+                     1e3 * g[1], 1e3 * g[2], 1e3 * g[3], 1e3 * g[4], 1e3 * g[5], L.t_mark[0], L.t_mark[1], L.t_mark[2]);
         L.traced = false;
     }
     return st;
@@ -1015,8 +1101,12 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
         for (auto& e : l.ev)
             if (cudaEventCreate(&e) != cudaSuccess) return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         if (cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&l.desc_copied, cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&l.desc_copied, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&l.ev_start, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&l.ev_inputs, cudaEventDisableTiming) != cudaSuccess)
             return failp("cudaEventCreate failed", APSM_ERR_CUDA);
+        if (cudaStreamCreateWithFlags(&l.copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+            return failp("cudaStreamCreate failed", APSM_ERR_CUDA);
         for (auto& e : l.tr)
             if (cudaEventCreate(&e) != cudaSuccess) return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         if (cudaMallocHost(reinterpret_cast<void**>(&l.err_host), sizeof(int)) != cudaSuccess)
@@ -1029,7 +1119,8 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
         p->trace = std::fopen(path, "w");
         if (p->trace)
             std::fprintf(p->trace, "# lane n_train n_detect run_us gap_us fin_wait_us fin_rest_us gpu_inputs_us "
-                                   "gpu_pack_us gpu_kcol_us gpu_sweep_us gpu_copyout_us gpu_detect_us\n");
+                                   "gpu_pack_us gpu_kcol_us gpu_sweep_us gpu_copyout_us gpu_detect_us "
+                                   "run_planned_us run_described_us run_staged_us\n");
     }
     if (batch_sweep_occupancy(cm, &p->sweep_ctas) != cudaSuccess || p->sweep_ctas < 1)
         return failp("the training sweep does not fit an SM", APSM_ERR_UNSUPPORTED);
