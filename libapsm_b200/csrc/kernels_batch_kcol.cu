@@ -16,32 +16,70 @@ namespace {
 
 constexpr int kColGroup = kKcolGroup; // columns per block
 constexpr int kColRows = kKcolRows;   // column entries per block pass (= threads)
+constexpr int kPitch = kColRows + 1;  // float2 pitch of the feature-major pairs
+
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// float2 slots of the feature-major pair block, rounded so the columns after it are 16-byte aligned
+__host__ __device__ inline size_t pair_block_slots(int N) { return (size_t(N) * kPitch + 1) & ~size_t(1); }
 
 __global__ void __launch_bounds__(kColRows)
     batch_kcol_kernel(const BatchTrainJob* __restrict__ jobs, BatchCommon cm, int smem_n)
 {
-    const BatchTrainJob& jb = jobs[blockIdx.y];
-    const int nP = jb.nP, N = jb.N, Np = jb.Np, capP = jb.capP, qP = cm.qP;
-    const int n0 = jb.n_first + blockIdx.x * kColGroup;
+    // the job's fields in registers: the column stores below cannot alias them then
+    const BatchTrainJob& jg = jobs[blockIdx.y];
+    const int nP = jg.nP, N = jg.N, Np = jg.Np, capP = jg.capP, qP = cm.qP;
+    const int n_first = jg.n_first;
+    const int n0 = n_first + blockIdx.x * kColGroup;
     if (n0 >= nP || N > smem_n) return; // shared memory is sized for smem_n antennas
     const int nc = min(kColGroup, nP - n0);
-    const float ew = jb.ew, wG = cm.wG, wL = cm.wL;
+    const float2* __restrict__ Y = jg.Y;
+    const float* __restrict__ nrm = jg.nrm;
+    const float* __restrict__ a = jg.a;
+    float4* __restrict__ Kc = const_cast<float4*>(jg.Kc);
+    float2* __restrict__ pro = jg.pro;
+    const int pro_stride = jg.pro_stride;
+    // exp(ew x) = 2^(ew log2(e) x) on the SFU
+    const float ewl2 = jg.ew * 1.4426950408889634f, wG = cm.wG, wL = cm.wL;
     const int tid = threadIdx.x;
 
-    extern __shared__ float2 smk[];
-    constexpr int kPitch = kColRows + 1;
-    float2* sY = smk;                         // [N][kPitch] feature-major universe pairs
-    float2* sC = sY + size_t(N) * kPitch;     // [kColGroup][N] the group's columns
+    extern __shared__ __align__(16) float2 smk[];
+    float2* sY = smk;                          // [N][kPitch] feature-major universe pairs
+    float2* sC = sY + pair_block_slots(N);     // [N][kColGroup] the group's columns, feature-major
     float* snb = reinterpret_cast<float*>(sC + kColGroup * N); // [kColRows]
-    __shared__ float2 spro[kColRows / 32][kColGroup]; // prologue sums: warp partials
+    __shared__ float2 spro[kColRows / 32][kColGroup];          // prologue sums: warp partials
+    // per column: entry range [blo, bhi), store offset of entry b (off + b), old-pair range of its sums
+    __shared__ long long s_off[kColGroup];
+    __shared__ int s_blo[kColGroup], s_bhi[kColGroup], s_plo[kColGroup], s_phi[kColGroup];
 
+    if (tid < kColGroup) {
+        const int n = n0 + tid;
+        int blo = 0, bhi = 0, plo = 0, phi = 0;
+        long long off = 0;
+        if (tid < nc) {
+            blo = col_begin(n, capP);
+            bhi = col_end(n, qP, nP);
+            off = column_prefix(n, qP, nP, capP) - jg.kc_base - blo;
+            if (pro) pro_range(jg, n, &plo, &phi);
+        }
+        s_blo[tid] = blo;
+        s_bhi[tid] = bhi;
+        s_off[tid] = off;
+        s_plo[tid] = plo;
+        s_phi[tid] = phi;
+    }
     for (int idx = tid; idx < kColGroup * N; idx += kColRows) {
-        const int c = idx / N, k = idx % N;
-        sC[idx] = c < nc ? jb.Y[size_t(n0 + c) * Np + k] : make_float2(0.f, 0.f);
+        const int k = idx / kColGroup, c = idx % kColGroup;
+        sC[idx] = c < nc ? Y[size_t(n0 + c) * Np + k] : make_float2(0.f, 0.f);
     }
     float nn[kColGroup];
 #pragma unroll
-    for (int c = 0; c < kColGroup; ++c) nn[c] = c < nc ? jb.nrm[n0 + c] : 0.f;
+    for (int c = 0; c < kColGroup; ++c) nn[c] = c < nc ? nrm[n0 + c] : 0.f;
 
     const int b_lo = col_begin(n0, capP); // columns of the group start no earlier
     const int b_hi = col_end(n0 + nc - 1, qP, nP);
@@ -51,13 +89,12 @@ __global__ void __launch_bounds__(kColRows)
         const int nr = min(kColRows, b_hi - b0);
         for (int idx = tid; idx < nr * N; idx += kColRows) {
             const int r = idx / N, k = idx % N;
-            sY[k * kPitch + r] = jb.Y[size_t(b0 + r) * Np + k];
+            sY[k * kPitch + r] = Y[size_t(b0 + r) * Np + k];
         }
-        if (tid < nr) snb[tid] = jb.nrm[b0 + tid];
+        if (tid < nr) snb[tid] = nrm[b0 + tid];
         __syncthreads();
         // sums over the old pairs (pro_range) of every column, for calls that append
         const int pass = (b0 - b_lo) / kColRows;
-        const bool pro_any = jb.pro != nullptr;
         float2 pg[kColGroup];
 #pragma unroll
         for (int c = 0; c < kColGroup; ++c) pg[c] = make_float2(0.f, 0.f);
@@ -68,37 +105,36 @@ __global__ void __launch_bounds__(kColRows)
             for (int c = 0; c < kColGroup; ++c) re[c] = im[c] = 0.f;
             for (int k = 0; k < N; ++k) {
                 const float2 yb = sY[k * kPitch + tid];
+                const float4* c4 = reinterpret_cast<const float4*>(sC + k * kColGroup);
 #pragma unroll
-                for (int c = 0; c < kColGroup; ++c) {
-                    const float2 yc = sC[c * N + k];
-                    re[c] = fmaf(yb.x, yc.x, fmaf(yb.y, yc.y, re[c]));
-                    im[c] = fmaf(yb.x, yc.y, fmaf(-yb.y, yc.x, im[c]));
+                for (int h = 0; h < kColGroup / 2; ++h) {
+                    const float4 v = c4[h]; // columns 2h (x, y) and 2h + 1 (z, w)
+                    re[2 * h] = fmaf(yb.x, v.x, fmaf(yb.y, v.y, re[2 * h]));
+                    im[2 * h] = fmaf(yb.x, v.y, fmaf(-yb.y, v.x, im[2 * h]));
+                    re[2 * h + 1] = fmaf(yb.x, v.z, fmaf(yb.y, v.w, re[2 * h + 1]));
+                    im[2 * h + 1] = fmaf(yb.x, v.w, fmaf(-yb.y, v.z, im[2 * h + 1]));
                 }
             }
             const float nb = snb[tid];
 #pragma unroll
             for (int c = 0; c < kColGroup; ++c) {
                 if (c >= nc) break;
-                const int n = n0 + c;
-                if (b < col_begin(n, capP) || b >= col_end(n, qP, nP)) continue;
+                if (b < s_blo[c] || b >= s_bhi[c]) continue;
                 const float s = nb + nn[c];
-                const float A = wG * expf(ew * fmaxf(fmaf(-2.f, re[c], s), 0.f));
-                const float Bp = wG * expf(ew * fmaxf(fmaf(-2.f, im[c], s), 0.f));
-                const float Bm = wG * expf(ew * fmaxf(fmaf(2.f, im[c], s), 0.f));
-                const long long off = column_prefix(n, qP, nP, capP) - jb.kc_base + (b - col_begin(n, capP));
+                const float A = wG * ex2_approx(ewl2 * fmaxf(fmaf(-2.f, re[c], s), 0.f));
+                const float Bp = wG * ex2_approx(ewl2 * fmaxf(fmaf(-2.f, im[c], s), 0.f));
+                const float Bm = wG * ex2_approx(ewl2 * fmaxf(fmaf(2.f, im[c], s), 0.f));
                 const float4 kt = make_float4(fmaf(wL, re[c], A), fmaf(wL, im[c], Bp), fmaf(-wL, im[c], Bm), 0.f);
-                const_cast<float4*>(jb.Kc)[off] = kt;
-                int plo = 0, phi = 0;
-                if (pro_any) pro_range(jb, n, &plo, &phi);
-                if (b >= plo && b < phi) {
+                Kc[s_off[c] + b] = kt;
+                if (b >= s_plo[c] && b < s_phi[c]) {
                     // a_2b Kt(2b, .) + a_2b+1 Kt(2b+1, .) for the column pair's two rows
-                    const float2 ab = *reinterpret_cast<const float2*>(jb.a + 2 * b);
+                    const float2 ab = *reinterpret_cast<const float2*>(a + 2 * b);
                     pg[c].x = fmaf(ab.x, kt.x, fmaf(ab.y, kt.z, pg[c].x));
                     pg[c].y = fmaf(ab.x, kt.y, fmaf(ab.y, kt.x, pg[c].y));
                 }
             }
         }
-        if (pro_any) {
+        if (pro) {
             // this pass's sums: warp shuffles, then the warps in order
 #pragma unroll
             for (int c = 0; c < kColGroup; ++c)
@@ -118,7 +154,7 @@ __global__ void __launch_bounds__(kColRows)
                     v.x += spro[w][tid].x;
                     v.y += spro[w][tid].y;
                 }
-                jb.pro[size_t(n0 + tid - jb.n_first) * jb.pro_stride + pass] = v;
+                pro[size_t(n0 + tid - n_first) * pro_stride + pass] = v;
             }
         }
     }
@@ -133,8 +169,7 @@ cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, int n_jobs, int max_c
                               BatchCommon cm, cudaStream_t s)
 {
     if (n_jobs <= 0 || max_cols <= 0) return cudaSuccess;
-    const size_t smem = sizeof(float2) * (size_t(max_n) * (kColRows + 1) + size_t(kColGroup) * max_n) +
-                        sizeof(float) * kColRows;
+    const size_t smem = sizeof(float2) * (pair_block_slots(max_n) + size_t(kColGroup) * max_n) + sizeof(float) * kColRows;
     cudaError_t e = cudaFuncSetAttribute(batch_kcol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     dim3 grid((max_cols + kColGroup - 1) / kColGroup, n_jobs, row_split > 1 ? row_split : 1);
