@@ -835,14 +835,9 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     if (direct && !overlap)
         for (const auto& in : ins)
             if (in.detect) POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, s));
-    if (overlap) {
-        POOL_CK(cudaEventRecord(L.ev_start, s));
-        POOL_CK(cudaStreamWaitEvent(L.copy_stream, L.ev_start, 0));
-        for (const auto& in : ins)
-            if (in.detect)
-                POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, L.copy_stream));
-        POOL_CK(cudaEventRecord(L.ev_inputs, L.copy_stream));
-    }
+    // (the copy commands themselves are issued after the training launches: a host call per
+    // input would otherwise hold the training back)
+    if (overlap) POOL_CK(cudaEventRecord(L.ev_start, s));
     POOL_CK(cudaEventRecord(L.desc_copied, s));
     L.have_train = timing && nT > 0;
     L.have_detect = timing && nD > 0;
@@ -892,6 +887,13 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     } else if (trace) {
         POOL_CK(cudaEventRecord(L.tr[3], s));
         POOL_CK(cudaEventRecord(L.tr[4], s));
+    }
+    if (overlap) {
+        POOL_CK(cudaStreamWaitEvent(L.copy_stream, L.ev_start, 0));
+        for (const auto& in : ins)
+            if (in.detect)
+                POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, L.copy_stream));
+        POOL_CK(cudaEventRecord(L.ev_inputs, L.copy_stream));
     }
     if (trace) POOL_CK(cudaEventRecord(L.tr[5], s));
     if (nD > 0) {
