@@ -53,9 +53,10 @@ struct Lane {
     cudaEvent_t done = nullptr;                                // end of the last batch
     cudaEvent_t desc_copied = nullptr;                         // the pinned descriptors were consumed
     // detection inputs copied while the batch trains: a second stream, ordered after the
-    // lane's earlier work (ev_start) and joined before the detections (ev_inputs)
+    // lane's earlier work (ev_start) and joined before each detection segment (seg_ev)
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t ev_start = nullptr, ev_inputs = nullptr;
+    cudaEvent_t ev_start = nullptr;
+    std::vector<cudaEvent_t> seg_ev; // per detection segment: its samples arrived
     bool have_train = false, have_detect = false;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -301,7 +302,8 @@ apsm_pool::~apsm_pool()
         if (l.desc_copied) cudaEventDestroy(l.desc_copied);
         if (l.copy_stream) cudaStreamSynchronize(l.copy_stream);
         if (l.ev_start) cudaEventDestroy(l.ev_start);
-        if (l.ev_inputs) cudaEventDestroy(l.ev_inputs);
+        for (auto& e : l.seg_ev)
+            if (e) cudaEventDestroy(e);
         if (l.copy_stream) cudaStreamDestroy(l.copy_stream);
         for (auto& e : l.tr)
             if (e) cudaEventDestroy(e);
@@ -702,7 +704,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     auto* h_co = reinterpret_cast<BatchCopyJob*>(hst + off_co);
     size_t ipack = 0, icopy = 0;
     int max_len = 0, max_np = 1, max_cols = 0, max_n = 1, max_pairs_in = 0, max_pairs_out = 0;
-    int max_len_d = 0, max_n_d = 1; // packing of the tensor-core detection jobs' samples
     for (size_t k = 0; k < nT; ++k) {
         TrainPlan& t = tp[k];
         PoolDet& d = *t.det;
@@ -765,8 +766,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         auto* ns = q.gram ? reinterpret_cast<float*>(D(q.off_nrm)) : nullptr;
         if (q.gram) {
             h_pj[ipack++] = BatchPackJob{rx, nullptr, nullptr, Ys, ns, nullptr, nullptr, int(q.S), int(d.N), int(d.Np)};
-            max_len_d = std::max(max_len_d, int(q.S));
-            max_n_d = std::max(max_n_d, int(d.N));
         }
         float2* out = host ? reinterpret_cast<float2*>(D(q.off_est)) : reinterpret_cast<float2*>(j.est);
         const bool split = det_parts > 1 && !q.gram;
@@ -888,63 +887,90 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         POOL_CK(cudaEventRecord(L.tr[3], s));
         POOL_CK(cudaEventRecord(L.tr[4], s));
     }
-    if (overlap) {
-        POOL_CK(cudaStreamWaitEvent(L.copy_stream, L.ev_start, 0));
-        for (const auto& in : ins)
-            if (in.detect)
-                POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, L.copy_stream));
-        POOL_CK(cudaEventRecord(L.ev_inputs, L.copy_stream));
-    }
     if (trace) POOL_CK(cudaEventRecord(L.tr[5], s));
     if (nD > 0) {
-        if (overlap) POOL_CK(cudaStreamWaitEvent(s, L.ev_inputs, 0));
-        if (timing) POOL_CK(cudaEventRecord(L.ev[2], s));
-        if (nPack > pack_train) {
-            POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)) + pack_train,
-                                      int(nPack - pack_train), max_len_d, max_n_d, s));
-            L.launches += max_len_d > 0;
-        }
-        const auto* d_dj = reinterpret_cast<const BatchDetectJob*>(D(off_dj));
-        size_t k0 = 0;
+        // detection in segments of one launch shape (the CUDA-core classes, then the tensor-core
+        // classes); when the samples travel on the copy stream each segment waits for its own
+        // only, and each segment's estimates are copied back behind it
+        struct Seg {
+            size_t k0, k1;
+            int g; // index into gseg; -1 for a CUDA-core class
+        };
+        std::vector<Seg> segs;
         const size_t nC = nD - nG; // CUDA-core jobs come first
-        while (k0 < nC) {
+        for (size_t k0 = 0; k0 < nC;) {
             size_t k1 = k0;
-            int tiles = 0;
-            while (k1 < nC && dp[k1].cls == dp[k0].cls) {
-                tiles = std::max(tiles, int((dp[k1].S + batch_detect_tile() - 1) / batch_detect_tile()));
-                ++k1;
-            }
-            POOL_CK(launch_batch_detect(d_dj + k0, int(k1 - k0), tiles, det_parts, dp[k0].cls, cfg.wL, cfg.wG, s));
-            L.launches += tiles > 0;
+            while (k1 < nC && dp[k1].cls == dp[k0].cls) ++k1;
+            segs.push_back({k0, k1, -1});
             k0 = k1;
         }
-        const auto* d_gj = reinterpret_cast<const BatchGramJob*>(D(off_gj));
-        const int* d_gp = reinterpret_cast<const int*>(D(off_gp));
-        for (const auto& g : gseg) {
-            const size_t base = size_t(g[0]) - nC;
-            POOL_CK(launch_batch_gram(gram_mode, d_gj + base, g[1] - g[0], g[4], g[5], d_gp + g[2], g[3], dp[g[0]].cls, cfg.wL,
-                                      cfg.wG, d_err, s));
-            L.launches += (g[4] > 0) + (g[5] > 0) + (g[3] > 0);
-        }
-        if (timing) POOL_CK(cudaEventRecord(L.ev[3], s));
-        if (host && est_bytes > 0) {
-            // page-locked outputs of a few jobs: one copy each; of many jobs: one copy of all
-            // estimates, scattered by finish() (per-copy cost exceeds a host memcpy then)
-            bool out_direct = dp.size() <= kDirectOutJobs;
-            for (const auto& q : dp)
-                if (out_direct && !is_pinned(jobs[q.job].est)) {
-                    out_direct = false;
-                    break;
+        for (size_t g = 0; g < gseg.size(); ++g) segs.push_back({size_t(gseg[g][0]), size_t(gseg[g][1]), int(g)});
+        if (overlap) {
+            while (L.seg_ev.size() < segs.size()) {
+                cudaEvent_t e = nullptr;
+                POOL_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                L.seg_ev.push_back(e);
+            }
+            POOL_CK(cudaStreamWaitEvent(L.copy_stream, L.ev_start, 0));
+            for (size_t i = 0; i < segs.size(); ++i) {
+                for (size_t k = segs[i].k0; k < segs[i].k1; ++k) {
+                    const DetectPlan& q = dp[k];
+                    POOL_CK(cudaMemcpyAsync(dev + q.off_rx, jobs[q.job].rx, sizeof(float2) * size_t(q.det->N) * q.S,
+                                            cudaMemcpyHostToDevice, L.copy_stream));
                 }
-            if (out_direct) {
-                for (const auto& q : dp)
-                    POOL_CK(cudaMemcpyAsync(jobs[q.job].est, D(q.off_est), sizeof(float2) * q.S, cudaMemcpyDeviceToHost, s));
-            } else {
-                POOL_CK(cudaMemcpyAsync(L.pinned_out, D(est_begin), est_bytes, cudaMemcpyDeviceToHost, s));
-                for (const auto& q : dp)
-                    L.pending.push_back({jobs[q.job].est, q.off_est - est_begin, sizeof(float2) * q.S});
+                POOL_CK(cudaEventRecord(L.seg_ev[i], L.copy_stream));
             }
         }
+        // page-locked outputs of a few jobs: one copy each; of many jobs: one copy per segment,
+        // scattered by finish() (per-copy cost exceeds a host memcpy then)
+        const bool est_out = host && est_bytes > 0;
+        bool out_direct = est_out && dp.size() <= kDirectOutJobs;
+        for (const auto& q : dp)
+            if (out_direct && !is_pinned(jobs[q.job].est)) {
+                out_direct = false;
+                break;
+            }
+        if (timing) POOL_CK(cudaEventRecord(L.ev[2], s));
+        const auto* d_dj = reinterpret_cast<const BatchDetectJob*>(D(off_dj));
+        const auto* d_gj = reinterpret_cast<const BatchGramJob*>(D(off_gj));
+        const int* d_gp = reinterpret_cast<const int*>(D(off_gp));
+        const auto* d_pj = reinterpret_cast<const BatchPackJob*>(D(off_pj));
+        for (size_t i = 0; i < segs.size(); ++i) {
+            const Seg& sg = segs[i];
+            if (overlap) POOL_CK(cudaStreamWaitEvent(s, L.seg_ev[i], 0));
+            if (sg.g < 0) {
+                int tiles = 0;
+                for (size_t k = sg.k0; k < sg.k1; ++k)
+                    tiles = std::max(tiles, int((dp[k].S + batch_detect_tile() - 1) / batch_detect_tile()));
+                POOL_CK(launch_batch_detect(d_dj + sg.k0, int(sg.k1 - sg.k0), tiles, det_parts, dp[sg.k0].cls, cfg.wL,
+                                            cfg.wG, s));
+                L.launches += tiles > 0;
+            } else {
+                // the class's samples packed first (one pack job per tensor-core job, after the training ones)
+                int ml = 0, mn = 1;
+                for (size_t k = sg.k0; k < sg.k1; ++k) {
+                    ml = std::max(ml, int(dp[k].S));
+                    mn = std::max(mn, int(dp[k].det->N));
+                }
+                POOL_CK(launch_batch_pack(d_pj + pack_train + (sg.k0 - nC), int(sg.k1 - sg.k0), ml, mn, s));
+                const auto& g = gseg[size_t(sg.g)];
+                POOL_CK(launch_batch_gram(gram_mode, d_gj + (sg.k0 - nC), g[1] - g[0], g[4], g[5], d_gp + g[2], g[3],
+                                          dp[sg.k0].cls, cfg.wL, cfg.wG, d_err, s));
+                L.launches += (ml > 0) + (g[4] > 0) + (g[5] > 0) + (g[3] > 0);
+            }
+            if (out_direct) {
+                for (size_t k = sg.k0; k < sg.k1; ++k)
+                    POOL_CK(cudaMemcpyAsync(jobs[dp[k].job].est, D(dp[k].off_est), sizeof(float2) * dp[k].S,
+                                            cudaMemcpyDeviceToHost, s));
+            } else if (est_out) {
+                const size_t lo = dp[sg.k0].off_est, hi = dp[sg.k1 - 1].off_est + sizeof(float2) * dp[sg.k1 - 1].S;
+                POOL_CK(cudaMemcpyAsync(static_cast<char*>(L.pinned_out) + (lo - est_begin), D(lo), hi - lo,
+                                        cudaMemcpyDeviceToHost, s));
+            }
+        }
+        if (est_out && !out_direct)
+            for (const auto& q : dp) L.pending.push_back({jobs[q.job].est, q.off_est - est_begin, sizeof(float2) * q.S});
+        if (timing) POOL_CK(cudaEventRecord(L.ev[3], s));
     }
     // the error flag of kernels with bounded waits (tensor-core detection) travels back with the
     // batch: finish() reads it without a synchronous copy
@@ -1104,8 +1130,7 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
             if (cudaEventCreate(&e) != cudaSuccess) return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         if (cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&l.desc_copied, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&l.ev_start, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&l.ev_inputs, cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&l.ev_start, cudaEventDisableTiming) != cudaSuccess)
             return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         if (cudaStreamCreateWithFlags(&l.copy_stream, cudaStreamNonBlocking) != cudaSuccess)
             return failp("cudaStreamCreate failed", APSM_ERR_CUDA);

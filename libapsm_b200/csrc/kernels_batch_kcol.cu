@@ -16,7 +16,6 @@ namespace {
 
 constexpr int kColGroup = kKcolGroup; // columns per block
 constexpr int kColRows = kKcolRows;   // column entries per block pass (= threads)
-constexpr int kPitch = kColRows + 1;  // float2 pitch of the feature-major pairs
 
 __device__ __forceinline__ float ex2_approx(float x)
 {
@@ -25,18 +24,19 @@ __device__ __forceinline__ float ex2_approx(float x)
     return y;
 }
 
-// float2 slots of the feature-major pair block, rounded so the columns after it are 16-byte aligned
-__host__ __device__ inline size_t pair_block_slots(int N) { return (size_t(N) * kPitch + 1) & ~size_t(1); }
-
+// Block: kColGroup columns (the group's pairs y_n and norms in shared memory,
+// read as broadcasts) against passes of kColRows rows, one row per thread held
+// in registers (NMAX >= N antennas of every job of the launch).
+template <int NMAX>
 __global__ void __launch_bounds__(kColRows)
-    batch_kcol_kernel(const BatchTrainJob* __restrict__ jobs, BatchCommon cm, int smem_n)
+    batch_kcol_kernel(const BatchTrainJob* __restrict__ jobs, BatchCommon cm)
 {
     // the job's fields in registers: the column stores below cannot alias them then
     const BatchTrainJob& jg = jobs[blockIdx.y];
     const int nP = jg.nP, N = jg.N, Np = jg.Np, capP = jg.capP, qP = cm.qP;
     const int n_first = jg.n_first;
     const int n0 = n_first + blockIdx.x * kColGroup;
-    if (n0 >= nP || N > smem_n) return; // shared memory is sized for smem_n antennas
+    if (n0 >= nP || N > NMAX) return;
     const int nc = min(kColGroup, nP - n0);
     const float2* __restrict__ Y = jg.Y;
     const float* __restrict__ nrm = jg.nrm;
@@ -48,11 +48,8 @@ __global__ void __launch_bounds__(kColRows)
     const float ewl2 = jg.ew * 1.4426950408889634f, wG = cm.wG, wL = cm.wL;
     const int tid = threadIdx.x;
 
-    extern __shared__ __align__(16) float2 smk[];
-    float2* sY = smk;                          // [N][kPitch] feature-major universe pairs
-    float2* sC = sY + pair_block_slots(N);     // [N][kColGroup] the group's columns, feature-major
-    float* snb = reinterpret_cast<float*>(sC + kColGroup * N); // [kColRows]
-    __shared__ float2 spro[kColRows / 32][kColGroup];          // prologue sums: warp partials
+    __shared__ __align__(16) float2 sC[NMAX][kColGroup]; // the group's columns, feature-major
+    __shared__ float2 spro[kColRows / 32][kColGroup];      // prologue sums: warp partials
     // per column: entry range [blo, bhi), store offset of entry b (off + b), old-pair range of its sums
     __shared__ long long s_off[kColGroup];
     __shared__ int s_blo[kColGroup], s_bhi[kColGroup], s_plo[kColGroup], s_phi[kColGroup];
@@ -75,55 +72,59 @@ __global__ void __launch_bounds__(kColRows)
     }
     for (int idx = tid; idx < kColGroup * N; idx += kColRows) {
         const int k = idx / kColGroup, c = idx % kColGroup;
-        sC[idx] = c < nc ? Y[size_t(n0 + c) * Np + k] : make_float2(0.f, 0.f);
+        sC[k][c] = c < nc ? Y[size_t(n0 + c) * Np + k] : make_float2(0.f, 0.f);
     }
     float nn[kColGroup];
 #pragma unroll
     for (int c = 0; c < kColGroup; ++c) nn[c] = c < nc ? nrm[n0 + c] : 0.f;
+    __syncthreads();
 
     const int b_lo = col_begin(n0, capP); // columns of the group start no earlier
     const int b_hi = col_end(n0 + nc - 1, qP, nP);
     // grid.z blocks share a column group, each taking every gridDim.z-th pass of rows
     for (int b0 = b_lo + int(blockIdx.z) * kColRows; b0 < b_hi; b0 += int(gridDim.z) * kColRows) {
-        __syncthreads();
-        const int nr = min(kColRows, b_hi - b0);
-        for (int idx = tid; idx < nr * N; idx += kColRows) {
-            const int r = idx / N, k = idx % N;
-            sY[k * kPitch + r] = Y[size_t(b0 + r) * Np + k];
-        }
-        if (tid < nr) snb[tid] = nrm[b0 + tid];
-        __syncthreads();
         // sums over the old pairs (pro_range) of every column, for calls that append
         const int pass = (b0 - b_lo) / kColRows;
         float2 pg[kColGroup];
 #pragma unroll
         for (int c = 0; c < kColGroup; ++c) pg[c] = make_float2(0.f, 0.f);
-        if (tid < nr) {
-            const int b = b0 + tid;
+        const int b = b0 + tid;
+        if (b < b_hi) {
+            // this thread's row (rows are 16-byte aligned: Np is even)
+            float2 yb[NMAX];
+            const float4* row = reinterpret_cast<const float4*>(Y + size_t(b) * Np);
+#pragma unroll
+            for (int j = 0; j < NMAX / 2; ++j) {
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (2 * j < N) v = __ldg(row + j);
+                yb[2 * j] = make_float2(v.x, v.y);
+                yb[2 * j + 1] = make_float2(v.z, v.w);
+            }
+            const float nb = __ldg(nrm + b);
             float re[kColGroup], im[kColGroup];
 #pragma unroll
             for (int c = 0; c < kColGroup; ++c) re[c] = im[c] = 0.f;
-            for (int k = 0; k < N; ++k) {
-                const float2 yb = sY[k * kPitch + tid];
-                const float4* c4 = reinterpret_cast<const float4*>(sC + k * kColGroup);
+#pragma unroll
+            for (int k = 0; k < NMAX; ++k) {
+                if (k >= N) break;
+                const float4* c4 = reinterpret_cast<const float4*>(&sC[k][0]);
 #pragma unroll
                 for (int h = 0; h < kColGroup / 2; ++h) {
                     const float4 v = c4[h]; // columns 2h (x, y) and 2h + 1 (z, w)
-                    re[2 * h] = fmaf(yb.x, v.x, fmaf(yb.y, v.y, re[2 * h]));
-                    im[2 * h] = fmaf(yb.x, v.y, fmaf(-yb.y, v.x, im[2 * h]));
-                    re[2 * h + 1] = fmaf(yb.x, v.z, fmaf(yb.y, v.w, re[2 * h + 1]));
-                    im[2 * h + 1] = fmaf(yb.x, v.w, fmaf(-yb.y, v.z, im[2 * h + 1]));
+                    re[2 * h] = fmaf(yb[k].x, v.x, fmaf(yb[k].y, v.y, re[2 * h]));
+                    im[2 * h] = fmaf(yb[k].x, v.y, fmaf(-yb[k].y, v.x, im[2 * h]));
+                    re[2 * h + 1] = fmaf(yb[k].x, v.z, fmaf(yb[k].y, v.w, re[2 * h + 1]));
+                    im[2 * h + 1] = fmaf(yb[k].x, v.w, fmaf(-yb[k].y, v.z, im[2 * h + 1]));
                 }
             }
-            const float nb = snb[tid];
 #pragma unroll
             for (int c = 0; c < kColGroup; ++c) {
                 if (c >= nc) break;
                 if (b < s_blo[c] || b >= s_bhi[c]) continue;
-                const float s = nb + nn[c];
-                const float A = wG * ex2_approx(ewl2 * fmaxf(fmaf(-2.f, re[c], s), 0.f));
-                const float Bp = wG * ex2_approx(ewl2 * fmaxf(fmaf(-2.f, im[c], s), 0.f));
-                const float Bm = wG * ex2_approx(ewl2 * fmaxf(fmaf(2.f, im[c], s), 0.f));
+                const float sn = nb + nn[c];
+                const float A = wG * ex2_approx(ewl2 * fmaxf(fmaf(-2.f, re[c], sn), 0.f));
+                const float Bp = wG * ex2_approx(ewl2 * fmaxf(fmaf(-2.f, im[c], sn), 0.f));
+                const float Bm = wG * ex2_approx(ewl2 * fmaxf(fmaf(2.f, im[c], sn), 0.f));
                 const float4 kt = make_float4(fmaf(wL, re[c], A), fmaf(wL, im[c], Bp), fmaf(-wL, im[c], Bm), 0.f);
                 Kc[s_off[c] + b] = kt;
                 if (b >= s_plo[c] && b < s_phi[c]) {
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(kColRows)
                     pg[c].x += __shfl_xor_sync(0xffffffffu, pg[c].x, o);
                     pg[c].y += __shfl_xor_sync(0xffffffffu, pg[c].y, o);
                 }
+            __syncthreads(); // the previous pass's partials were read
             if ((tid & 31) == 0)
 #pragma unroll
                 for (int c = 0; c < kColGroup; ++c) spro[tid >> 5][c] = pg[c];
@@ -169,11 +171,12 @@ cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, int n_jobs, int max_c
                               BatchCommon cm, cudaStream_t s)
 {
     if (n_jobs <= 0 || max_cols <= 0) return cudaSuccess;
-    const size_t smem = sizeof(float2) * (pair_block_slots(max_n) + size_t(kColGroup) * max_n) + sizeof(float) * kColRows;
-    cudaError_t e = cudaFuncSetAttribute(batch_kcol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
     dim3 grid((max_cols + kColGroup - 1) / kColGroup, n_jobs, row_split > 1 ? row_split : 1);
-    batch_kcol_kernel<<<grid, kColRows, smem, s>>>(d_jobs, cm, max_n);
+    if (max_n <= 8) batch_kcol_kernel<8><<<grid, kColRows, 0, s>>>(d_jobs, cm);
+    else if (max_n <= 16) batch_kcol_kernel<16><<<grid, kColRows, 0, s>>>(d_jobs, cm);
+    else if (max_n <= 32) batch_kcol_kernel<32><<<grid, kColRows, 0, s>>>(d_jobs, cm);
+    else if (max_n <= 64) batch_kcol_kernel<64><<<grid, kColRows, 0, s>>>(d_jobs, cm);
+    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
