@@ -212,6 +212,7 @@ private:
 };
 
 constexpr size_t kDirectOutJobs = 16; // detection jobs whose estimates are copied to the caller one by one
+constexpr size_t kArenaJobs = 32;     // training jobs from which a batch reads its step lists from the arena
 
 int detect_class(uint32_t N)
 {
@@ -243,9 +244,10 @@ struct apsm_pool {
     struct Schedule {
         std::vector<TrainStep> steps;
         int final_hi = 0;
+        long long dev = -1; // offset of its copy in sched_arena (-1: none)
     };
     std::map<std::pair<uint32_t, uint32_t>, Schedule> schedules;
-    const std::vector<TrainStep>& schedule(uint32_t used_before, uint32_t P, int* final_hi)
+    Schedule& schedule(uint32_t used_before, uint32_t P)
     {
         auto it = schedules.find({used_before, P});
         if (it == schedules.end()) {
@@ -253,9 +255,15 @@ struct apsm_pool {
             sc.steps = build_schedule(cfg, used_before, P, 2 * cfg.dict_size, &sc.final_hi);
             it = schedules.emplace(std::make_pair(used_before, P), std::move(sc)).first;
         }
-        *final_hi = it->second.final_hi;
-        return it->second.steps;
+        return it->second;
     }
+    // Device copies of the schedules for batches of many training jobs, so such a batch
+    // uploads (and stages) no step lists once their shapes recur: one arena, each schedule
+    // uploaded (synchronously) the first time a large batch uses it; reset, with every lane
+    // idle, when full.  Small batches carry their few steps in the descriptor upload.
+    DevBuf<TrainStep> sched_arena;
+    size_t sched_used = 0;
+    cudaStream_t sched_stream = nullptr;
 
     ~apsm_pool();
     apsm_status fail(apsm_status st, const std::string& msg)
@@ -271,7 +279,7 @@ struct apsm_pool {
     }
     uint64_t in_use() const
     {
-        uint64_t s = resident;
+        uint64_t s = resident + sizeof(TrainStep) * sched_arena.n;
         for (const auto& l : lanes) s += l.scratch_bytes;
         return s;
     }
@@ -310,6 +318,10 @@ apsm_pool::~apsm_pool()
         if (l.err_host) cudaFreeHost(l.err_host);
         if (l.stream) cudaStreamDestroy(l.stream);
     }
+    if (sched_stream) {
+        cudaStreamSynchronize(sched_stream);
+        cudaStreamDestroy(sched_stream);
+    }
     for (auto& d : dets)
         if (d.mem) cudaFree(d.mem);
     if (mempool) cudaMemPoolDestroy(mempool);
@@ -336,6 +348,7 @@ struct TrainPlan {
     uint32_t job = 0; // index in the caller's list
     PoolDet* det = nullptr;
     const std::vector<TrainStep>* steps = nullptr; // the pool's cached schedule for (rows before, P)
+    long long* steps_dev = nullptr; // its offset in the pool's device schedule arena (-1: not there)
     int final_hi = 0;
     uint32_t P = 0, usedP = 0, nP = 0, n_first = 0;
     long long kc_base = 0, n_kc = 0;
@@ -449,7 +462,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             t.P = jobs[i].length;
             t.fresh = (jobs[i].flags & APSM_JOB_FRESH) != 0;
             const uint32_t used0 = t.fresh ? 0u : t.det->used;
-            t.steps = &schedule(used0, t.P, &t.final_hi);
+            Schedule& sc = schedule(used0, t.P);
+            t.steps = &sc.steps;
+            t.steps_dev = &sc.dev;
+            t.final_hi = sc.final_hi;
             t.usedP = used0 / 2;
             t.nP = t.usedP + t.P;
             t.n_first = t.steps->empty() ? t.nP : uint32_t((*t.steps)[0].hi - (*t.steps)[0].wk) / 2;
@@ -467,6 +483,39 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             t.lo_new = fhP - t.usedP_new;
             tp.push_back(std::move(t));
         }
+    // step lists of a large batch from the device arena (new ones uploaded now)
+    const bool arena = tp.size() >= kArenaJobs;
+    if (arena) {
+        size_t fresh_steps = 0, all_steps = 0;
+        for (const auto& t : tp) {
+            all_steps += t.steps->size();
+            if (*t.steps_dev < 0) fresh_steps += t.steps->size();
+        }
+        if (sched_used + fresh_steps > sched_arena.n) {
+            // full: every lane idle, then start over (and grow to hold at least this batch)
+            for (auto& l : lanes) {
+                POOL_CK(cudaStreamSynchronize(l.stream));
+                POOL_CK(cudaStreamSynchronize(l.copy_stream));
+            }
+            for (auto& kv : schedules) kv.second.dev = -1;
+            sched_used = 0;
+            if (all_steps > sched_arena.n) {
+                const size_t want = std::max(all_steps + all_steps / 2, size_t(1) << 20);
+                const uint64_t others = in_use() - sizeof(TrainStep) * sched_arena.n;
+                if (budget && others + sizeof(TrainStep) * want > budget)
+                    return fail(APSM_ERR_OUT_OF_MEMORY, "the batch's training schedules exceed the HBM budget");
+                POOL_CK(sched_arena.ensure(want));
+            }
+        }
+        for (auto& t : tp)
+            if (*t.steps_dev < 0) {
+                *t.steps_dev = (long long)sched_used;
+                POOL_CK(cudaMemcpyAsync(sched_arena.p + sched_used, t.steps->data(), sizeof(TrainStep) * t.steps->size(),
+                                        cudaMemcpyHostToDevice, sched_stream));
+                sched_used += t.steps->size();
+            }
+        POOL_CK(cudaStreamSynchronize(sched_stream)); // in place before any lane's later batch reads it
+    }
     // longest sweeps first (the persistent kernel takes jobs in this order)
     std::stable_sort(tp.begin(), tp.end(),
                      [](const TrainPlan& x, const TrainPlan& y) { return x.steps->size() > y.steps->size(); });
@@ -537,10 +586,11 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     const size_t off_co = o; o = align_up(o + sizeof(BatchCopyJob) * nT, 256);
     const size_t off_gj = o; o = align_up(o + sizeof(BatchGramJob) * nG, 256);
     const size_t off_gp = o; o = align_up(o + sizeof(int) * (nG + nGcls), 256);
-    for (auto& t : tp) {
-        t.off_steps = o;
-        o = align_up(o + sizeof(TrainStep) * t.steps->size(), 16);
-    }
+    if (!arena)
+        for (auto& t : tp) {
+            t.off_steps = o;
+            o = align_up(o + sizeof(TrainStep) * t.steps->size(), 16);
+        }
     std::map<uint32_t, size_t> perm_off;
     if (cfg.shuffle)
         for (auto& t : tp) {
@@ -708,7 +758,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         TrainPlan& t = tp[k];
         PoolDet& d = *t.det;
         const apsm_job& j = jobs[t.job];
-        std::memcpy(hst + t.off_steps, t.steps->data(), sizeof(TrainStep) * t.steps->size());
+        if (!arena) std::memcpy(hst + t.off_steps, t.steps->data(), sizeof(TrainStep) * t.steps->size());
         const float2* rx = host ? reinterpret_cast<const float2*>(D(t.off_rx)) : reinterpret_cast<const float2*>(j.rx);
         const float2* tx = host ? reinterpret_cast<const float2*>(D(t.off_tx)) : reinterpret_cast<const float2*>(j.tx);
         auto* Y = reinterpret_cast<float2*>(D(t.off_Y));
@@ -733,7 +783,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         tj.w = d.w;
         tj.r = d.r;
         tj.Kc = reinterpret_cast<const float4*>(D(t.off_kc));
-        tj.steps = reinterpret_cast<const TrainStep*>(D(t.off_steps));
+        tj.steps = arena ? sched_arena.p + *t.steps_dev : reinterpret_cast<const TrainStep*>(D(t.off_steps));
         tj.n_steps = int(t.steps->size());
         tj.nP = int(t.nP);
         tj.N = int(d.N);
@@ -1149,6 +1199,8 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
                                    "gpu_pack_us gpu_kcol_us gpu_sweep_us gpu_copyout_us gpu_detect_us "
                                    "run_planned_us run_described_us run_staged_us\n");
     }
+    if (cudaStreamCreateWithFlags(&p->sched_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return failp("cudaStreamCreate failed", APSM_ERR_CUDA);
     if (batch_sweep_occupancy(cm, &p->sweep_ctas) != cudaSuccess || p->sweep_ctas < 1)
         return failp("the training sweep does not fit an SM", APSM_ERR_UNSUPPORTED);
     *out = p;
