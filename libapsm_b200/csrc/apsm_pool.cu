@@ -179,7 +179,8 @@ private:
     void start()
     {
         if (!th_.empty()) return;
-        const unsigned n = std::min(7u, std::max(1u, std::thread::hardware_concurrency() / 2));
+        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned n = std::min(15u, std::max(1u, hw > 1 ? hw - 1 : 1u));
         for (unsigned k = 0; k < n; ++k)
             th_.emplace_back([this] {
                 uint64_t seen = 0;
