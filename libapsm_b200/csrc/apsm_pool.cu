@@ -145,15 +145,19 @@ public:
         for (const auto& r : pieces)
             for (size_t o = 0; o < r.bytes; o += kStageGrain)
                 work_own_.push_back({r.dst + o, r.src + o, std::min(kStageGrain, r.bytes - o)});
+        // one helper per kPiecesPerHelper pieces at most: a request-sized batch wakes a few
+        // helpers, not every core (which would preempt the threads serving requests)
+        const unsigned want = unsigned(std::min(th_.size(), work_own_.size() / kPiecesPerHelper));
         {
             std::lock_guard<std::mutex> g(mu_);
             work_ = &work_own_;
             next_.store(0);
-            busy_ = unsigned(th_.size());
+            busy_ = want;
+            want_ = want;
             ++gen_;
         }
         active_ = true;
-        cv_.notify_all();
+        if (want > 0) cv_.notify_all();
     }
 
     void wait()
@@ -169,6 +173,7 @@ public:
 private:
     static constexpr size_t kStageSplit = size_t(1) << 20;
     static constexpr size_t kStageGrain = size_t(256) << 10;
+    static constexpr size_t kPiecesPerHelper = 8;
 
     void drain(std::vector<Range>& work)
     {
@@ -182,13 +187,13 @@ private:
         const unsigned hw = std::thread::hardware_concurrency();
         const unsigned n = std::min(15u, std::max(1u, hw > 1 ? hw - 1 : 1u));
         for (unsigned k = 0; k < n; ++k)
-            th_.emplace_back([this] {
+            th_.emplace_back([this, k] {
                 uint64_t seen = 0;
                 for (;;) {
                     std::vector<Range>* w;
                     {
                         std::unique_lock<std::mutex> lk(mu_);
-                        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                        cv_.wait(lk, [&] { return stop_ || (gen_ != seen && k < want_); });
                         if (stop_) return;
                         seen = gen_;
                         w = work_;
@@ -208,6 +213,7 @@ private:
     std::vector<Range>* work_ = nullptr;
     std::atomic<size_t> next_{0};
     unsigned busy_ = 0;
+    unsigned want_ = 0; // helpers taking part in the current copies
     uint64_t gen_ = 0;
     bool stop_ = false;
 };
