@@ -35,7 +35,7 @@ constexpr int kChunkPairs = 64;  // dictionary pairs per chunk
 constexpr int kChunkN = 128;     // accumulator columns per chunk (UMMA N)
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = (kEpiWarps + 2) * 32;
-constexpr int kBx = 2 * kChunkPairs + kChunkPairs; // per chunk: a*wG (128, column order) then pair norms (64)
+constexpr int kBx = 2 * kChunkPairs + kChunkPairs; // per chunk: a*wG (128, column order) then ew log2(e) * pair norms (64)
 
 // bytes of one operand tile of R rows at K extent Kp (hi [+ lo])
 template <int MODE> __host__ __device__ constexpr size_t tile_bytes(int R, int Kp)
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJ
             v = b < jb.Mp ? jb.a[2 * b + (i & 1)] * wG : 0.f;
         } else {
             const int b = c * kChunkPairs + (i - 2 * kChunkPairs);
-            v = b < jb.Mp ? jb.nrm_d[b] : 0.f;
+            v = b < jb.Mp ? jb.ew2 * jb.nrm_d[b] : 0.f; // norms pre-scaled by ew log2(e)
         }
         bx[i] = v;
     }
@@ -234,7 +234,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int q = warp & 3, h = warp >> 2;
         const int row = tile * kTileM + q * 32 + lane;
         const float xn = row < jb.S ? jb.nrm_s[row] : 0.f;
-        const float ew2 = jb.ew2;
+        // exponents in base 2: ew log2(e) (|x|^2 + |y|^2 - 2 r) = exn + eyn + m2 r, the pair norms
+        // pre-scaled in the chunk data; ew <= 0, so clamping the distance at 0 is clamping the
+        // exponent at 0
+        const float exn = jb.ew2 * xn, m2 = -2.f * jb.ew2;
         float f0 = 0.f, f1 = 0.f;
         for (int i = 0; i < nch; ++i) {
             const int s = i % stages, buf = i & 1;
@@ -253,18 +256,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const float4 aw = *reinterpret_cast<const float4*>(xs + 2 * pj); // pairs pj, pj+1
                     const float2 nb = *reinterpret_cast<const float2*>(xs + 2 * kChunkPairs + pj);
                     {
-                        const float sum = xn + nb.x, re = gv[2 * j], im = gv[2 * j + 1];
-                        const float kA = ex2(ew2 * fmaxf(fmaf(-2.f, re, sum), 0.f));
-                        const float kP = ex2(ew2 * fmaxf(fmaf(-2.f, im, sum), 0.f));
-                        const float kM = ex2(ew2 * fmaxf(fmaf(2.f, im, sum), 0.f));
+                        const float es = exn + nb.x, re = gv[2 * j], im = gv[2 * j + 1];
+                        const float kA = ex2(fminf(fmaf(m2, re, es), 0.f));
+                        const float kP = ex2(fminf(fmaf(m2, im, es), 0.f));
+                        const float kM = ex2(fminf(fmaf(-m2, im, es), 0.f));
                         f0 = fmaf(aw.x, kA, fmaf(aw.y, kM, f0));
                         f1 = fmaf(aw.x, kP, fmaf(aw.y, kA, f1));
                     }
                     {
-                        const float sum = xn + nb.y, re = gv[2 * j + 2], im = gv[2 * j + 3];
-                        const float kA = ex2(ew2 * fmaxf(fmaf(-2.f, re, sum), 0.f));
-                        const float kP = ex2(ew2 * fmaxf(fmaf(-2.f, im, sum), 0.f));
-                        const float kM = ex2(ew2 * fmaxf(fmaf(2.f, im, sum), 0.f));
+                        const float es = exn + nb.y, re = gv[2 * j + 2], im = gv[2 * j + 3];
+                        const float kA = ex2(fminf(fmaf(m2, re, es), 0.f));
+                        const float kP = ex2(fminf(fmaf(m2, im, es), 0.f));
+                        const float kM = ex2(fminf(fmaf(-m2, im, es), 0.f));
                         f0 = fmaf(aw.z, kA, fmaf(aw.w, kM, f0));
                         f1 = fmaf(aw.z, kP, fmaf(aw.w, kA, f1));
                     }
