@@ -169,6 +169,9 @@ def run_batched(args, rank: int, world: int) -> dict | None:
     for _ in range(args.warmup):
         pool.run_prepared(jobs, mode=1)
     pool.wait()
+    # launch shapes chosen by the pool's autotuner on this batch (untimed; changes no result)
+    tuned = pool.autotune(jobs, mode=1)
+    shape = {k: tuned[k] for k in ("sweep_ctas_per_sm", "gram_stages", "detect_blocks_per_sm")}
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     stage = {"train": [], "sweep": [], "detect": []}
@@ -240,7 +243,8 @@ def run_batched(args, rank: int, world: int) -> dict | None:
         "metric": METRIC, "value": symbols / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded NOMA frames; no public dataset)",
-        "config": dict(WORKLOAD, parallelism=f"replicas x{world}", detectors=len(dets)),
+        "config": dict(WORKLOAD, parallelism=f"replicas x{world}", detectors=len(dets),
+                       launch_shape=dict(shape, chosen_by="apsm_pool_autotune")),
         "e2e": {"value": symbols / (e2e_total / args.steps * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_total / args.steps},
         "gpu_launches": launches,

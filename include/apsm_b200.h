@@ -253,6 +253,19 @@ apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uin
 /* Waits for the lane's last batch and, for APSM_RUN_HOST_ASYNC, writes its
  * estimates to the caller's buffers. */
 apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane);
+
+/*
+ * Launch-shape autotuner: runs the batch (same arguments as apsm_pool_run;
+ * it is waited for) once per candidate of each launch shape it exercises --
+ * training-sweep CTAs per SM, tensor-core detection pipeline stages, CUDA-core
+ * detection split threshold -- keeps the fastest by GPU time, and uses it for
+ * every later batch of this pool.  The detectors the batch trains get their
+ * state back: the call changes no detector and no result.  report (may be
+ * NULL) receives a JSON object with the trials and the chosen shape.  No
+ * reference counterpart (the reference launches fixed shapes).
+ */
+apsm_status apsm_pool_autotune(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs, int mode,
+                               char* report, size_t report_len);
 /* 1 when the lane's GPU work finished (call apsm_pool_wait for the estimates
  * of an asynchronous host batch), 0 while it runs, < 0 on error. */
 int apsm_pool_query(apsm_pool* p, uint32_t lane);

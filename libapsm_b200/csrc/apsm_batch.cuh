@@ -174,8 +174,9 @@ int batch_gram_kp(int mode, int N);
 size_t batch_gram_a_bytes(int mode, int Kp);
 size_t batch_gram_b_bytes(int mode, int Kp);
 size_t batch_gram_bx_floats();
+// stages: dictionary chunks in flight, 2 or 3 (0: the built-in choice; 3 only where it fits)
 cudaError_t launch_batch_gram(int mode, const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
                               const int* d_tile_prefix, int total_tiles, int Kp_max, float wL, float wG, int* d_err,
-                              cudaStream_t s);
+                              int stages, cudaStream_t s);
 
 } // namespace apsm

@@ -239,6 +239,12 @@ struct apsm_pool {
     std::vector<PoolDet> dets;
     std::vector<Lane> lanes;
     int device = 0, sms = 0, sweep_ctas = 1;
+    // launch shapes (0: the built-in choice), set by apsm_pool_autotune
+    struct Shape {
+        int sweep_per_sm = 0;         // training-sweep CTAs per SM (1 .. sweep_ctas)
+        int gram_stages = 0;          // tensor-core detection: dictionary chunks in flight (2, 3)
+        int detect_blocks_per_sm = 0; // CUDA-core detection: blocks per SM below which chunks are split
+    } shape;
     std::string last_error;
     std::mutex mu;
     std::FILE* trace = nullptr; // batch timeline lines (env APSM_POOL_TRACE = file path)
@@ -295,6 +301,7 @@ struct apsm_pool {
     apsm_status run(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode);
     apsm_status check_lane(uint32_t lane);
     apsm_status finish(uint32_t lane); // wait for the lane, hand out estimates, check its error flag
+    apsm_status autotune(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode, std::string* report);
 };
 
 #define POOL_CK(call)                                                                  \
@@ -577,7 +584,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             tiles_all += (dp[k].S + tile - 1) / tile;
             chunks_max = std::max(chunks_max, int((dp[k].Mp + chunk - 1) / chunk));
         }
-        const long long target = 4LL * std::max(1, sms);
+        const long long target = (shape.detect_blocks_per_sm > 0 ? shape.detect_blocks_per_sm : 4LL) * std::max(1, sms);
         if (tiles_all > 0 && tiles_all < target)
             det_parts = int(std::min<long long>(std::max(chunks_max, 1), (target + tiles_all - 1) / tiles_all));
     }
@@ -931,7 +938,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         }
         POOL_CK(launch_batch_kcol(d_tj, int(nT), max_cols, max_n, row_split, cm, s));
         if (trace) POOL_CK(cudaEventRecord(L.tr[3], s));
-        const int grid = int(std::min<size_t>(nT, size_t(sweep_ctas) * sms));
+        const int per_sm = shape.sweep_per_sm > 0 ? std::min(shape.sweep_per_sm, sweep_ctas) : sweep_ctas;
+        const int grid = int(std::min<size_t>(nT, size_t(per_sm) * sms));
         if (timing) POOL_CK(cudaEventRecord(L.ev[4], s));
         POOL_CK(launch_batch_sweep(d_tj, int(nT), cm, grid, d_counter, d_err, s));
         if (timing) POOL_CK(cudaEventRecord(L.ev[5], s));
@@ -1012,7 +1020,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                 POOL_CK(launch_batch_pack(d_pj + pack_train + (sg.k0 - nC), int(sg.k1 - sg.k0), ml, mn, s));
                 const auto& g = gseg[size_t(sg.g)];
                 POOL_CK(launch_batch_gram(gram_mode, d_gj + (sg.k0 - nC), g[1] - g[0], g[4], g[5], d_gp + g[2], g[3],
-                                          dp[sg.k0].cls, cfg.wL, cfg.wG, d_err, s));
+                                          dp[sg.k0].cls, cfg.wL, cfg.wG, d_err, shape.gram_stages, s));
                 L.launches += (ml > 0) + (g[4] > 0) + (g[5] > 0) + (g[3] > 0);
             }
             if (out_direct) {
@@ -1046,6 +1054,130 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     }
     POOL_CK(cudaEventRecord(L.done, s));
     if (mode == APSM_RUN_HOST) return finish(lane_id);
+    return APSM_OK;
+}
+
+// Launch-shape autotuner: the batch is run once per candidate of each knob
+// that it exercises (one knob at a time, the others at their current values),
+// the GPU time from its first to its last kernel compared, and the fastest
+// candidate kept.  The detectors the batch trains get their resident state back
+// after every trial and at the end, so the call leaves every detector as it
+// found it; no knob changes any result (each is a launch shape over the same
+// per-job arithmetic).
+apsm_status apsm_pool::autotune(uint32_t lane_id, const apsm_job* jobs, uint32_t n, int mode, std::string* report)
+{
+    apsm_pool* p = this;
+    Lane& L = lanes[lane_id];
+    if (!L.pending.empty()) {
+        apsm_status st = finish(lane_id);
+        if (st != APSM_OK) return st;
+    }
+    bool any_train = false, any_gram = false, any_core = false;
+    std::vector<uint32_t> ids;
+    for (uint32_t i = 0; i < n; ++i) {
+        const apsm_job& j = jobs[i];
+        if (j.detector >= dets.size() || !dets[j.detector].live)
+            return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": unknown detector");
+        if (j.kind == APSM_JOB_TRAIN) {
+            if (std::find(ids.begin(), ids.end(), j.detector) == ids.end()) ids.push_back(j.detector);
+            any_train = any_train || j.length > 0;
+        } else if (j.kind == APSM_JOB_DETECT && j.length > 0) {
+            const bool gram = cfg.detect_mode != DetectMode::Exact && dets[j.detector].N <= 32;
+            any_gram = any_gram || gram;
+            any_core = any_core || !gram;
+        }
+    }
+    // every lane idle: their batches may read the detectors being saved
+    for (auto& l : lanes) POOL_CK(cudaStreamSynchronize(l.stream));
+    size_t total = 0;
+    for (uint32_t id : ids) total += dets[id].bytes;
+    char* save = nullptr;
+    if (total > 0) POOL_CK(cudaMalloc(&save, total));
+    std::vector<uint32_t> used0;
+    {
+        size_t o = 0;
+        for (uint32_t id : ids) {
+            cudaError_t e = cudaMemcpy(save + o, dets[id].mem, dets[id].bytes, cudaMemcpyDeviceToDevice);
+            if (e != cudaSuccess) {
+                cudaFree(save);
+                return cuda_fail(e, "cudaMemcpy (autotune save)");
+            }
+            used0.push_back(dets[id].used);
+            o += dets[id].bytes;
+        }
+    }
+    auto restore = [&]() -> cudaError_t {
+        size_t o = 0;
+        for (size_t k = 0; k < ids.size(); ++k) {
+            PoolDet& d = dets[ids[k]];
+            cudaError_t e = cudaMemcpy(d.mem, save + o, d.bytes, cudaMemcpyDeviceToDevice);
+            if (e != cudaSuccess) return e;
+            d.used = used0[k];
+            o += d.bytes;
+        }
+        return cudaSuccess;
+    };
+    const bool timing0 = timing;
+    timing = true;
+    // GPU time of one run of the batch (best of two), first kernel to last
+    auto trial = [&](float* ms) -> apsm_status {
+        *ms = 0.f;
+        float best = -1.f;
+        for (int rep = 0; rep < 2; ++rep) {
+            cudaError_t e = restore();
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy (autotune restore)");
+            apsm_status st = run(lane_id, jobs, n, mode);
+            if (st == APSM_OK && mode != APSM_RUN_HOST) st = finish(lane_id);
+            if (st != APSM_OK) return st;
+            float t = 0.f;
+            cudaEvent_t a = L.have_train ? L.ev[0] : L.ev[2];
+            cudaEvent_t b = L.have_detect ? L.ev[3] : L.ev[1];
+            if (!L.have_train && !L.have_detect) return APSM_OK;
+            e = cudaEventElapsedTime(&t, a, b);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime (autotune)");
+            if (best < 0.f || t < best) best = t;
+        }
+        *ms = best;
+        return APSM_OK;
+    };
+    std::string rep = "{\"trials\": [";
+    bool first = true;
+    apsm_status st = APSM_OK;
+    auto tune = [&](const char* name, int* knob, const std::vector<int>& cands) {
+        if (st != APSM_OK || cands.size() < 2) return;
+        int best_v = *knob;
+        float best_ms = -1.f;
+        for (int v : cands) {
+            *knob = v;
+            float ms = 0.f;
+            st = trial(&ms);
+            if (st != APSM_OK) return;
+            rep += std::string(first ? "" : ", ") + "{\"" + name + "\": " + std::to_string(v) + ", \"ms\": " +
+                   std::to_string(ms) + "}";
+            first = false;
+            if (best_ms < 0.f || ms < best_ms) {
+                best_ms = ms;
+                best_v = v;
+            }
+        }
+        *knob = best_v;
+    };
+    if (any_train) {
+        std::vector<int> c;
+        for (int v = 1; v <= sweep_ctas; ++v) c.push_back(v);
+        tune("sweep_ctas_per_sm", &shape.sweep_per_sm, c);
+    }
+    if (any_gram) tune("gram_stages", &shape.gram_stages, {2, 3});
+    if (any_core) tune("detect_blocks_per_sm", &shape.detect_blocks_per_sm, {1, 2, 4, 8, 16});
+    timing = timing0;
+    const cudaError_t e = restore();
+    cudaFree(save);
+    if (st != APSM_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy (autotune restore)");
+    rep += "], \"sweep_ctas_per_sm\": " + std::to_string(shape.sweep_per_sm) +
+           ", \"gram_stages\": " + std::to_string(shape.gram_stages) +
+           ", \"detect_blocks_per_sm\": " + std::to_string(shape.detect_blocks_per_sm) + "}";
+    if (report) *report = rep;
     return APSM_OK;
 }
 
@@ -1310,6 +1442,20 @@ extern "C" apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job
     if (n_jobs > 0 && !jobs) return p->fail(APSM_ERR_INVALID_ARGUMENT, "null job list");
     if (device_buffers < 0 || device_buffers > 2) return p->fail(APSM_ERR_INVALID_ARGUMENT, "unknown run mode");
     return p->run(lane, jobs, n_jobs, device_buffers);
+}
+
+extern "C" apsm_status apsm_pool_autotune(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs,
+                                          int mode, char* report, size_t report_len)
+{
+    if (!p) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    if (lane >= p->lanes.size()) return p->fail(APSM_ERR_INVALID_ARGUMENT, "lane out of range");
+    if (n_jobs == 0 || !jobs) return p->fail(APSM_ERR_INVALID_ARGUMENT, "autotune needs a batch");
+    if (mode < 0 || mode > 2) return p->fail(APSM_ERR_INVALID_ARGUMENT, "unknown run mode");
+    std::string rep;
+    const apsm_status st = p->autotune(lane, jobs, n_jobs, mode, &rep);
+    if (st == APSM_OK) copy_err(report, report_len, rep);
+    return st;
 }
 
 extern "C" apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane)

@@ -308,7 +308,7 @@ template <int MODE> size_t gram_smem(int Kpmax, int stages)
 template <int MODE>
 cudaError_t launch_mode(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
                         const int* d_tile_prefix, int total_tiles, int Kp, float wL, float wG, int* d_err,
-                        cudaStream_t s)
+                        int stages_req, cudaStream_t s)
 {
     if (Kp % OpTraits<MODE>::kStepK != 0 || Kp > 64) return cudaErrorInvalidValue;
     if (max_tiles > 0) batch_gram_pack_a_kernel<MODE><<<dim3(max_tiles, n_jobs), 256, 0, s>>>(d_jobs, wL);
@@ -316,7 +316,9 @@ cudaError_t launch_mode(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, i
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || total_tiles <= 0) return e;
     // two pipeline stages when that lets two CTAs share an SM, else three if they fit
+    // (stages_req 2 or 3 overrides the choice where that many fit)
     int stages = (2 * gram_smem<MODE>(Kp, 3) > 227 * 1024) ? 2 : 3;
+    if (stages_req == 2 || (stages_req == 3 && gram_smem<MODE>(Kp, 3) <= 227 * 1024)) stages = stages_req;
     // every CTA holds 256 TMEM columns: at most two CTAs per SM (512 columns), so
     // shared memory is padded to more than a third of the SM's
     const size_t smem = std::max<size_t>(gram_smem<MODE>(Kp, stages), 80 * 1024);
@@ -348,20 +350,20 @@ size_t batch_gram_bx_floats() { return kBx; }
 
 cudaError_t launch_batch_gram(int mode, const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
                               const int* d_tile_prefix, int total_tiles, int Kp, float wL, float wG, int* d_err,
-                              cudaStream_t s)
+                              int stages, cudaStream_t s)
 {
     if (n_jobs <= 0) return cudaSuccess;
     switch (mode) {
     case kBF16:
-        return launch_mode<kBF16>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err, s);
+        return launch_mode<kBF16>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err, stages, s);
     case kBF16x3:
         return launch_mode<kBF16x3>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err,
-                                    s);
+                                    stages, s);
     case kTF32:
-        return launch_mode<kTF32>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err, s);
+        return launch_mode<kTF32>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err, stages, s);
     case kTF32x3:
         return launch_mode<kTF32x3>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err,
-                                    s);
+                                    stages, s);
     default:
         return cudaErrorInvalidValue;
     }

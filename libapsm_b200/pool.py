@@ -168,6 +168,17 @@ class DetectorPool:
         arr, _ = self._cjobs(jobs, device=True)
         self._check(self._lib.apsm_pool_run(self._h, int(lane), ctypes.cast(arr, ctypes.c_void_p), len(jobs), 1))
 
+    def autotune(self, prepared, lane: int = 0, mode: int = 0) -> dict:
+        """apsm_pool_autotune on a prepared batch (mode as in run_prepared): times the
+        batch under each candidate launch shape, keeps the fastest for later batches,
+        and leaves every detector's state as it was.  Returns the trials and the
+        chosen shape."""
+        arr, n, _, _ = prepared
+        buf = ctypes.create_string_buffer(1 << 14)
+        self._check(self._lib.apsm_pool_autotune(self._h, int(lane), ctypes.cast(arr, ctypes.c_void_p), n, int(mode),
+                                                  buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     def wait(self, lane: int = 0) -> None:
         self._check(self._lib.apsm_pool_wait(self._h, int(lane)))
 

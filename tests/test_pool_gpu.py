@@ -250,3 +250,40 @@ def test_pool_pinned_host_buffers_equal_pageable(native_lib):
              [PoolJob(d, pin(f[2]), est=o) for d, f, o in zip(dets, frames, outs)])
     for k in range(3):
         assert np.array_equal(outs[k], ref[3 + k])
+
+
+@pytest.mark.parametrize("dv", ["balanced", "gram_tf32x3"])
+def test_pool_autotune_changes_no_detector_and_no_result(native_lib, dv):
+    """apsm_pool_autotune runs the batch once per candidate launch shape; the
+    detectors it trains get their state back, and batches run with the chosen
+    shapes give the same estimates as with the built-in ones."""
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    cfg = dict(CFG, detectVersion=dv)
+    specs = [(3, 220, 200), (8, 160, 96), (16, 250, 300), (32, 150, 128)]
+    frames = [(N,) + _frame(400 + i, N, P, S) for i, (N, P, S) in enumerate(specs)]
+
+    def setup(pool):
+        ids = [pool.add(f[0]) for f in frames]
+        pool.run([PoolJob(d, f[1][:, :100], f[2][:100]) for d, f in zip(ids, frames)])  # resident state to append to
+        batch = ([PoolJob(d, f[1][:, 100:], f[2][100:]) for d, f in zip(ids, frames)] +
+                 [PoolJob(d, f[3]) for d, f in zip(ids, frames)])
+        return ids, batch
+
+    tuned = DetectorPool(cfg)
+    ids, batch = setup(tuned)
+    before = [tuned.get_state(d) for d in ids]
+    rep = tuned.autotune(tuned.prepare(batch))
+    assert rep["trials"] and rep["sweep_ctas_per_sm"] >= 1
+    after = [tuned.get_state(d) for d in ids]
+    for x, y in zip(before, after):
+        assert x[0] == y[0]
+        np.testing.assert_array_equal(x[1], y[1])
+        np.testing.assert_array_equal(x[2], y[2])
+    outs = tuned.run(batch)
+
+    plain = DetectorPool(cfg)
+    _, batch2 = setup(plain)
+    ref = plain.run(batch2)
+    for k in range(len(specs), 2 * len(specs)):
+        np.testing.assert_array_equal(outs[k], ref[k])
