@@ -59,7 +59,7 @@ def build(ptxas_verbose: bool = False) -> Path:
     if not LIB.exists() or LIB.stat().st_mtime < newest:
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", str(tmp)] + [str(o) for o in objs] + [
-            "-lcublas", "-lcudart"]
+            "-lcudart"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

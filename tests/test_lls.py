@@ -71,3 +71,24 @@ def test_lls_initialization_matches_oracle_and_reference(oracle_mod):
         r.train(f.rx_train, f.tx_train[1])
         er, _ = r.detect(f.rx_data)
         assert rel(est, er) < 1e-4
+
+
+@pytest.mark.gpu
+def test_lls_large_features_many_users(oracle_mod):
+    # 128 real features, 16 users (right-hand sides): the in-house FP64 normal-equation
+    # solve against the FP64 least-squares restatement
+    f = synth.generate_frame(42, K=16, N=64, P=500, S=300, modulation="QAM16", snr_db=15)
+    det = L.NomaDetectorFactory.build({"otype": "LLS"}, 64, num_users=16)
+    det.train(f.rx_train, f.tx_train)
+    est, _ = det.detect(f.rx_data)
+    for u in (0, 7, 15):
+        ref = oracle_mod.lls_detect(f.rx_data, oracle_mod.lls_weights(f.rx_train, f.tx_train[u]))
+        assert rel(est[u], ref) < 1e-4
+
+
+@pytest.mark.gpu
+def test_lls_too_few_pilots_is_an_error():
+    f = synth.generate_frame(43, K=2, N=16, P=10, S=20, modulation="QPSK")
+    det = L.NomaDetectorFactory.build({"otype": "LLS"}, 16)
+    with pytest.raises(ValueError, match="at least as many"):
+        det.train(f.rx_train, f.tx_train[0])
