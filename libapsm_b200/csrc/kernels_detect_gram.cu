@@ -325,19 +325,35 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
     if (threadIdx.x == 0 && *abort_flag) atomicExch(g.err, 1);
 }
 
-// out[u][s] = wL <w_u, x_s> + sum_split part[split][u][s] (fixed order).
-__global__ void gram_finish_kernel(const float* __restrict__ xs, int Dp, int D, const float* __restrict__ w, float wL,
-                                   const float* __restrict__ part, int splits, int users, int n_samples,
-                                   float* __restrict__ out, size_t out_stride)
+// out[u][s] = wL <w_u, x_s> + sum_split part[split][u][s] (fixed order).  A block
+// takes kFinSamples samples: their rows are read once, coalesced, into shared
+// memory, and warp u forms user u's linear terms (lane = sample, d in order).
+constexpr int kFinSamples = 32;
+constexpr int kFinWarps = 16;
+
+__global__ void __launch_bounds__(kFinWarps * 32)
+    gram_finish_kernel(const float* __restrict__ xs, int Dp, int D, const float* __restrict__ w, float wL,
+                       const float* __restrict__ part, int splits, int users, int n_samples, float* __restrict__ out,
+                       size_t out_stride)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= users * n_samples) return;
-    const int u = i / n_samples, s = i % n_samples;
-    float lin = 0.f;
-    for (int d = 0; d < D; ++d) lin = fmaf(w[size_t(u) * D + d], xs[size_t(s) * Dp + d], lin);
-    float gsum = 0.f;
-    for (int sp = 0; sp < splits; ++sp) gsum += part[(size_t(sp) * users + u) * n_samples + s];
-    out[size_t(u) * out_stride + s] = fmaf(wL, lin, gsum);
+    __shared__ float xt[kFinSamples][kMaxFeatures + 1];
+    const int s0 = blockIdx.x * kFinSamples;
+    for (int idx = threadIdx.x; idx < kFinSamples * D; idx += kFinWarps * 32) {
+        const int r = idx / D, d = idx % D;
+        xt[r][d] = s0 + r < n_samples ? xs[size_t(s0 + r) * Dp + d] : 0.f;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, s = s0 + lane;
+    for (int u = threadIdx.x >> 5; u < users; u += kFinWarps) {
+        const float* wu = w + size_t(u) * D;
+        float lin = 0.f;
+        for (int d = 0; d < D; ++d) lin = fmaf(__ldg(wu + d), xt[lane][d], lin);
+        if (s < n_samples) {
+            float gsum = 0.f;
+            for (int sp = 0; sp < splits; ++sp) gsum += part[(size_t(sp) * users + u) * n_samples + s];
+            out[size_t(u) * out_stride + s] = fmaf(wL, lin, gsum);
+        }
+    }
 }
 
 template <int MODE, int NU> void launch_gram(const GramArgs& ga, int n_tiles, int splits, size_t smem, cudaStream_t s,
@@ -435,7 +451,7 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     else if (U <= 8) launch_gram<MODE, 8>(ga, n_tiles, splits, smem, s, &e);
     else launch_gram<MODE, 16>(ga, n_tiles, splits, smem, s, &e);
     if (e != cudaSuccess) return h->cuda_fail(e, "gram_detect_kernel launch");
-    gram_finish_kernel<<<(U * ns + 255) / 256, 256, 0, s>>>(h->xs.p, Dp, D, h->w.p, h->cfg.wL, gw->part.p, splits, U,
+    gram_finish_kernel<<<(ns + kFinSamples - 1) / kFinSamples, kFinWarps * 32, 0, s>>>(h->xs.p, Dp, D, h->w.p, h->cfg.wL, gw->part.p, splits, U,
                                                             ns, d_out, size_t(ns));
     GR_CK(cudaGetLastError());
     GR_CK(cudaMemcpyAsync(gw->h_err, gw->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
