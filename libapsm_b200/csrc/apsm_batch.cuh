@@ -105,8 +105,8 @@ struct BatchDetectJob {
 
 // One detection job on the tensor cores (kernels_batch_gram.cu).
 struct BatchGramJob {
-    const float2* Ys;   // S x Np data samples
-    const float* nrm_s; // S norms
+    const float2* rx;   // N x S data samples, antenna-major (as the caller holds them)
+    float* nrm_s;       // S squared norms (written by the operand packing)
     const float* w;     // 2N linear weights
     float2* lin;        // S: wL <w, x_2s>, wL <w, x_2s+1>
     uint8_t* a_ops;     // ceil(S / 128) sample tiles, UMMA canonical layout (hi [| lo] of the Gram form)

@@ -590,7 +590,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     }
     size_t nCopyIn = 0;
     for (const auto& t : tp) nCopyIn += t.usedP > 0;
-    const size_t nPack = nT + nG; // CUDA-core detection reads the samples as the caller holds them
+    const size_t nPack = nT; // detection reads the samples as the caller holds them
     // descriptor region
     size_t o = 0;
     const size_t off_tj = o; o = align_up(o + sizeof(BatchTrainJob) * nT, 256);
@@ -656,7 +656,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     }
     for (auto& d : dp) {
         if (d.gram) {
-            d.off_Y = o; o = align_up(o + sizeof(float2) * size_t(d.S) * d.det->Np, 256);
             d.off_nrm = o; o = align_up(o + sizeof(float) * d.S, 256);
         }
         if (det_parts > 1 && !d.gram) {
@@ -826,11 +825,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         PoolDet& d = *q.det;
         const apsm_job& j = jobs[q.job];
         const float2* rx = host ? reinterpret_cast<const float2*>(D(q.off_rx)) : reinterpret_cast<const float2*>(j.rx);
-        auto* Ys = q.gram ? reinterpret_cast<float2*>(D(q.off_Y)) : nullptr;
         auto* ns = q.gram ? reinterpret_cast<float*>(D(q.off_nrm)) : nullptr;
-        if (q.gram) {
-            h_pj[ipack++] = BatchPackJob{rx, nullptr, nullptr, Ys, ns, nullptr, nullptr, int(q.S), int(d.N), int(d.Np)};
-        }
         float2* out = host ? reinterpret_cast<float2*>(D(q.off_est)) : reinterpret_cast<float2*>(j.est);
         const bool split = det_parts > 1 && !q.gram;
         h_dj[k] = BatchDetectJob{rx,       d.Y,       d.nrm, d.a,  d.w, out, int(q.S), int(q.Mp), int(d.N), int(d.Np),
@@ -838,7 +833,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                                  split ? reinterpret_cast<int*>(D(q.off_cnt)) : nullptr};
         if (q.gram) {
             BatchGramJob g{};
-            g.Ys = Ys;
+            g.rx = rx;
             g.nrm_s = ns;
             g.w = d.w;
             g.lin = reinterpret_cast<float2*>(D(q.off_lin));
@@ -920,7 +915,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_ci)), int(nCopyIn), max_pairs_in, max_np, s));
         L.launches += nCopyIn > 0 && max_pairs_in > 0;
     }
-    if (pack_train > 0) { // training samples (the detection jobs' are packed when they are needed)
+    if (pack_train > 0) { // training samples (detection reads its samples as the caller holds them)
         POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)), int(pack_train), max_len, max_n, s));
         L.launches += max_len > 0;
     }
@@ -999,7 +994,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         const auto* d_dj = reinterpret_cast<const BatchDetectJob*>(D(off_dj));
         const auto* d_gj = reinterpret_cast<const BatchGramJob*>(D(off_gj));
         const int* d_gp = reinterpret_cast<const int*>(D(off_gp));
-        const auto* d_pj = reinterpret_cast<const BatchPackJob*>(D(off_pj));
         for (size_t i = 0; i < segs.size(); ++i) {
             const Seg& sg = segs[i];
             if (overlap) POOL_CK(cudaStreamWaitEvent(s, L.seg_ev[i], 0));
@@ -1011,17 +1005,11 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                                             cfg.wG, s));
                 L.launches += tiles > 0;
             } else {
-                // the class's samples packed first (one pack job per tensor-core job, after the training ones)
-                int ml = 0, mn = 1;
-                for (size_t k = sg.k0; k < sg.k1; ++k) {
-                    ml = std::max(ml, int(dp[k].S));
-                    mn = std::max(mn, int(dp[k].det->N));
-                }
-                POOL_CK(launch_batch_pack(d_pj + pack_train + (sg.k0 - nC), int(sg.k1 - sg.k0), ml, mn, s));
+                // (the operand packing reads the class's samples as the caller holds them)
                 const auto& g = gseg[size_t(sg.g)];
                 POOL_CK(launch_batch_gram(gram_mode, d_gj + (sg.k0 - nC), g[1] - g[0], g[4], g[5], d_gp + g[2], g[3],
                                           dp[sg.k0].cls, cfg.wL, cfg.wG, d_err, shape.gram_stages, s));
-                L.launches += (ml > 0) + (g[4] > 0) + (g[5] > 0) + (g[3] > 0);
+                L.launches += (g[4] > 0) + (g[5] > 0) + (g[3] > 0);
             }
             if (out_direct) {
                 for (size_t k = sg.k0; k < sg.k1; ++k)

@@ -43,39 +43,71 @@ template <int MODE> __host__ __device__ constexpr size_t tile_bytes(int R, int K
     return size_t(R) * (OpTraits<MODE>::kSplit ? 2 * Kp : Kp) * OpTraits<MODE>::kElem;
 }
 
-// A operand tiles (hi [then lo] halves along K), the samples' linear terms wL <w, x>.
+// A operand tiles (hi [then lo] halves along K) straight from the caller's
+// antenna-major samples, with the samples' squared norms (the order of the
+// training-side packing: real parts, then imaginary parts) and linear terms
+// wL <w, x>.  The tile's samples are staged in shared memory (coalesced reads
+// along the samples); each thread then writes whole 16-byte K chunks.
 template <int MODE>
 __global__ void __launch_bounds__(256) batch_gram_pack_a_kernel(const BatchGramJob* __restrict__ jobs, float wL)
 {
+    using T = OpTraits<MODE>;
     const BatchGramJob& jb = jobs[blockIdx.y];
     const int t = blockIdx.x;
-    if (t * kTileM >= jb.S) return;
-    const int N = jb.N, Np = jb.Np, Kp = jb.Kp;
-    uint8_t* tile = jb.a_ops + size_t(t) * tile_bytes<MODE>(kTileM, Kp);
-    for (int idx = threadIdx.x; idx < kTileM * Kp; idx += blockDim.x) {
-        const int r = idx / Kp, k = idx % Kp;
-        const int s = t * kTileM + r;
-        float x = 0.f;
-        if (s < jb.S && k < 2 * N) {
-            const float2 v = jb.Ys[size_t(s) * Np + (k < N ? k : k - N)];
-            x = k < N ? v.x : v.y;
-        }
-        float hi, lo;
-        split_operand<MODE>(x, &hi, &lo);
-        put_operand<MODE>(tile, kTileM, r, k, hi);
-        if constexpr (OpTraits<MODE>::kSplit) put_operand<MODE>(tile, kTileM, r, Kp + k, lo);
+    const int S = jb.S;
+    const int s0 = t * kTileM;
+    if (s0 >= S) return;
+    const int N = jb.N, Kp = jb.Kp, pitch = N + 1;
+    const int nr = min(kTileM, S - s0);
+    extern __shared__ float2 sx[]; // [kTileM][N + 1]
+    for (int idx = threadIdx.x; idx < N * kTileM; idx += blockDim.x) {
+        const int k = idx / kTileM, i = idx % kTileM;
+        sx[i * pitch + k] = i < nr ? jb.rx[size_t(k) * S + s0 + i] : make_float2(0.f, 0.f);
     }
-    for (int r = threadIdx.x; r < kTileM; r += blockDim.x) {
-        const int s = t * kTileM + r;
-        if (s >= jb.S) continue;
+    __syncthreads();
+    uint8_t* tile = jb.a_ops + size_t(t) * tile_bytes<MODE>(kTileM, Kp);
+    const int nchunk = Kp / T::kChunk;
+    for (int idx = threadIdx.x; idx < kTileM * nchunk; idx += blockDim.x) {
+        const int r = idx % kTileM, c = idx / kTileM; // consecutive threads: consecutive rows
+        const float2* xr = sx + r * pitch;
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) hw[q] = lw[q] = 0u;
+#pragma unroll
+        for (int e = 0; e < T::kChunk; ++e) {
+            const int k = c * T::kChunk + e;
+            const float x = k < N ? xr[k].x : (k < 2 * N ? xr[k - N].y : 0.f);
+            float hi, lo;
+            split_operand<MODE>(x, &hi, &lo);
+            if constexpr (T::kTF) {
+                hw[e] = __float_as_uint(hi);
+                lw[e] = __float_as_uint(lo);
+            } else {
+                const uint32_t hb = __bfloat16_as_ushort(__float2bfloat16_rn(hi));
+                const uint32_t lb = __bfloat16_as_ushort(__float2bfloat16_rn(lo));
+                hw[e >> 1] |= hb << (16 * (e & 1));
+                lw[e >> 1] |= lb << (16 * (e & 1));
+            }
+        }
+        const size_t off = size_t(c) * (kTileM * 16) + (r >> 3) * 128 + (r & 7) * 16;
+        *reinterpret_cast<uint4*>(tile + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        if constexpr (T::kSplit)
+            *reinterpret_cast<uint4*>(tile + size_t(nchunk) * (kTileM * 16) + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+        const float2* xr = sx + r * pitch;
+        float nv = 0.f;
+        for (int k = 0; k < N; ++k) nv = fmaf(xr[k].x, xr[k].x, nv);
+        for (int k = 0; k < N; ++k) nv = fmaf(xr[k].y, xr[k].y, nv);
+        jb.nrm_s[s0 + r] = nv;
         float l0 = 0.f, l1 = 0.f;
         for (int k = 0; k < N; ++k) {
-            const float2 v = jb.Ys[size_t(s) * Np + k];
+            const float2 v = xr[k];
             const float w0 = jb.w[k], w1 = jb.w[N + k];
             l0 = fmaf(w0, v.x, fmaf(w1, v.y, l0));
             l1 = fmaf(w0, v.y, fmaf(-w1, v.x, l1));
         }
-        jb.lin[s] = make_float2(wL * l0, wL * l1);
+        jb.lin[s0 + r] = make_float2(wL * l0, wL * l1);
     }
 }
 
@@ -311,7 +343,10 @@ cudaError_t launch_mode(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, i
                         int stages_req, cudaStream_t s)
 {
     if (Kp % OpTraits<MODE>::kStepK != 0 || Kp > 64) return cudaErrorInvalidValue;
-    if (max_tiles > 0) batch_gram_pack_a_kernel<MODE><<<dim3(max_tiles, n_jobs), 256, 0, s>>>(d_jobs, wL);
+    // the tile's samples in shared memory: N <= Kp / 2 antennas
+    if (max_tiles > 0)
+        batch_gram_pack_a_kernel<MODE><<<dim3(max_tiles, n_jobs), 256, sizeof(float2) * kTileM * (Kp / 2 + 1), s>>>(
+            d_jobs, wL);
     if (max_chunks > 0) batch_gram_pack_b_kernel<MODE><<<dim3(max_chunks, n_jobs), 256, 0, s>>>(d_jobs, wG);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || total_tiles <= 0) return e;
