@@ -254,20 +254,44 @@ __global__ void __launch_bounds__(1024) train_sweep_kernel(TrainArgs args)
                 p = __fadd_rn(p, __fmul_rn(__fmul_rn(mp.wL, xv[b]), w_s[b]));
                 if (b < M) p = __fadd_rn(p, __fmul_rn(kStaged ? kc[lo + b] : __ldg(kc + lo + b), a_ring[(lo + b) & amask]));
             }
-            // Gaussian-only tail in chunks of 8: all loads first, then the ordered sum.
-            // Past the end the product is +0, and p + (+0) == p for the p this sum can reach.
-            for (; b < M; b += 8 * 32) {
+            // Gaussian-only tail in chunks of 8: all loads first, then the ordered sum.  Rows
+            // lo + b sit at ring positions (lo & amask) + b until the ring wraps at b = bw, then
+            // at b - bw: whole chunks on either side of the wrap index both arrays directly
+            // (no masks, no range checks); the chunk across the wrap and the last one are
+            // checked, where past the end the product is +0, and p + (+0) == p for the p this
+            // sum can reach.
+            const float* kp = kc + lo;
+            const int lo_m = lo & amask, bw = args.A_ring - lo_m;
+            auto chunk_direct = [&](const float* ap) {
+                float kv[8], av[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    kv[j] = kStaged ? kp[b + 32 * j] : __ldg(kp + b + 32 * j);
+                    av[j] = ap[b + 32 * j];
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) p = __fadd_rn(p, __fmul_rn(kv[j], av[j]));
+            };
+            auto chunk_checked = [&]() {
                 float kv[8], av[8];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const int bb = b + 32 * j;
                     const bool ok = bb < M;
-                    kv[j] = ok ? (kStaged ? kc[lo + bb] : __ldg(kc + lo + bb)) : 0.f;
+                    kv[j] = ok ? (kStaged ? kp[bb] : __ldg(kp + bb)) : 0.f;
                     av[j] = ok ? a_ring[(lo + bb) & amask] : 0.f;
                 }
 #pragma unroll
                 for (int j = 0; j < 8; ++j) p = __fadd_rn(p, __fmul_rn(kv[j], av[j]));
+            };
+            const int lim1 = min(M, bw);
+            for (; b + 7 * 32 < lim1; b += 8 * 32) chunk_direct(a_ring + lo_m);
+            if (b < lim1) { // the chunk that reaches the wrap or the end
+                chunk_checked();
+                b += 8 * 32;
             }
+            for (; b + 7 * 32 < M; b += 8 * 32) chunk_direct(a_ring - bw); // past the wrap: b >= bw
+            for (; b < M; b += 8 * 32) chunk_checked();
             if (v == first) APSM_PROF_MARK(6);
             red[warp * 32 + lane] = p;
             __syncwarp();
