@@ -170,8 +170,11 @@ def run_batched(args, rank: int, world: int) -> dict | None:
         pool.run_prepared(jobs, mode=1)
     pool.wait()
     # launch shapes chosen by the pool's autotuner on this batch (untimed; changes no result)
-    tuned = pool.autotune(jobs, mode=1)
-    shape = {k: tuned[k] for k in ("sweep_ctas_per_sm", "gram_stages", "detect_blocks_per_sm")}
+    if args.no_autotune:
+        shape = {"sweep_ctas_per_sm": 0, "gram_stages": 0, "detect_blocks_per_sm": 0}
+    else:
+        tuned = pool.autotune(jobs, mode=1)
+        shape = {k: tuned[k] for k in ("sweep_ctas_per_sm", "gram_stages", "detect_blocks_per_sm")}
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     stage = {"train": [], "sweep": [], "detect": []}
@@ -244,7 +247,8 @@ def run_batched(args, rank: int, world: int) -> dict | None:
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded NOMA frames; no public dataset)",
         "config": dict(WORKLOAD, parallelism=f"replicas x{world}", detectors=len(dets),
-                       launch_shape=dict(shape, chosen_by="apsm_pool_autotune")),
+                       launch_shape=dict(shape, chosen_by="built-in (0 = built-in choice)" if args.no_autotune
+                                         else "apsm_pool_autotune")),
         "e2e": {"value": symbols / (e2e_total / args.steps * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_total / args.steps},
         "gpu_launches": launches,
@@ -573,6 +577,8 @@ def main():
     ap.add_argument("--detectors", type=int, default=N_DET,
                     help="detectors of the batched workload (the first ones of the same seeded draw; 512 is the "
                          "benchmark, fewer only for profiling captures)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip the pool's launch-shape autotuner (profiler runs: its timings are distorted there)")
     ap.add_argument("--precision-only", action="store_true",
                     help="run only the large-detect precision study (N=64, dictionary 8192) and print it")
     ap.add_argument("--serving-only", action="store_true",
