@@ -434,8 +434,8 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
     pool.run([L.PoolJob(i, p.frame.rx_train, p.frame.tx_train) for i, p in zip(ids, pop)])
     srv = L.DetectorServer(pool, max_batch=max_batch)
 
-    # warm-up batches of the largest requests (every lane's scratch and page-locked buffers
-    # grown to the largest batch before timing: growing them allocates, which stalls a request)
+    # the largest requests (every lane's scratch and page-locked buffers are grown to a batch
+    # of them before timing: growing them allocates, which would stall a timed request)
     big = sorted(range(len(pop)), key=lambda d: -pop[d].frame.N)[: lanes * max_batch]
     big_reqs = [(0.0, d, "detect", 4000) for d in big] + [(0.0, d, "train", 64) for d in big]
     need = sum(8 * (pop[d].frame.N + 1) * n + 512 for (_, d, _, n) in reqs + warm_reqs + big_reqs)
@@ -456,10 +456,12 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
             return L.PoolJob(ids[d], pinned(p.pilots_rx[:, :n]), pinned(p.pilots_tx[:n]))
         return L.PoolJob(ids[d], pinned(p.data_rx[:, :n]), est=pinned(np.zeros(n, np.complex64)))
 
-    # warm-up: every lane's scratch and staging buffers at their working sizes
+    # warm-up: every lane's scratch and staging buffers reserved for a batch of the largest
+    # requests of each kind, then requests like the timed ones
     for kind in ("detect", "train"):
-        for t in [srv.submit_prepared(srv.make_job(job(d, k, n))) for (_, d, k, n) in big_reqs if k == kind]:
-            srv.wait(t)
+        big_batch = pool.prepare([job(d, k, n) for (_, d, k, n) in big_reqs if k == kind][:max_batch])
+        for lane in range(lanes):
+            pool.reserve(big_batch, lane=lane)
     for t in [srv.submit_prepared(srv.make_job(job(d, kind, n))) for (_, d, kind, n) in warm_reqs]:
         srv.wait(t)
     prepared = [(ta, kind, n, srv.make_job(job(d, kind, n))) for (ta, d, kind, n) in reqs]

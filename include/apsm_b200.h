@@ -255,6 +255,17 @@ apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uin
 apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane);
 
 /*
+ * Grows the lane's device scratch and page-locked buffers to what this batch
+ * (same arguments as apsm_pool_run) needs, without running it or changing any
+ * detector; returns once the memory is in place.  A lane grows its buffers on
+ * demand otherwise, and growing them (mapping device memory, page-locking
+ * host memory) stalls the batch that needs it for milliseconds: a request
+ * server reserves every lane for its largest batch before taking requests.
+ * No reference counterpart.
+ */
+apsm_status apsm_pool_reserve(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs, int mode);
+
+/*
  * Launch-shape autotuner: runs the batch (same arguments as apsm_pool_run;
  * it is waited for) once per candidate of each launch shape it exercises --
  * training-sweep CTAs per SM, tensor-core detection pipeline stages, CUDA-core

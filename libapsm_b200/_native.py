@@ -67,6 +67,7 @@ SIGNATURES = [
     ("apsm_pool_reset", ctypes.c_int, [_P, _U32]),
     ("apsm_pool_run", ctypes.c_int, [_P, _U32, _P, _U32, ctypes.c_int]),
     ("apsm_pool_wait", ctypes.c_int, [_P, _U32]),
+    ("apsm_pool_reserve", ctypes.c_int, [_P, _U32, _P, _U32, ctypes.c_int]),
     ("apsm_pool_autotune", ctypes.c_int, [_P, _U32, _P, _U32, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
     ("apsm_pool_query", ctypes.c_int, [_P, _U32]),
     ("apsm_pool_stream", _P, [_P, _U32]),

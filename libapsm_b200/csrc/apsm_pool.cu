@@ -298,7 +298,8 @@ struct apsm_pool {
     }
     size_t train_bytes(const PoolDet& d, uint32_t P, bool host) const;
     size_t detect_bytes(const PoolDet& d, uint32_t S, bool host) const;
-    apsm_status run(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode);
+    // reserve_only: plan the batch and grow the lane's buffers to its needs, run nothing
+    apsm_status run(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode, bool reserve_only = false);
     apsm_status check_lane(uint32_t lane);
     apsm_status finish(uint32_t lane); // wait for the lane, hand out estimates, check its error flag
     apsm_status autotune(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode, std::string* report);
@@ -423,7 +424,7 @@ size_t apsm_pool::detect_bytes(const PoolDet& d, uint32_t S, bool host) const
     return b + sizeof(BatchDetectJob) + sizeof(BatchPackJob);
 }
 
-apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, int mode)
+apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, int mode, bool reserve_only)
 {
     apsm_pool* p = this;
     Lane& L = lanes[lane_id];
@@ -716,6 +717,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         L.pinned_out_bytes = 0;
         POOL_CK(cudaMallocHost(&L.pinned_out, want));
         L.pinned_out_bytes = want;
+    }
+    if (reserve_only) {
+        POOL_CK(cudaStreamSynchronize(L.stream)); // the scratch is mapped now, not under a later batch
+        return APSM_OK;
     }
     POOL_CK(cudaEventSynchronize(L.desc_copied)); // the previous batch's descriptors were consumed
     char* dev = static_cast<char*>(L.scratch);
@@ -1430,6 +1435,17 @@ extern "C" apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job
     if (n_jobs > 0 && !jobs) return p->fail(APSM_ERR_INVALID_ARGUMENT, "null job list");
     if (device_buffers < 0 || device_buffers > 2) return p->fail(APSM_ERR_INVALID_ARGUMENT, "unknown run mode");
     return p->run(lane, jobs, n_jobs, device_buffers);
+}
+
+extern "C" apsm_status apsm_pool_reserve(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs,
+                                         int mode)
+{
+    if (!p) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    if (lane >= p->lanes.size()) return p->fail(APSM_ERR_INVALID_ARGUMENT, "lane out of range");
+    if (n_jobs > 0 && !jobs) return p->fail(APSM_ERR_INVALID_ARGUMENT, "null job list");
+    if (mode < 0 || mode > 2) return p->fail(APSM_ERR_INVALID_ARGUMENT, "unknown run mode");
+    return p->run(lane, jobs, n_jobs, mode, true);
 }
 
 extern "C" apsm_status apsm_pool_autotune(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs,

@@ -168,6 +168,12 @@ class DetectorPool:
         arr, _ = self._cjobs(jobs, device=True)
         self._check(self._lib.apsm_pool_run(self._h, int(lane), ctypes.cast(arr, ctypes.c_void_p), len(jobs), 1))
 
+    def reserve(self, prepared, lane: int = 0, mode: int = 0) -> None:
+        """apsm_pool_reserve: grow the lane's buffers to this batch's needs now, so that
+        no later batch stalls on growing them; runs nothing."""
+        arr, n, _, _ = prepared
+        self._check(self._lib.apsm_pool_reserve(self._h, int(lane), ctypes.cast(arr, ctypes.c_void_p), n, int(mode)))
+
     def autotune(self, prepared, lane: int = 0, mode: int = 0) -> dict:
         """apsm_pool_autotune on a prepared batch (mode as in run_prepared): times the
         batch under each candidate launch shape, keeps the fastest for later batches,

@@ -287,3 +287,28 @@ def test_pool_autotune_changes_no_detector_and_no_result(native_lib, dv):
     ref = plain.run(batch2)
     for k in range(len(specs), 2 * len(specs)):
         np.testing.assert_array_equal(outs[k], ref[k])
+
+
+def test_pool_reserve_runs_nothing(native_lib):
+    """apsm_pool_reserve grows a lane's buffers for a batch without running it:
+    the detectors keep their state, and the batch run afterwards gives what it
+    gives without the reservation."""
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    frames = [(N,) + _frame(500 + i, N, P, S) for i, (N, P, S) in enumerate([(4, 120, 3000), (32, 200, 2000)])]
+
+    def batch(pool, ids):
+        return ([PoolJob(d, f[1], f[2]) for d, f in zip(ids, frames)] + [PoolJob(d, f[3]) for d, f in zip(ids, frames)])
+
+    a = DetectorPool(dict(CFG, detectVersion="gram_tf32x3"), lanes=2)
+    ids = [a.add(f[0]) for f in frames]
+    b0 = batch(a, ids)
+    a.reserve(a.prepare(b0), lane=1)
+    for d in ids:
+        assert a.get_state(d)[0] == 0  # untrained still
+    outs = a.run(b0, lane=1)
+    ref_pool = DetectorPool(dict(CFG, detectVersion="gram_tf32x3"), lanes=2)
+    ids2 = [ref_pool.add(f[0]) for f in frames]
+    ref = ref_pool.run(batch(ref_pool, ids2), lane=1)
+    for k in range(2, 4):
+        np.testing.assert_array_equal(outs[k], ref[k])
