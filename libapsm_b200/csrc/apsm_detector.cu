@@ -99,6 +99,7 @@ apsm_status apsm_detector::init(const Config& c, uint32_t num_antennas, uint32_t
     APSM_CK(train_err.ensure(1));
     APSM_CK(cudaMemset(train_err.p, 0, sizeof(int)));
     cluster = env_int("APSM_TRAIN_CLUSTER", 16);
+    gram_one_product = env_int("APSM_GRAM_ONE_PRODUCT", 0) != 0;
     force_glob_a = env_int("APSM_TRAIN_GLOBAL_RING", 0) != 0;
     return reset();
 }

@@ -116,6 +116,7 @@ struct apsm_detector {
     apsm::GramWorkspace* gram = nullptr;
     apsm::LlsWorkspace* lls = nullptr; // least-squares detector / llsInitialization
     bool is_lls = false;               // "otype": "LLS"
+    bool gram_one_product = false;     // APSM_GRAM_ONE_PRODUCT=1: users' sums on the CUDA cores for any user count
 
     // training-kernel launch shape: requested cluster size, and the last one used
     int cluster = 0;

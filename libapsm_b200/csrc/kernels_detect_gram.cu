@@ -42,7 +42,7 @@ constexpr int kThreads = (kEpiWarps + 2) * 32;
 constexpr int kMaxUsers = 16;
 
 struct GramWorkspace {
-    DevBuf<uint8_t> a_ops, b_ops; // operand tiles in the UMMA canonical K-major layout
+    DevBuf<uint8_t> a_ops, b_ops, w_ops; // operand tiles in the UMMA canonical K-major layout
     DevBuf<float> xn, dn, aw, part, lin_unused;
     DevBuf<int> err;
     int* h_err = nullptr;
@@ -356,6 +356,292 @@ __global__ void __launch_bounds__(kFinWarps * 32)
     }
 }
 
+// ------------------------------------------------ two-product form (users >= 4) --
+// The users' contraction on the tensor cores too: per chunk of N dictionary
+// rows, the epilogue turns the Gram tile into kernel values P (128 x N, in the
+// mode's operand format: hi [+ lo]) in shared memory, and a second UMMA
+// (M = 128, N = 16 users, K = N rows) accumulates P W with W the chunk's
+// coefficients a * wG (16 x N, padded with zero users) into tensor memory for
+// the whole dictionary range of the CTA.  The epilogue then costs one
+// exponential and a store per kernel value instead of one FMA per user; the
+// second product rounds P and W to the operand format (split modes: hi/lo, 3
+// products).  Used for the BF16 form with 4 or more users: at N = 64, 16
+// users, a 65536-symbol detection takes 2.54 ms instead of 3.21 ms, the soft
+// outputs moving from 1.4e-6 to 5.2e-5 of the largest output away from the
+// float64 model (decisions unchanged); the TF32 form gains 2 % for a 10x
+// larger error and the split forms lose time (larger P buffers, 3 products),
+// so they keep the one-product kernel.
+constexpr int kUsers2 = 16; // UMMA N of the users' product
+
+struct Gram2Args {
+    const uint8_t* a_ops; // data tiles (kTileM rows)
+    const uint8_t* b_ops; // dictionary chunks (N rows)
+    const uint8_t* w_ops; // per chunk: W, 16 rows x N (K), canonical K-major, hi [| lo]
+    const float* xn;      // data norms
+    const float* dn;      // dictionary norms (Mpad)
+    float* part;          // splits x users x n_samples partial sums
+    int* err;
+    int n_samples, users, Kp, N;
+    int chunks_per_split, n_chunks;
+    int stages;
+    float ewl2; // ew * log2(e)
+};
+
+// W chunks: element (u, k) = a[u][c N + k] * wG (0 past M and for u >= users)
+template <int MODE>
+__global__ void gram_pack_w_kernel(const float* __restrict__ a, size_t a_stride, int users, int M, int N, int n_chunks,
+                                   float wG, uint8_t* __restrict__ w_ops)
+{
+    using T = OpTraits<MODE>;
+    const int KE2 = T::kSplit ? 2 * N : N;
+    const size_t total = size_t(n_chunks) * kUsers2 * N;
+    for (size_t idx = blockIdx.x * size_t(blockDim.x) + threadIdx.x; idx < total; idx += size_t(gridDim.x) * blockDim.x) {
+        const int k = int(idx % N);
+        const size_t rest = idx / N;
+        const int u = int(rest % kUsers2), c = int(rest / kUsers2);
+        const int b = c * N + k;
+        const float v = (u < users && b < M) ? __fmul_rn(a[size_t(u) * a_stride + b], wG) : 0.f;
+        float hi, lo;
+        split_operand<MODE>(v, &hi, &lo);
+        uint8_t* tile = w_ops + size_t(c) * kUsers2 * KE2 * T::kElem;
+        put_operand<MODE>(tile, kUsers2, u, k, hi);
+        if constexpr (T::kSplit) put_operand<MODE>(tile, kUsers2, u, N + k, lo);
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1) gram_detect2_kernel(Gram2Args g)
+{
+    using T = OpTraits<MODE>;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int N = g.N, NS = g.stages;
+    const int KE = T::kSplit ? 2 * g.Kp : g.Kp;
+    const int KE2 = T::kSplit ? 2 * N : N; // K extent of the second product's operands
+    const uint32_t a_bytes = uint32_t(kTileM) * KE * T::kElem;
+    const uint32_t b_bytes = uint32_t(N) * KE * T::kElem;
+    const uint32_t w_bytes = uint32_t(kUsers2) * KE2 * T::kElem;
+    const uint32_t p_bytes = uint32_t(kTileM) * KE2 * T::kElem;
+    uint8_t* sA = smem;
+    uint8_t* sB = sA + a_bytes;                          // [NS] chunk rows
+    uint8_t* sW = sB + size_t(NS) * b_bytes;             // [NS] chunk coefficients
+    uint8_t* sP = sW + size_t(NS) * w_bytes;             // [2] kernel values
+    float* sD = reinterpret_cast<float*>(sP + 2 * size_t(p_bytes)); // [NS][N] chunk norms
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sD + size_t(NS) * N);
+    uint64_t* full = bars;             // [NS]
+    uint64_t* empty = bars + NS;       // [NS]
+    uint64_t* tfull = bars + 2 * NS;   // [2]
+    uint64_t* tempty = tfull + 2;      // [2]
+    uint64_t* pfull = tempty + 2;      // [2]
+    uint64_t* pempty = pfull + 2;      // [2]
+    uint64_t* afull = pempty + 2;      // [1]
+    uint64_t* done = afull + 1;        // [1] every product of the CTA completed
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x, split = blockIdx.y;
+    const int c0 = split * g.chunks_per_split;
+    const int c1 = min(g.n_chunks, c0 + g.chunks_per_split);
+    const int nch = max(0, c1 - c0);
+    uint32_t ncols = 32;
+    while (ncols < uint32_t(2 * N + kUsers2)) ncols <<= 1;
+    const uint32_t acc2 = uint32_t(2 * N); // column of the users' accumulator
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1 + kEpiWarps);
+        }
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&tfull[s], 1);
+            mbar_init(&tempty[s], kEpiWarps);
+            mbar_init(&pfull[s], kEpiWarps);
+            mbar_init(&pempty[s], 1);
+        }
+        mbar_init(afull, 1);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == kEpiWarps + 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == kEpiWarps) {
+        // ---------------- producer: data tile once, then dictionary chunks with their W and norms ----------------
+        if (lane == 0) {
+            mbar_expect_tx(afull, a_bytes);
+            bulk_g2s(sA, g.a_ops + size_t(tile) * a_bytes, a_bytes, afull);
+            int issued = 0;
+            for (int i = 0; i < nch; ++i) {
+                const int s = i % NS;
+                if (i >= NS && !mbar_wait(&empty[s], ((i / NS) - 1) & 1, abort_flag)) break;
+                ++issued;
+                const int c = c0 + i;
+                mbar_expect_tx(&full[s], b_bytes + w_bytes + uint32_t(N) * 4);
+                bulk_g2s(sB + size_t(s) * b_bytes, g.b_ops + size_t(c) * b_bytes, b_bytes, &full[s]);
+                bulk_g2s(sW + size_t(s) * w_bytes, g.w_ops + size_t(c) * w_bytes, w_bytes, &full[s]);
+                bulk_g2s(sD + size_t(s) * N, g.dn + size_t(c) * N, uint32_t(N) * 4, &full[s]);
+            }
+            mbar_drain(afull, 0);
+            for (int i = max(0, issued - NS); i < issued; ++i) mbar_drain(&full[i % NS], (i / NS) & 1);
+        }
+    } else if (warp == kEpiWarps + 1) {
+        // ---------------- MMA issuer: Gram tile of chunk i, then the users' product of chunk i - 1 ----------------
+        if (lane == 0 && mbar_wait(afull, 0, abort_flag)) {
+            const uint32_t idesc = instr_desc<MODE>(kTileM, N);
+            const uint32_t idesc2 = instr_desc<MODE>(kTileM, kUsers2);
+            const uint32_t lbo_a = kTileM * 16, lbo_b = uint32_t(N) * 16, lbo_w = kUsers2 * 16;
+            const int ksteps = g.Kp / T::kStepK, ksteps2 = N / T::kStepK;
+            const int lo_off = g.Kp / T::kChunk, lo_off2 = N / T::kChunk;
+            bool ok = true;
+            auto product2 = [&](int j) {
+                const int pb = j & 1, sj = j % NS;
+                if (!mbar_wait(&pfull[pb], (j >> 1) & 1, abort_flag)) {
+                    ok = false;
+                    return;
+                }
+                tc_fence_after();
+                const uint8_t* p = sP + size_t(pb) * p_bytes;
+                const uint8_t* w = sW + size_t(sj) * w_bytes;
+                for (int kk = 0; kk < ksteps2; ++kk) {
+                    const uint64_t ah = smem_desc(p + size_t(2 * kk) * lbo_a, lbo_a, 128);
+                    const uint64_t bh = smem_desc(w + size_t(2 * kk) * lbo_w, lbo_w, 128);
+                    umma<MODE>(tmem + acc2, ah, bh, idesc2, (j > 0 || kk > 0) ? 1u : 0u);
+                    if constexpr (T::kSplit) {
+                        const uint64_t al = smem_desc(p + size_t(lo_off2 + 2 * kk) * lbo_a, lbo_a, 128);
+                        const uint64_t bl = smem_desc(w + size_t(lo_off2 + 2 * kk) * lbo_w, lbo_w, 128);
+                        umma<MODE>(tmem + acc2, ah, bl, idesc2, 1u);
+                        umma<MODE>(tmem + acc2, al, bh, idesc2, 1u);
+                    }
+                }
+                umma_commit(&pempty[pb]); // kernel-value buffer free once these products completed
+                umma_commit(&empty[sj]);  // the chunk's rows and coefficients too
+            };
+            for (int i = 0; i < nch && ok; ++i) {
+                const int s = i % NS, buf = i & 1;
+                if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag)) break;
+                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag)) break;
+                tc_fence_after();
+                const uint8_t* b = sB + size_t(s) * b_bytes;
+                const uint32_t d = tmem + uint32_t(buf * N);
+                for (int kk = 0; kk < ksteps; ++kk) {
+                    const uint64_t ah = smem_desc(sA + size_t(2 * kk) * lbo_a, lbo_a, 128);
+                    const uint64_t bh = smem_desc(b + size_t(2 * kk) * lbo_b, lbo_b, 128);
+                    umma<MODE>(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
+                    if constexpr (T::kSplit) {
+                        const uint64_t al = smem_desc(sA + size_t(lo_off + 2 * kk) * lbo_a, lbo_a, 128);
+                        const uint64_t bl = smem_desc(b + size_t(lo_off + 2 * kk) * lbo_b, lbo_b, 128);
+                        umma<MODE>(d, ah, bl, idesc, 1);
+                        umma<MODE>(d, al, bh, idesc, 1);
+                    }
+                }
+                umma_commit(&tfull[buf]); // Gram tile ready for the epilogue
+                if (i >= 1) product2(i - 1);
+            }
+            if (ok && nch > 0 && !*abort_flag) product2(nch - 1);
+        }
+        if (lane == 0) {
+            umma_commit(done);
+            mbar_drain(done, 0);
+        }
+    } else {
+        // ---------------- epilogue: kernel values of each chunk into P; at the end the users' sums ----------------
+        const int q = warp & 3, h = warp >> 2;
+        const int r = q * 32 + lane; // row of the tile (tensor-memory lane)
+        const int row = tile * kTileM + r;
+        const float xn = row < g.n_samples ? g.xn[row] : 0.f;
+        const int half = N / 2;
+        bool ok = true;
+        for (int i = 0; i < nch; ++i) {
+            const int s = i % NS, buf = i & 1, pb = i & 1;
+            if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag) || !mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag) ||
+                (i >= 2 && !mbar_wait(&pempty[pb], ((i >> 1) - 1) & 1, abort_flag))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const float* dn = sD + size_t(s) * N;
+            uint8_t* p = sP + size_t(pb) * p_bytes;
+            const uint32_t trow = tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * N);
+            for (int cb = 0; cb < half; cb += 16) {
+                const int col = h * half + cb;
+                float gv[16];
+                tmem_ld16(trow + uint32_t(col), gv);
+#pragma unroll
+                for (int j0 = 0; j0 < 16; j0 += T::kChunk) {
+                    // one 16-byte K chunk of this row: hi, and lo for split modes
+                    uint32_t hw[4] = {0u, 0u, 0u, 0u}, lw[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                    for (int e = 0; e < T::kChunk; ++e) {
+                        const int j = j0 + e;
+                        const float kv = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j], xn + dn[col + j]), 0.f));
+                        float hi, lo;
+                        split_operand<MODE>(kv, &hi, &lo);
+                        if constexpr (T::kTF) {
+                            hw[e] = __float_as_uint(hi);
+                            lw[e] = __float_as_uint(lo);
+                        } else {
+                            hw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(hi))) << (16 * (e & 1));
+                            lw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(lo))) << (16 * (e & 1));
+                        }
+                    }
+                    const int kc = (col + j0) / T::kChunk;
+                    const size_t off = size_t(kc) * (kTileM * 16) + (r >> 3) * 128 + (r & 7) * 16;
+                    *reinterpret_cast<uint4*>(p + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+                    if constexpr (T::kSplit)
+                        *reinterpret_cast<uint4*>(p + size_t(N / T::kChunk) * (kTileM * 16) + off) =
+                            make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                }
+            }
+            tc_fence_before();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // P visible to the tensor cores
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&tempty[buf]);
+                mbar_arrive(&empty[s]);
+                mbar_arrive(&pfull[pb]);
+            }
+        }
+        if (h == 0) {
+            // warps 0-3 read the users' sums of their 32 lanes (tcgen05.ld is warp-wide: the
+            // whole warp loads, the lanes of rows past the end discard)
+            float acc[kUsers2];
+#pragma unroll
+            for (int u = 0; u < kUsers2; ++u) acc[u] = 0.f;
+            const bool have = ok && nch > 0 && mbar_wait(done, 0, abort_flag);
+            if (__all_sync(0xffffffffu, have)) {
+                tc_fence_after();
+                tmem_ld16(tmem + (uint32_t(q * 32) << 16) + acc2, acc);
+            }
+            if (row < g.n_samples)
+                for (int u = 0; u < g.users; ++u) g.part[(size_t(split) * g.users + u) * g.n_samples + row] = acc[u];
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == kEpiWarps + 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+    }
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(g.err, 1);
+}
+
+template <int MODE> size_t gram2_smem(int Kp, int N, int stages)
+{
+    using T = OpTraits<MODE>;
+    const size_t KE = T::kSplit ? 2 * Kp : Kp, KE2 = T::kSplit ? 2 * N : N;
+    return size_t(kTileM) * KE * T::kElem + size_t(stages) * (size_t(N) * KE * T::kElem + kUsers2 * KE2 * T::kElem) +
+           2 * size_t(kTileM) * KE2 * T::kElem + size_t(stages) * N * 4 + (2 * stages + 10) * 8 + 16;
+}
+
 template <int MODE, int NU> void launch_gram(const GramArgs& ga, int n_tiles, int splits, size_t smem, cudaStream_t s,
                                              cudaError_t* e)
 {
@@ -363,6 +649,78 @@ template <int MODE, int NU> void launch_gram(const GramArgs& ga, int n_tiles, in
     if (*e != cudaSuccess) return;
     gram_detect_kernel<MODE, NU><<<dim3(n_tiles, splits), kThreads, smem, s>>>(ga);
     *e = cudaGetLastError();
+}
+
+template <int MODE>
+apsm_status run_gram2(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s, int Kp, int N, int stages)
+{
+    using T = OpTraits<MODE>;
+    GramWorkspace* gw = h->gram;
+    const int ns = int(2 * S);
+    const int M = int(h->used);
+    const int D = int(h->D), Dp = int(h->Dp), U = int(h->U);
+    const int KE = T::kSplit ? 2 * Kp : Kp, KE2 = T::kSplit ? 2 * N : N;
+    const int n_tiles = (ns + kTileM - 1) / kTileM;
+    const int n_chunks = std::max(1, (M + N - 1) / N);
+    const int Mpad = n_chunks * N;
+    int splits = std::max(1, std::min(n_chunks, (148 + n_tiles - 1) / n_tiles)); // one CTA per SM
+    const int cps = (n_chunks + splits - 1) / splits;
+    splits = (n_chunks + cps - 1) / cps;
+
+    cudaError_t e;
+#define GR_CK(x)                                                   \
+    do {                                                           \
+        e = (x);                                                   \
+        if (e != cudaSuccess) return h->cuda_fail(e, #x);          \
+    } while (0)
+    GR_CK(gw->a_ops.ensure(size_t(n_tiles) * kTileM * KE * T::kElem));
+    GR_CK(gw->b_ops.ensure(size_t(n_chunks) * N * KE * T::kElem));
+    GR_CK(gw->w_ops.ensure(size_t(n_chunks) * kUsers2 * KE2 * T::kElem));
+    GR_CK(gw->xn.ensure(size_t(n_tiles) * kTileM));
+    GR_CK(gw->dn.ensure(Mpad));
+    GR_CK(gw->part.ensure(size_t(splits) * U * ns));
+    GR_CK(gw->err.ensure(1));
+    GR_CK(cudaMemsetAsync(gw->err.p, 0, sizeof(int), s));
+    GR_CK(cudaMemsetAsync(gw->dn.p, 0, sizeof(float) * Mpad, s));
+
+    const int threads = 256;
+    gram_pack_kernel<MODE><<<std::min(4096, (n_tiles * kTileM * Kp + threads - 1) / threads), threads, 0, s>>>(
+        h->xs.p, ns, Dp, D, Kp, kTileM, n_tiles, gw->a_ops.p, gw->xn.p);
+    GR_CK(cudaGetLastError());
+    gram_pack_kernel<MODE><<<std::min(4096, (n_chunks * N * Kp + threads - 1) / threads), threads, 0, s>>>(
+        h->dict_X.p, M, Dp, D, Kp, N, n_chunks, gw->b_ops.p, gw->dn.p);
+    GR_CK(cudaGetLastError());
+    gram_pack_w_kernel<MODE><<<std::min(4096, (n_chunks * kUsers2 * N + threads - 1) / threads), threads, 0, s>>>(
+        h->dict_a.p, h->cap, U, M, N, n_chunks, h->cfg.wG, gw->w_ops.p);
+    GR_CK(cudaGetLastError());
+
+    Gram2Args ga;
+    ga.a_ops = gw->a_ops.p;
+    ga.b_ops = gw->b_ops.p;
+    ga.w_ops = gw->w_ops.p;
+    ga.xn = gw->xn.p;
+    ga.dn = gw->dn.p;
+    ga.part = gw->part.p;
+    ga.err = gw->err.p;
+    ga.n_samples = ns;
+    ga.users = U;
+    ga.Kp = Kp;
+    ga.N = N;
+    ga.chunks_per_split = cps;
+    ga.n_chunks = n_chunks;
+    ga.stages = stages;
+    ga.ewl2 = h->model_params().ew * 1.4426950408889634f;
+    // >= 120 KB keeps one CTA per SM: its tensor memory (up to 512 columns) is never contended
+    const size_t smem = std::max<size_t>(gram2_smem<MODE>(Kp, N, stages) + 1024, 120 * 1024);
+    GR_CK(cudaFuncSetAttribute(gram_detect2_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    gram_detect2_kernel<MODE><<<dim3(n_tiles, splits), kThreads, smem, s>>>(ga);
+    GR_CK(cudaGetLastError());
+    gram_finish_kernel<<<(ns + kFinSamples - 1) / kFinSamples, kFinWarps * 32, 0, s>>>(
+        h->xs.p, Dp, D, h->w.p, h->cfg.wL, gw->part.p, splits, U, ns, d_out, size_t(ns));
+    GR_CK(cudaGetLastError());
+    GR_CK(cudaMemcpyAsync(gw->h_err, gw->err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+#undef GR_CK
+    return APSM_OK;
 }
 
 template <int MODE>
@@ -379,6 +737,14 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     }
     const int Kp = int(round_up(uint32_t(D), uint32_t(T::kStepK)));
     const int KE = T::kSplit ? 2 * Kp : Kp;
+    if (MODE == kBF16 && U >= 4 && !h->gram_one_product) {
+        // the users' contraction on the tensor cores where its operands fit shared memory; only
+        // in the BF16 form, whose kernel values and coefficients may be BF16 too (in the other
+        // forms the second product's rounding would cost more accuracy than its time saves)
+        for (int n2 = 256; n2 >= 32; n2 /= 2)
+            for (int st2 = kMaxStages; st2 >= 2; --st2)
+                if (gram2_smem<MODE>(Kp, n2, st2) + 1024 <= 220 * 1024) return run_gram2<MODE>(h, S, d_out, s, Kp, n2, st2);
+    }
     // dictionary chunk width and stages: the data tile and the chunk ring within shared memory
     // (chunks of 256 down to 64 columns in 3 stages, then 32 columns in 3 or 2 stages)
     int N = 256, stages = kMaxStages;

@@ -87,3 +87,26 @@ def test_copy_state_takes_heuristic_variance_and_continues_training(oracle_mod):
     a.train(g.rx_train, g.tx_train[0])
     b.train(g.rx_train, g.tx_train[0])
     np.testing.assert_array_equal(a.detect(f.rx_data)[0], b.detect(f.rx_data)[0])
+
+
+def test_bf16_two_product_form_matches_one_product(monkeypatch):
+    # 4+ users in the BF16 form contract on the tensor cores (kernel values and
+    # coefficients in BF16); APSM_GRAM_ONE_PRODUCT=1 keeps the users' sums on the
+    # CUDA cores.  Both stay within the BF16 bound of the float64 model; against each
+    # other they agree to the BF16 rounding of the second product.
+    f = synth.generate_frame(46, K=8, N=32, P=400, S=700, modulation="QAM16", snr_db=15)
+    cfg = dict(BASE, detectVersion="gram_bf16")
+    base = L.NomaDetectorFactory.build(BASE, 32, num_users=8)
+    base.train(f.rx_train, f.tx_train)
+    two = L.NomaDetectorFactory.build(cfg, 32, num_users=8)
+    two.copy_state_from(base)
+    monkeypatch.setenv("APSM_GRAM_ONE_PRODUCT", "1")
+    one = L.NomaDetectorFactory.build(cfg, 32, num_users=8)
+    one.copy_state_from(base)
+    e2, _ = two.detect(f.rx_data)
+    e1, _ = one.detect(f.rx_data)
+    scale = float(np.max(np.abs(e1)))
+    err = float(np.max(np.abs(e2 - e1))) / scale
+    assert 0 < err < 1e-3, err
+    for _ in range(2):  # repeatable
+        np.testing.assert_array_equal(two.detect(f.rx_data)[0], e2)
