@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(kFinWarps * 32)
 // exponential and a store per kernel value instead of one FMA per user; the
 // second product rounds P and W to the operand format (split modes: hi/lo, 3
 // products).  Used for the BF16 form with 4 or more users: at N = 64, 16
-// users, a 65536-symbol detection takes 2.54 ms instead of 3.21 ms, the soft
+// users, a 65536-symbol detection takes 1.66 ms instead of 3.21 ms, the soft
 // outputs moving from 1.4e-6 to 5.2e-5 of the largest output away from the
 // float64 model (decisions unchanged); the TF32 form gains 2 % for a 10x
 // larger error and the split forms lose time (larger P buffers, 3 products),
@@ -578,18 +578,31 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect2_kernel(Gram2Args g)
                 for (int j0 = 0; j0 < 16; j0 += T::kChunk) {
                     // one 16-byte K chunk of this row: hi, and lo for split modes
                     uint32_t hw[4] = {0u, 0u, 0u, 0u}, lw[4] = {0u, 0u, 0u, 0u};
+                    float kv[T::kChunk];
 #pragma unroll
                     for (int e = 0; e < T::kChunk; ++e) {
                         const int j = j0 + e;
-                        const float kv = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j], xn + dn[col + j]), 0.f));
-                        float hi, lo;
-                        split_operand<MODE>(kv, &hi, &lo);
-                        if constexpr (T::kTF) {
-                            hw[e] = __float_as_uint(hi);
-                            lw[e] = __float_as_uint(lo);
-                        } else {
-                            hw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(hi))) << (16 * (e & 1));
-                            lw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(lo))) << (16 * (e & 1));
+                        kv[e] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j], xn + dn[col + j]), 0.f));
+                    }
+                    if constexpr (MODE == kBF16) {
+                        // pairs converted by one instruction each (round to nearest)
+#pragma unroll
+                        for (int e = 0; e < T::kChunk; e += 2) {
+                            const __nv_bfloat162 v2 = __floats2bfloat162_rn(kv[e], kv[e + 1]);
+                            hw[e >> 1] = *reinterpret_cast<const uint32_t*>(&v2);
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < T::kChunk; ++e) {
+                            float hi, lo;
+                            split_operand<MODE>(kv[e], &hi, &lo);
+                            if constexpr (T::kTF) {
+                                hw[e] = __float_as_uint(hi);
+                                lw[e] = __float_as_uint(lo);
+                            } else {
+                                hw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(hi))) << (16 * (e & 1));
+                                lw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(lo))) << (16 * (e & 1));
+                            }
                         }
                     }
                     const int kc = (col + j0) / T::kChunk;
