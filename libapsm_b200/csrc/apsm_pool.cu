@@ -9,6 +9,7 @@
 // columns, the persistent sweep, universe tail -> dictionary copies, then the
 // detection launches (one per antenna class).
 #include "apsm_batch.cuh"
+#include <cuda.h>
 #include "apsm_host.hpp"
 #include "apsm_tc.cuh"
 
@@ -90,6 +91,39 @@ double host_us()
 }
 
 // Page-locked host memory (cudaMallocHost or cudaHostRegister): copies need no staging.
+// A device address for the bytes [p, p + bytes) when they lie inside one page-locked host
+// allocation mapped for the device (kernels then read them over the bus); nullptr otherwise.
+const void* device_view(const void* p, size_t bytes)
+{
+    if (!p || bytes == 0) return nullptr;
+    // the driver's pointer query, looked up through the runtime (the library links no libcuda)
+    using PtrAttrFn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+    static PtrAttrFn cuPointerGetAttribute = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            fn = nullptr;
+        }
+        return reinterpret_cast<PtrAttrFn>(fn);
+    }();
+    if (!cuPointerGetAttribute) return nullptr;
+    const CUdeviceptr a = CUdeviceptr(reinterpret_cast<uintptr_t>(p));
+    unsigned int type = 0;
+    CUdeviceptr start = 0, dptr = 0;
+    size_t size = 0;
+    if (cuPointerGetAttribute(&type, CU_POINTER_ATTRIBUTE_MEMORY_TYPE, a) != CUDA_SUCCESS || type != CU_MEMORYTYPE_HOST)
+        return nullptr;
+    if (cuPointerGetAttribute(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, a) != CUDA_SUCCESS ||
+        cuPointerGetAttribute(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, a) != CUDA_SUCCESS)
+        return nullptr;
+    if (a < start || a - start > size || bytes > size - (a - start)) return nullptr;
+    if (cuPointerGetAttribute(&dptr, CU_POINTER_ATTRIBUTE_DEVICE_POINTER, a) != CUDA_SUCCESS || dptr == 0)
+        return nullptr;
+    return reinterpret_cast<const void*>(dptr);
+}
+
 bool is_pinned(const void* p)
 {
     cudaPointerAttributes a;
@@ -219,6 +253,7 @@ private:
 };
 
 constexpr size_t kDirectOutJobs = 16; // detection jobs whose estimates are copied to the caller one by one
+constexpr size_t kZeroCopyMin = size_t(4) << 20; // training inputs read in place from this many bytes on
 constexpr size_t kArenaJobs = 32;     // training jobs from which a batch reads its step lists from the arena
 
 int detect_class(uint32_t N)
@@ -363,6 +398,8 @@ struct TrainPlan {
     uint32_t job = 0; // index in the caller's list
     PoolDet* det = nullptr;
     const std::vector<TrainStep>* steps = nullptr; // the pool's cached schedule for (rows before, P)
+    const void* zc_rx = nullptr; // host-buffer batch: the caller's pilots as the device reads them in place
+    const void* zc_tx = nullptr;
     long long* steps_dev = nullptr; // its offset in the pool's device schedule arena (-1: not there)
     int final_hi = 0;
     uint32_t P = 0, usedP = 0, nP = 0, n_first = 0;
@@ -592,6 +629,22 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     size_t nCopyIn = 0;
     for (const auto& t : tp) nCopyIn += t.usedP > 0;
     const size_t nPack = nT; // detection reads the samples as the caller holds them
+    // Training inputs of a large host-buffer batch in page-locked, device-mapped buffers are
+    // read in place by the packing kernel (no staging copy, no upload); small batches stage
+    // them (a copy of a few KB costs less than reading them over the bus).
+    bool zc_train = false;
+    if (host && nT > 0) {
+        size_t bytes = 0;
+        for (const auto& t : tp) bytes += sizeof(float2) * (size_t(t.det->N) + 1) * t.P;
+        zc_train = bytes >= kZeroCopyMin;
+        for (auto& t : tp) {
+            if (!zc_train) break;
+            const apsm_job& j = jobs[t.job];
+            t.zc_rx = device_view(j.rx, sizeof(float2) * size_t(t.det->N) * t.P);
+            t.zc_tx = device_view(j.tx, sizeof(float2) * t.P);
+            zc_train = t.zc_rx && t.zc_tx;
+        }
+    }
     // descriptor region
     size_t o = 0;
     const size_t off_tj = o; o = align_up(o + sizeof(BatchTrainJob) * nT, 256);
@@ -631,10 +684,11 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     o = align_up(o, 256);
     const size_t dcnt_bytes = o - off_dcnt;
     if (host) { // staged host inputs travel with the descriptors
-        for (auto& t : tp) {
-            t.off_rx = o; o = align_up(o + sizeof(float2) * size_t(t.det->N) * t.P, 16);
-            t.off_tx = o; o = align_up(o + sizeof(float2) * t.P, 16);
-        }
+        if (!zc_train)
+            for (auto& t : tp) {
+                t.off_rx = o; o = align_up(o + sizeof(float2) * size_t(t.det->N) * t.P, 16);
+                t.off_tx = o; o = align_up(o + sizeof(float2) * t.P, 16);
+            }
         for (auto& d : dp) {
             d.off_rx = o;
             o = align_up(o + sizeof(float2) * size_t(d.det->N) * d.S, 16);
@@ -737,11 +791,12 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     std::vector<HostIn> ins;
     bool direct = false;
     if (host) {
-        for (const auto& t : tp) {
-            const apsm_job& j = jobs[t.job];
-            ins.push_back({j.rx, t.off_rx, sizeof(float2) * size_t(t.det->N) * t.P, false});
-            ins.push_back({j.tx, t.off_tx, sizeof(float2) * t.P, false});
-        }
+        if (!zc_train)
+            for (const auto& t : tp) {
+                const apsm_job& j = jobs[t.job];
+                ins.push_back({j.rx, t.off_rx, sizeof(float2) * size_t(t.det->N) * t.P, false});
+                ins.push_back({j.tx, t.off_tx, sizeof(float2) * t.P, false});
+            }
         for (const auto& q : dp)
             ins.push_back({jobs[q.job].rx, q.off_rx, sizeof(float2) * size_t(q.det->N) * q.S, true});
         // small batches travel in the one descriptor upload even from page-locked buffers: a
@@ -777,8 +832,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         PoolDet& d = *t.det;
         const apsm_job& j = jobs[t.job];
         if (!arena) std::memcpy(hst + t.off_steps, t.steps->data(), sizeof(TrainStep) * t.steps->size());
-        const float2* rx = host ? reinterpret_cast<const float2*>(D(t.off_rx)) : reinterpret_cast<const float2*>(j.rx);
-        const float2* tx = host ? reinterpret_cast<const float2*>(D(t.off_tx)) : reinterpret_cast<const float2*>(j.tx);
+        const float2* rx = !host ? reinterpret_cast<const float2*>(j.rx)
+                                 : zc_train ? static_cast<const float2*>(t.zc_rx) : reinterpret_cast<const float2*>(D(t.off_rx));
+        const float2* tx = !host ? reinterpret_cast<const float2*>(j.tx)
+                                 : zc_train ? static_cast<const float2*>(t.zc_tx) : reinterpret_cast<const float2*>(D(t.off_tx));
         auto* Y = reinterpret_cast<float2*>(D(t.off_Y));
         auto* nrm = reinterpret_cast<float*>(D(t.off_nrm));
         auto* yv = reinterpret_cast<float*>(D(t.off_y));

@@ -312,3 +312,38 @@ def test_pool_reserve_runs_nothing(native_lib):
     ref = ref_pool.run(batch(ref_pool, ids2), lane=1)
     for k in range(2, 4):
         np.testing.assert_array_equal(outs[k], ref[k])
+
+
+def test_pool_page_locked_training_inputs_read_in_place(native_lib):
+    """A host-buffer batch whose training inputs (>= 4 MB) sit in page-locked
+    memory has them read in place by the packing kernel; the estimates equal
+    those of the same batch from pageable buffers (staged and uploaded)."""
+    import torch
+
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    specs = [(32, 1800, 600), (16, 1500, 900), (8, 1900, 300), (32, 1700, 200)]
+    frames = [(N,) + _frame(600 + i, N, P, S) for i, (N, P, S) in enumerate(specs)]
+    pinned = []
+
+    def pin(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        pinned.append(t)
+        return t.numpy()
+
+    outs = {}
+    for mode in ("pageable", "page-locked"):
+        pool = DetectorPool(dict(CFG, windowSize=80, dictionarySize=2000, detectVersion="gram_tf32x3"))
+        ids = [pool.add(f[0]) for f in frames]
+        # enough detectors of the same frames for 4 MB of training inputs in one batch
+        reps = 8
+        more = [pool.add(f[0]) for _ in range(reps - 1) for f in frames]
+        all_ids = ids + more
+        all_frames = frames * reps
+        conv = (lambda a: a) if mode == "pageable" else pin
+        jobs = ([PoolJob(d, conv(f[1]), conv(f[2]), fresh=True) for d, f in zip(all_ids, all_frames)] +
+                [PoolJob(d, conv(f[3]), est=conv(np.zeros(f[3].shape[1], np.complex64))) for d, f in zip(all_ids, all_frames)])
+        res = pool.run(jobs)
+        outs[mode] = [res[len(all_ids) + k] for k in range(len(all_ids))]
+    for a, b in zip(outs["pageable"], outs["page-locked"]):
+        np.testing.assert_array_equal(a, b)
