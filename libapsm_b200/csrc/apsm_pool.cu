@@ -423,6 +423,7 @@ struct DetectPlan {
     bool gram = false; // tensor-core (tcgen05) form
     int Kp = 0, tiles = 0, chunks = 0;
     size_t off_rx = 0, off_Y = 0, off_nrm = 0, off_est = 0;
+    void* zc_est = nullptr; // host-buffer batch: the caller's estimates as the device writes them in place
     size_t off_aops = 0, off_bops = 0, off_bx = 0, off_lin = 0;
     size_t off_part = 0, off_cnt = 0; // split CUDA-core launches: chunk sums, tile counters
 };
@@ -645,6 +646,19 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             zc_train = t.zc_rx && t.zc_tx;
         }
     }
+    // Estimates of a large host-buffer batch into page-locked, device-mapped buffers are written
+    // there by the detection kernels (no copy back, no scatter).
+    bool zc_est = false;
+    if (host && nD > 0) {
+        size_t bytes = 0;
+        for (const auto& q : dp) bytes += sizeof(float2) * q.S;
+        zc_est = bytes >= kZeroCopyMin;
+        for (auto& q : dp) {
+            if (!zc_est) break;
+            q.zc_est = const_cast<void*>(device_view(jobs[q.job].est, sizeof(float2) * q.S));
+            zc_est = q.zc_est != nullptr;
+        }
+    }
     // descriptor region
     size_t o = 0;
     const size_t off_tj = o; o = align_up(o + sizeof(BatchTrainJob) * nT, 256);
@@ -726,7 +740,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         }
     }
     const size_t est_begin = o;
-    if (host)
+    if (host && !zc_est)
         for (auto& d : dp) {
             d.off_est = o;
             o = align_up(o + sizeof(float2) * d.S, 16);
@@ -888,7 +902,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         const apsm_job& j = jobs[q.job];
         const float2* rx = host ? reinterpret_cast<const float2*>(D(q.off_rx)) : reinterpret_cast<const float2*>(j.rx);
         auto* ns = q.gram ? reinterpret_cast<float*>(D(q.off_nrm)) : nullptr;
-        float2* out = host ? reinterpret_cast<float2*>(D(q.off_est)) : reinterpret_cast<float2*>(j.est);
+        float2* out = !host ? reinterpret_cast<float2*>(j.est)
+                            : zc_est ? static_cast<float2*>(q.zc_est) : reinterpret_cast<float2*>(D(q.off_est));
         const bool split = det_parts > 1 && !q.gram;
         h_dj[k] = BatchDetectJob{rx,       d.Y,       d.nrm, d.a,  d.w, out, int(q.S), int(q.Mp), int(d.N), int(d.Np),
                                  d.ew,     split ? reinterpret_cast<float2*>(D(q.off_part)) : nullptr,

@@ -347,3 +347,32 @@ def test_pool_page_locked_training_inputs_read_in_place(native_lib):
         outs[mode] = [res[len(all_ids) + k] for k in range(len(all_ids))]
     for a, b in zip(outs["pageable"], outs["page-locked"]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_pool_page_locked_estimates_written_in_place(native_lib):
+    """Estimates (>= 4 MB) of a host-buffer batch into page-locked buffers are
+    written there by the detection kernels; they equal those of the same batch
+    with pageable outputs (copied back and scattered)."""
+    import torch
+
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    frames = [(N,) + _frame(700 + i, N, 200, 10000) for i, N in enumerate([4, 8, 16, 32])]
+    outs = {}
+    for mode in ("pageable", "page-locked"):
+        pool = DetectorPool(dict(CFG, detectVersion="gram_tf32x3"))
+        dets = [(pool.add(f[0]), f) for _ in range(16) for f in frames]  # 64 detectors, 5 MB of estimates
+        pool.run([PoolJob(d, f[1], f[2]) for d, f in dets])
+        ests = []
+        for d, f in dets:
+            e = np.zeros(f[3].shape[1], np.complex64)
+            if mode == "page-locked":
+                t = torch.from_numpy(e).pin_memory()
+                ests.append(t)
+                e = t.numpy()
+            ests.append(e)
+        arrays = [e for e in ests if isinstance(e, np.ndarray)]
+        res = pool.run([PoolJob(d, f[3], est=e) for (d, f), e in zip(dets, arrays)])
+        outs[mode] = [np.array(r) for r in res]
+    for a, b in zip(outs["pageable"], outs["page-locked"]):
+        np.testing.assert_array_equal(a, b)
