@@ -143,9 +143,12 @@ struct BatchCopyJob {
 cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s);
 cudaError_t launch_batch_copy(const BatchCopyJob* d_jobs, int n_jobs, int max_pairs, int max_np, cudaStream_t s);
 // row_split: blocks per column group, each taking every row_split-th pass of
-// kColRows column entries (entries are computed alike whatever the split)
-cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, int n_jobs, int max_cols, int max_n, int row_split,
-                              BatchCommon cm, cudaStream_t s);
+// kColRows column entries (entries are computed alike whatever the split).
+// order (device, n_jobs entries, or null for 0..n_jobs-1): the jobs of the
+// launch as indices into d_jobs; the pool launches one antenna class at a
+// time, so each launch's kernel keeps rows of its class's size in registers.
+cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, const int* order, int n_jobs, int max_cols, int max_n,
+                              int row_split, BatchCommon cm, cudaStream_t s);
 int batch_kcol_group(); // columns per block
 int batch_kcol_rows();  // column entries per block pass
 size_t batch_sweep_smem(const BatchCommon& cm);

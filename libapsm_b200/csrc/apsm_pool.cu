@@ -666,6 +666,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     const size_t off_pj = o; o = align_up(o + sizeof(BatchPackJob) * nPack, 256);
     const size_t off_ci = o; o = align_up(o + sizeof(BatchCopyJob) * nCopyIn, 256);
     const size_t off_co = o; o = align_up(o + sizeof(BatchCopyJob) * nT, 256);
+    const size_t off_ko = o; o = align_up(o + sizeof(int) * nT, 256); // training jobs by antenna class
     const size_t off_gj = o; o = align_up(o + sizeof(BatchGramJob) * nG, 256);
     const size_t off_gp = o; o = align_up(o + sizeof(int) * (nG + nGcls), 256);
     if (!arena)
@@ -840,7 +841,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     auto* h_ci = reinterpret_cast<BatchCopyJob*>(hst + off_ci);
     auto* h_co = reinterpret_cast<BatchCopyJob*>(hst + off_co);
     size_t ipack = 0, icopy = 0;
-    int max_len = 0, max_np = 1, max_cols = 0, max_n = 1, max_pairs_in = 0, max_pairs_out = 0;
+    int max_len = 0, max_np = 1, max_n = 1, max_pairs_in = 0, max_pairs_out = 0;
     for (size_t k = 0; k < nT; ++k) {
         TrainPlan& t = tp[k];
         PoolDet& d = *t.det;
@@ -889,13 +890,31 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         tj.pro_hi = int(t.usedP);
         tj.pro_stride = t.pro_stride;
         h_tj[k] = tj;
-        max_cols = std::max(max_cols, int(t.nP - t.n_first));
         h_co[k] = BatchCopyJob{Y + size_t(t.lo_new) * d.Np, nrm + t.lo_new, yv + 2 * t.lo_new, av + 2 * t.lo_new,
                                d.Y, d.nrm, d.y, d.a, int(t.usedP_new), int(d.Np)};
         max_pairs_out = std::max(max_pairs_out, int(t.usedP_new));
     }
     for (auto& kv : perm_off) std::memcpy(hst + kv.second, perms[kv.first].data(), sizeof(int) * kv.first);
     const size_t pack_train = ipack;
+    // kernel-column launches, one per antenna class (rows of the class's size in registers)
+    struct KcolClass {
+        int first = 0, count = 0, max_cols = 0, max_n = 1;
+    };
+    KcolClass kcls[5];
+    {
+        auto cls_of = [](int n) { return n <= 4 ? 0 : n <= 8 ? 1 : n <= 16 ? 2 : n <= 32 ? 3 : 4; };
+        for (size_t k = 0; k < nT; ++k) ++kcls[cls_of(int(tp[k].det->N))].count;
+        for (int c = 1; c < 5; ++c) kcls[c].first = kcls[c - 1].first + kcls[c - 1].count;
+        int fill[5];
+        for (int c = 0; c < 5; ++c) fill[c] = kcls[c].first;
+        auto* h_ko = reinterpret_cast<int*>(hst + off_ko);
+        for (size_t k = 0; k < nT; ++k) {
+            KcolClass& kc = kcls[cls_of(int(tp[k].det->N))];
+            h_ko[fill[cls_of(int(tp[k].det->N))]++] = int(k);
+            kc.max_cols = std::max(kc.max_cols, int(tp[k].nP - tp[k].n_first));
+            kc.max_n = std::max(kc.max_n, int(tp[k].det->N));
+        }
+    }
     for (size_t k = 0; k < nD; ++k) {
         DetectPlan& q = dp[k];
         PoolDet& d = *q.det;
@@ -999,16 +1018,19 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     if (trace) POOL_CK(cudaEventRecord(L.tr[2], s));
     if (nT > 0) {
         const auto* d_tj = reinterpret_cast<const BatchTrainJob*>(D(off_tj));
-        // small batches (single train requests): spread each column group's rows over blocks
-        int row_split = 1;
-        {
-            const long long blocks = (long long)nT * ((max_cols + batch_kcol_group() - 1) / batch_kcol_group());
+        const int* d_ko = reinterpret_cast<const int*>(D(off_ko));
+        for (const KcolClass& kc : kcls) {
+            if (kc.count == 0 || kc.max_cols <= 0) continue;
+            // small launches (single train requests): spread each column group's rows over blocks
+            int row_split = 1;
+            const long long blocks = (long long)kc.count * ((kc.max_cols + batch_kcol_group() - 1) / batch_kcol_group());
             const int passes = int((int(cfg.dict_size) + cm.qP + batch_kcol_rows() - 1) / batch_kcol_rows());
             const long long target = 4LL * std::max(1, sms);
-            if (blocks > 0 && blocks < target)
+            if (blocks < target)
                 row_split = int(std::min<long long>(std::max(passes, 1), (target + blocks - 1) / blocks));
+            POOL_CK(launch_batch_kcol(d_tj, d_ko + kc.first, kc.count, kc.max_cols, kc.max_n, row_split, cm, s));
+            ++L.launches;
         }
-        POOL_CK(launch_batch_kcol(d_tj, int(nT), max_cols, max_n, row_split, cm, s));
         if (trace) POOL_CK(cudaEventRecord(L.tr[3], s));
         const int per_sm = shape.sweep_per_sm > 0 ? std::min(shape.sweep_per_sm, sweep_ctas) : sweep_ctas;
         const int grid = int(std::min<size_t>(nT, size_t(per_sm) * sms));
@@ -1017,7 +1039,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         if (timing) POOL_CK(cudaEventRecord(L.ev[5], s));
         if (trace) POOL_CK(cudaEventRecord(L.tr[4], s));
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_co)), int(nT), max_pairs_out, max_np, s));
-        L.launches += (max_cols > 0) + 1 + (max_pairs_out > 0);
+        L.launches += 1 + (max_pairs_out > 0);
         if (timing) POOL_CK(cudaEventRecord(L.ev[1], s));
         for (const auto& t : tp) t.det->used = 2 * t.usedP_new;
     } else if (trace) {

@@ -29,10 +29,10 @@ __device__ __forceinline__ float ex2_approx(float x)
 // in registers (NMAX >= N antennas of every job of the launch).
 template <int NMAX>
 __global__ void __launch_bounds__(kColRows)
-    batch_kcol_kernel(const BatchTrainJob* __restrict__ jobs, BatchCommon cm)
+    batch_kcol_kernel(const BatchTrainJob* __restrict__ jobs, const int* __restrict__ order, BatchCommon cm)
 {
     // the job's fields in registers: the column stores below cannot alias them then
-    const BatchTrainJob& jg = jobs[blockIdx.y];
+    const BatchTrainJob& jg = jobs[order ? order[blockIdx.y] : int(blockIdx.y)];
     const int nP = jg.nP, N = jg.N, Np = jg.Np, capP = jg.capP, qP = cm.qP;
     const int n_first = jg.n_first;
     const int n0 = n_first + blockIdx.x * kColGroup;
@@ -167,15 +167,16 @@ __global__ void __launch_bounds__(kColRows)
 int batch_kcol_group() { return kColGroup; }
 int batch_kcol_rows() { return kColRows; }
 
-cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, int n_jobs, int max_cols, int max_n, int row_split,
-                              BatchCommon cm, cudaStream_t s)
+cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, const int* order, int n_jobs, int max_cols, int max_n,
+                              int row_split, BatchCommon cm, cudaStream_t s)
 {
     if (n_jobs <= 0 || max_cols <= 0) return cudaSuccess;
     dim3 grid((max_cols + kColGroup - 1) / kColGroup, n_jobs, row_split > 1 ? row_split : 1);
-    if (max_n <= 8) batch_kcol_kernel<8><<<grid, kColRows, 0, s>>>(d_jobs, cm);
-    else if (max_n <= 16) batch_kcol_kernel<16><<<grid, kColRows, 0, s>>>(d_jobs, cm);
-    else if (max_n <= 32) batch_kcol_kernel<32><<<grid, kColRows, 0, s>>>(d_jobs, cm);
-    else if (max_n <= 64) batch_kcol_kernel<64><<<grid, kColRows, 0, s>>>(d_jobs, cm);
+    if (max_n <= 4) batch_kcol_kernel<4><<<grid, kColRows, 0, s>>>(d_jobs, order, cm);
+    else if (max_n <= 8) batch_kcol_kernel<8><<<grid, kColRows, 0, s>>>(d_jobs, order, cm);
+    else if (max_n <= 16) batch_kcol_kernel<16><<<grid, kColRows, 0, s>>>(d_jobs, order, cm);
+    else if (max_n <= 32) batch_kcol_kernel<32><<<grid, kColRows, 0, s>>>(d_jobs, order, cm);
+    else if (max_n <= 64) batch_kcol_kernel<64><<<grid, kColRows, 0, s>>>(d_jobs, order, cm);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
