@@ -55,7 +55,7 @@ UNIT = "symbols/s"
 N_DET = 512
 # DRAM bytes per algorithmic byte of the batched sweep (ncu capture of the first
 # 32 detectors: 367.8 MB read + 4.6 MB written for 361.3 MB algorithmic)
-SWEEP_TRAFFIC_PER_ALG_BYTE = (367.794176 + 4.560128) / 361.273728
+SWEEP_TRAFFIC_PER_ALG_BYTE = (368.360704 + 4.627968) / 361.273728
 WORKLOAD = {"workload": "512 detectors: N~U{4,8,16,32}, P~U[200,2000], S~U[1000,16000], SNR~U[10,25] dB, "
                         "QPSK/16QAM, window 80, dictionary 2000, fresh train + detect per step",
             "detectors": N_DET, "window": 80, "dictionary": 2000, "detect": "gram_tf32x3 (FP32-accurate)",
@@ -257,7 +257,7 @@ def run_batched(args, rank: int, world: int) -> dict | None:
                      "traffic": alg * SWEEP_TRAFFIC_PER_ALG_BYTE, "algorithmic_bytes_per_launch": alg,
                      "launch_ms": sweep,
                      "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of the "
-                                       "32-detector case (372.4 MB for 361.3 MB algorithmic), scaled to this "
+                                       "32-detector case (373.0 MB for 361.3 MB algorithmic), scaled to this "
                                        "launch by its algorithmic bytes",
                      "note": "a chain of P dependent steps per detector: latency / shared-memory bound, "
                              "not HBM; see profiles/",
