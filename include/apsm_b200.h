@@ -189,6 +189,18 @@ apsm_status apsm_last_kernel_ms(apsm_detector* h, float* sweep_ms, float* detect
 /* Last error message of the handle ("" if none). */
 const char* apsm_last_error(const apsm_detector* h);
 
+/* Limit of the bounded waits inside the tensor-core detection kernels
+ * (nanoseconds, process-wide; 2 s by default).  No counterpart in the
+ * reference, whose CUDA errors end the process (CUDA_CHECK,
+ * cpp/lib/cuda/cuda_errorhandling.cuh:98-108).  A kernel whose wait expires
+ * stops its work, still waits for its own copies and tensor-core products,
+ * releases tensor memory and flags the call, which returns APSM_ERR_CUDA; the
+ * handle stays usable.  0 makes every wait that is not already complete give
+ * up at once: a way to test the expiry path.  Launches read the value when
+ * they are issued. */
+void apsm_set_wait_limit_ns(uint64_t ns);
+uint64_t apsm_wait_limit_ns(void);
+
 /* ======================================================================
  * Detector pool: many resident detectors (users x cells), batched jobs.
  *

@@ -58,6 +58,8 @@ SIGNATURES = [
     ("apsm_copy_state", ctypes.c_int, [_P, _P]),
     ("apsm_last_kernel_ms", ctypes.c_int, [_P, _F, _F]),
     ("apsm_last_error", ctypes.c_char_p, [_P]),
+    ("apsm_set_wait_limit_ns", None, [ctypes.c_uint64]),
+    ("apsm_wait_limit_ns", ctypes.c_uint64, []),
     # detector pool (batched many-detector form)
     ("apsm_pool_create", ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, _U32, ctypes.POINTER(_P), ctypes.c_char_p,
                                         ctypes.c_size_t]),

@@ -6,6 +6,7 @@
 #include "apsm_host.hpp"
 #include "json_lite.hpp"
 
+#include <atomic>
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -185,6 +186,16 @@ static void copy_err(char* err, size_t errlen, const std::string& msg)
 }
 
 extern "C" const char* apsm_version(void) { return "apsm_b200 0.1.0 (sm_100a)"; }
+
+namespace {
+std::atomic<unsigned long long> g_wait_limit_ns{2000000000ull};
+}
+
+unsigned long long apsm::wait_limit_ns() { return g_wait_limit_ns.load(std::memory_order_relaxed); }
+
+extern "C" void apsm_set_wait_limit_ns(uint64_t ns) { g_wait_limit_ns.store(ns, std::memory_order_relaxed); }
+
+extern "C" uint64_t apsm_wait_limit_ns(void) { return g_wait_limit_ns.load(std::memory_order_relaxed); }
 
 extern "C" apsm_status apsm_create(const char* algorithm_json, uint32_t num_antennas, uint32_t num_users,
                                    apsm_detector** out, char* err, size_t errlen)

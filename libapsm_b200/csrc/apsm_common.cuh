@@ -32,6 +32,10 @@ struct TrainStep {
 
 __host__ __device__ inline uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
 
+// Limit (ns) of the bounded barrier waits of the tensor-core kernels, read by
+// their launchers (apsm_set_wait_limit_ns; 2 s unless changed).
+unsigned long long wait_limit_ns();
+
 // Row pitch (floats) of dictionary / sample rows in HBM: D padded to 4 so
 // that every row starts 16-byte aligned.
 __host__ __device__ inline uint32_t row_pitch(uint32_t D) { return round_up(D, 4); }

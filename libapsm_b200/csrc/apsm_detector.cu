@@ -637,6 +637,8 @@ apsm_status apsm_detector::detect_host(const float2* rx, uint32_t S, float2* est
     APSM_CK(cudaEventRecord(ev1, stream));
     APSM_CK(cudaMemcpyAsync(est, est_stage.p, sizeof(float2) * size_t(U) * S, cudaMemcpyDeviceToHost, stream));
     APSM_CK(cudaStreamSynchronize(stream));
+    st = detect_gram_check(this);
+    if (st != APSM_OK) return st;
     if (ms) APSM_CK(cudaEventElapsedTime(ms, ev0, ev1));
     return APSM_OK;
 }

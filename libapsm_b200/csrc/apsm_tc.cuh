@@ -86,16 +86,37 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-// Bounded wait (2 s): false (and *abort set) when the barrier did not complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort)
+// Non-blocking test of a barrier phase.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity)
 {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Bounded wait (limit_ns, 2 s by default): false (and *abort set) when the
+// barrier did not complete in time.  limit_ns == 0 gives up at once unless the
+// phase is already complete (a test of the expiry path).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                          unsigned long long limit_ns = kWaitLimitNs)
+{
+    if (limit_ns == 0) {
+        if (mbar_test_wait(bar, parity)) return true;
+        *abort = 1;
+        return false;
+    }
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (;;) {
         for (int i = 0; i < 64; ++i)
             if (mbar_try_wait(bar, parity)) return true;
         if (*abort) return false;
-        if (global_ns() - t0 > kWaitLimitNs) break;
+        if (global_ns() - t0 > limit_ns) break;
     }
     *abort = 1;
     return false;

@@ -19,6 +19,19 @@
 // the dictionary chunks), warp 9 TMEM allocator and MMA issuer.  Every
 // mbarrier wait is bounded; on expiry the CTA records an error, still waits
 // for its own copies and MMAs, releases tensor memory and returns.
+//
+// Compensated cross terms (single-product forms bf16 / tf32).  Rounding both
+// operands to the format's unit u perturbs r and m by at most 2u |x||y|, so a
+// base-2 exponent es + m2 r (es = ew log2(e) (|x|^2 + |y|^2) <= 0) moves by at
+// most 2u |es| and the pair's contribution to the two soft outputs by at most
+//   (|a_2b| + |a_2b+1|) wG * max(kA, kP, kM) * ln 2 * 2u |es|.
+// Where cancellation bites (near-duplicate points: r ~ (|x|^2 + |y|^2) / 2,
+// kernel values near 1) that bound is large; the epilogue flags every pair
+// whose bound exceeds kFixEps, leaves it out of the tensor-core sums and adds
+// it back with r and m recomputed exactly in FP32 from the samples.  Per pair
+// the chunk data carries fw = (|a_2b| + |a_2b+1|) wG ln2 2u / kFixEps, and per
+// chunk max fw and max fw |ew2 |y|^2|, so a warp whose samples cannot flag any
+// pair of a chunk (kernel value <= 1) skips the test.
 #include "apsm_batch.cuh"
 #include "apsm_tc.cuh"
 
@@ -35,7 +48,19 @@ constexpr int kChunkPairs = 64;  // dictionary pairs per chunk
 constexpr int kChunkN = 128;     // accumulator columns per chunk (UMMA N)
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = (kEpiWarps + 2) * 32;
-constexpr int kBx = 2 * kChunkPairs + kChunkPairs; // per chunk: a*wG (128, column order) then ew log2(e) * pair norms (64)
+// per chunk: a*wG (128, column order), ew log2(e) * pair norms (64), fix weights fw (64), then
+// max fw and max fw * |ew log2(e) * pair norm| (padded to 4)
+constexpr int kBxAw = 0, kBxNrm = 2 * kChunkPairs, kBxFw = 3 * kChunkPairs, kBxGate = 4 * kChunkPairs;
+constexpr int kBx = 4 * kChunkPairs + 4;
+// per-pair error a flagged pair would exceed (soft-output units) in the single-product forms
+constexpr float kFixEps = 1.0f / 8192.0f;
+
+// ln 2 * 2u / kFixEps of a mode's operand rounding unit u (0: split forms, no correction)
+template <int MODE> __host__ __device__ constexpr float fix_scale()
+{
+    return MODE == kBF16 ? 0.69314718f * (2.0f / 256.0f) / kFixEps
+                         : (MODE == kTF32 ? 0.69314718f * (2.0f / 2048.0f) / kFixEps : 0.0f);
+}
 
 // bytes of one operand tile of R rows at K extent Kp (hi [+ lo])
 template <int MODE> __host__ __device__ constexpr size_t tile_bytes(int R, int Kp)
@@ -136,23 +161,81 @@ __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJ
         if constexpr (OpTraits<MODE>::kSplit) put_operand<MODE>(chunk, kChunkN, r, Kp + k, lo);
     }
     float* bx = jb.bx + size_t(c) * kBx;
-    for (int i = threadIdx.x; i < kBx; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kBxFw; i += blockDim.x) {
         float v = 0.f;
-        if (i < 2 * kChunkPairs) {
+        if (i < kBxNrm) {
             const int b = c * kChunkPairs + (i >> 1);
             v = b < jb.Mp ? jb.a[2 * b + (i & 1)] * wG : 0.f;
         } else {
-            const int b = c * kChunkPairs + (i - 2 * kChunkPairs);
+            const int b = c * kChunkPairs + (i - kBxNrm);
             v = b < jb.Mp ? jb.ew2 * jb.nrm_d[b] : 0.f; // norms pre-scaled by ew log2(e)
         }
         bx[i] = v;
     }
+    // fix weights of the pairs and the chunk's gate values (warp 0; 0 in the split forms)
+    if (threadIdx.x < 32) {
+        float g0 = 0.f, g1 = 0.f;
+        for (int p = threadIdx.x; p < kChunkPairs; p += 32) {
+            const int b = c * kChunkPairs + p;
+            float fw = 0.f, en = 0.f;
+            if (b < jb.Mp) {
+                fw = (fabsf(jb.a[2 * b] * wG) + fabsf(jb.a[2 * b + 1] * wG)) * fix_scale<MODE>();
+                en = -jb.ew2 * jb.nrm_d[b];
+            }
+            bx[kBxFw + p] = fw;
+            g0 = fmaxf(g0, fw);
+            g1 = fmaxf(g1, fw * en);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            g0 = fmaxf(g0, __shfl_xor_sync(0xffffffffu, g0, o));
+            g1 = fmaxf(g1, __shfl_xor_sync(0xffffffffu, g1, o));
+        }
+        if (threadIdx.x < 4) bx[kBxGate + threadIdx.x] = threadIdx.x == 0 ? g0 : (threadIdx.x == 1 ? g1 : 0.f);
+    }
+}
+
+// 16 pairs (32 accumulator columns) of one sample: kernel values from the Gram
+// cross terms, contracted with the pairs' coefficients into the two soft
+// outputs.  CHECK: pairs whose error bound exceeds kFixEps are left out and
+// returned as bits of the mask (pair j -> bit j).
+template <bool CHECK>
+__device__ __forceinline__ uint32_t epilogue_pairs16(const float* gv, const float* xs, int p0, float exn, float m2,
+                                                     float& f0, float& f1)
+{
+    uint32_t mask = 0u;
+#pragma unroll
+    for (int j = 0; j < 16; j += 2) {
+        const int pj = p0 + j; // pair index within the chunk
+        const float4 aw = *reinterpret_cast<const float4*>(xs + kBxAw + 2 * pj); // pairs pj, pj+1
+        const float2 nb = *reinterpret_cast<const float2*>(xs + kBxNrm + pj);
+        float2 fw = make_float2(0.f, 0.f);
+        if constexpr (CHECK) fw = *reinterpret_cast<const float2*>(xs + kBxFw + pj);
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const float es = exn + (e ? nb.y : nb.x), re = gv[2 * (j + e)], im = gv[2 * (j + e) + 1];
+            float kA = ex2(fminf(fmaf(m2, re, es), 0.f));
+            float kP = ex2(fminf(fmaf(m2, im, es), 0.f));
+            float kM = ex2(fminf(fmaf(-m2, im, es), 0.f));
+            if constexpr (CHECK) {
+                const float kmax = fmaxf(kA, fmaxf(kP, kM));
+                if (kmax * es * (e ? fw.y : fw.x) < -1.f) {
+                    mask |= 1u << (j + e);
+                    kA = kP = kM = 0.f;
+                }
+            }
+            const float a0 = e ? aw.z : aw.x, a1 = e ? aw.w : aw.y;
+            f0 = fmaf(a0, kA, fmaf(a1, kM, f0));
+            f1 = fmaf(a0, kP, fmaf(a1, kA, f1));
+        }
+    }
+    return mask;
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1)
     batch_gram_kernel(const BatchGramJob* __restrict__ jobs, int n_jobs, const int* __restrict__ tile_prefix, int Kpmax,
-                      int stages, int* err)
+                      int stages, int* err, unsigned long long wait_ns)
 {
     using T = OpTraits<MODE>;
     // job of this CTA: tile_prefix[j] <= blockIdx.x < tile_prefix[j + 1]
@@ -219,7 +302,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             int issued = 0;
             for (int i = 0; i < nch; ++i) {
                 const int s = i % stages;
-                if (i >= stages && !mbar_wait(&empty[s], ((i / stages) - 1) & 1, abort_flag)) break;
+                if (i >= stages && !mbar_wait(&empty[s], ((i / stages) - 1) & 1, abort_flag, wait_ns)) break;
                 ++issued;
                 mbar_expect_tx(&full[s], b_bytes + kBx * 4);
                 bulk_g2s(sB + size_t(s) * b_stride, jb.b_ops + size_t(i) * b_bytes, b_bytes, &full[s]);
@@ -230,15 +313,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp == kEpiWarps + 1) {
         // ---------------- MMA issuer ----------------
-        if (lane == 0 && nch > 0 && mbar_wait(afull, 0, abort_flag)) {
+        if (lane == 0 && nch > 0 && mbar_wait(afull, 0, abort_flag, wait_ns)) {
             const uint32_t idesc = instr_desc<MODE>(kTileM, kChunkN);
             const uint32_t lbo_a = kTileM * 16, lbo_b = kChunkN * 16;
             const int ksteps = jb.Kp / T::kStepK; // 32 bytes of K per UMMA
             const int lo_off = jb.Kp / T::kChunk; // 16-byte K chunks to the lo half
             for (int i = 0; i < nch; ++i) {
                 const int s = i % stages, buf = i & 1;
-                if (!mbar_wait(&full[s], (i / stages) & 1, abort_flag)) break;
-                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag)) break;
+                if (!mbar_wait(&full[s], (i / stages) & 1, abort_flag, wait_ns)) break;
+                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag, wait_ns)) break;
                 tc_fence_after();
                 const uint8_t* b = sB + size_t(s) * b_stride;
                 const uint32_t d = tmem + uint32_t(buf * kChunkN);
@@ -265,44 +348,58 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---------------- epilogue ----------------
         const int q = warp & 3, h = warp >> 2;
         const int row = tile * kTileM + q * 32 + lane;
-        const float xn = row < jb.S ? jb.nrm_s[row] : 0.f;
+        const bool valid = row < jb.S;
+        const float xn = valid ? jb.nrm_s[row] : 0.f;
         // exponents in base 2: ew log2(e) (|x|^2 + |y|^2 - 2 r) = exn + eyn + m2 r, the pair norms
         // pre-scaled in the chunk data; ew <= 0, so clamping the distance at 0 is clamping the
         // exponent at 0
         const float exn = jb.ew2 * xn, m2 = -2.f * jb.ew2;
+        // largest |exn| of the warp's samples (gate of the compensated forms)
+        float exn_max = -exn;
+        if constexpr (fix_scale<MODE>() > 0.f) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) exn_max = fmaxf(exn_max, __shfl_xor_sync(0xffffffffu, exn_max, o));
+        }
         float f0 = 0.f, f1 = 0.f;
         for (int i = 0; i < nch; ++i) {
             const int s = i % stages, buf = i & 1;
-            if (!mbar_wait(&full[s], (i / stages) & 1, abort_flag)) break;
-            if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag)) break;
+            if (!mbar_wait(&full[s], (i / stages) & 1, abort_flag, wait_ns)) break;
+            if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag, wait_ns)) break;
             tc_fence_after();
             const float* xs = sX + size_t(s) * kBx;
+            // can any pair of this chunk exceed the bound for a sample of this warp?  (warp-uniform)
+            const bool check = fix_scale<MODE>() > 0.f && fmaf(exn_max, xs[kBxGate], xs[kBxGate + 1]) > 1.f;
 #pragma unroll 1
             for (int cb = 0; cb < kChunkN / 2; cb += 32) {
                 const int col = h * (kChunkN / 2) + cb; // 32 columns = 16 pairs
                 float gv[32];
                 tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * kChunkN + col), gv);
-#pragma unroll
-                for (int j = 0; j < 16; j += 2) {
-                    const int pj = (col >> 1) + j; // pair index within the chunk
-                    const float4 aw = *reinterpret_cast<const float4*>(xs + 2 * pj); // pairs pj, pj+1
-                    const float2 nb = *reinterpret_cast<const float2*>(xs + 2 * kChunkPairs + pj);
-                    {
-                        const float es = exn + nb.x, re = gv[2 * j], im = gv[2 * j + 1];
-                        const float kA = ex2(fminf(fmaf(m2, re, es), 0.f));
-                        const float kP = ex2(fminf(fmaf(m2, im, es), 0.f));
-                        const float kM = ex2(fminf(fmaf(-m2, im, es), 0.f));
-                        f0 = fmaf(aw.x, kA, fmaf(aw.y, kM, f0));
-                        f1 = fmaf(aw.x, kP, fmaf(aw.y, kA, f1));
+                if (!check) {
+                    epilogue_pairs16<false>(gv, xs, col >> 1, exn, m2, f0, f1);
+                    continue;
+                }
+                uint32_t mask = epilogue_pairs16<true>(gv, xs, col >> 1, exn, m2, f0, f1);
+                if (!valid) mask = 0u;
+                // flagged pairs: r = Re(y^H x), m = Im(y^H x) in FP32 from the samples themselves
+                while (mask) {
+                    const int j = __ffs(mask) - 1;
+                    mask &= mask - 1u;
+                    const int pj = (col >> 1) + j;
+                    const float2* yb = jb.Yd + size_t(i * kChunkPairs + pj) * jb.Np;
+                    float re = 0.f, im = 0.f;
+                    for (int k = 0; k < jb.N; ++k) {
+                        const float2 x = jb.rx[size_t(k) * jb.S + row];
+                        const float2 y = yb[k];
+                        re = fmaf(y.x, x.x, fmaf(y.y, x.y, re));
+                        im = fmaf(y.x, x.y, fmaf(-y.y, x.x, im));
                     }
-                    {
-                        const float es = exn + nb.y, re = gv[2 * j + 2], im = gv[2 * j + 3];
-                        const float kA = ex2(fminf(fmaf(m2, re, es), 0.f));
-                        const float kP = ex2(fminf(fmaf(m2, im, es), 0.f));
-                        const float kM = ex2(fminf(fmaf(-m2, im, es), 0.f));
-                        f0 = fmaf(aw.z, kA, fmaf(aw.w, kM, f0));
-                        f1 = fmaf(aw.z, kP, fmaf(aw.w, kA, f1));
-                    }
+                    const float es = exn + xs[kBxNrm + pj];
+                    const float a0 = xs[kBxAw + 2 * pj], a1 = xs[kBxAw + 2 * pj + 1];
+                    const float kA = ex2(fminf(fmaf(m2, re, es), 0.f));
+                    const float kP = ex2(fminf(fmaf(m2, im, es), 0.f));
+                    const float kM = ex2(fminf(fmaf(-m2, im, es), 0.f));
+                    f0 = fmaf(a0, kA, fmaf(a1, kM, f0));
+                    f1 = fmaf(a0, kP, fmaf(a1, kA, f1));
                 }
             }
             tc_fence_before();
@@ -359,7 +456,8 @@ cudaError_t launch_mode(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, i
     const size_t smem = std::max<size_t>(gram_smem<MODE>(Kp, stages), 80 * 1024);
     e = cudaFuncSetAttribute(batch_gram_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
-    batch_gram_kernel<MODE><<<total_tiles, kThreads, smem, s>>>(d_jobs, n_jobs, d_tile_prefix, Kp, stages, d_err);
+    batch_gram_kernel<MODE><<<total_tiles, kThreads, smem, s>>>(d_jobs, n_jobs, d_tile_prefix, Kp, stages, d_err,
+                                                                wait_limit_ns());
     return cudaGetLastError();
 }
 

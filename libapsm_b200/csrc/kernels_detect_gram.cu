@@ -13,10 +13,19 @@
 //                x.d ~ xh.dh + xh.dl + xl.dh (3 products, ~2^-16 relative)
 //   gram_tf32    TF32 operands (1 product)
 //   gram_tf32x3  compensated TF32 split (3 products, ~FP32 accuracy)
-// The squared distance is clamped at 0 (cancellation for near-duplicate
-// points).  Each CTA owns one tile of data rows and a contiguous range of
-// dictionary chunks; partial sums per range are combined in a fixed order by
-// gram_finish_kernel, so results are deterministic.
+// The squared distance is clamped at 0.  Compensated cross terms (the
+// single-product forms bf16 / tf32): rounding both operands to the format's
+// unit u moves x.d by at most 2u |x||d|, the base-2 exponent
+// ew log2(e) (|x|^2 + |d|^2 - 2 x.d) by at most 2u |es| (es = ew log2(e)
+// (|x|^2 + |d|^2)), and a kernel value's contribution to user u's output by at
+// most |a_u wG| k ln2 2u |es|.  Where cancellation bites (near-duplicate
+// points: x.d ~ (|x|^2 + |d|^2) / 2 with k near 1) the epilogue flags the
+// entries whose bound, with the largest coefficient of the row over the
+// users, exceeds kFixEps, and recomputes their squared distance exactly as
+// sum (x - d)^2 in FP32 from the rows themselves.  Each CTA owns one tile of
+// data rows and a contiguous range of dictionary chunks; partial sums per
+// range are combined in a fixed order by gram_finish_kernel, so results are
+// deterministic.
 //
 // Roles (320 threads): warps 0-7 epilogue (warp w reads TMEM lanes
 // 32*(w%4).., columns of half w/4 of each chunk), warp 8 producer (bulk copies
@@ -43,7 +52,7 @@ constexpr int kMaxUsers = 16;
 
 struct GramWorkspace {
     DevBuf<uint8_t> a_ops, b_ops, w_ops; // operand tiles in the UMMA canonical K-major layout
-    DevBuf<float> xn, dn, aw, part, lin_unused;
+    DevBuf<float> xn, dn, aw, part, fw, gate;
     DevBuf<int> err;
     int* h_err = nullptr;
 };
@@ -96,6 +105,76 @@ __global__ void gram_pack_kernel(const float* __restrict__ rows, int n, int Dp, 
     }
 }
 
+// per-entry error a flagged entry would exceed (soft-output units) in the single-product forms
+constexpr float kFixEps = 1.0f / 8192.0f;
+
+// ln 2 * 2u / kFixEps of a mode's operand rounding unit u (0: split forms, no correction)
+template <int MODE> __host__ __device__ constexpr float fix_scale()
+{
+    return MODE == kBF16 ? 0.69314718f * (2.0f / 256.0f) / kFixEps
+                         : (MODE == kTF32 ? 0.69314718f * (2.0f / 2048.0f) / kFixEps : 0.0f);
+}
+
+// Fix weights of the compensated forms: fw[b] = max_u |a_u[b] wG| ln2 2u / kFixEps (0 past M)
+// and per chunk of N dictionary rows gate[c] = (max fw, max fw |ewl2 dn[b]|, 0, 0).
+template <int MODE>
+__global__ void __launch_bounds__(256) gram_fix_kernel(const float* __restrict__ a, size_t a_stride, int users, int M,
+                                                       int N, float wG, float ewl2, const float* __restrict__ dn,
+                                                       float* __restrict__ fw, float* __restrict__ gate)
+{
+    __shared__ float red[2][8];
+    const int c = blockIdx.x;
+    float g0 = 0.f, g1 = 0.f;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        const int b = c * N + k;
+        float v = 0.f;
+        if (b < M) {
+            for (int u = 0; u < users; ++u) v = fmaxf(v, fabsf(__fmul_rn(a[size_t(u) * a_stride + b], wG)));
+            v *= fix_scale<MODE>();
+        }
+        fw[b] = v;
+        g0 = fmaxf(g0, v);
+        g1 = fmaxf(g1, v * fabsf(ewl2 * dn[b]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        g0 = fmaxf(g0, __shfl_xor_sync(0xffffffffu, g0, o));
+        g1 = fmaxf(g1, __shfl_xor_sync(0xffffffffu, g1, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = g0;
+        red[1][threadIdx.x >> 5] = g1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < int(blockDim.x >> 5); ++w) {
+            g0 = fmaxf(g0, red[0][w]);
+            g1 = fmaxf(g1, red[1][w]);
+        }
+        gate[4 * c] = g0;
+        gate[4 * c + 1] = g1;
+        gate[4 * c + 2] = 0.f;
+        gate[4 * c + 3] = 0.f;
+    }
+}
+
+// Exact squared distance of two FP32 rows (16-byte aligned, D features), in feature order.
+__device__ __forceinline__ float row_distance(const float* __restrict__ x, const float* __restrict__ d, int D)
+{
+    float acc = 0.f;
+    int k = 0;
+    for (; k + 4 <= D; k += 4) {
+        const float4 xv = *reinterpret_cast<const float4*>(x + k);
+        const float4 dv = *reinterpret_cast<const float4*>(d + k);
+        acc = fmaf(xv.x - dv.x, xv.x - dv.x, acc);
+        acc = fmaf(xv.y - dv.y, xv.y - dv.y, acc);
+        acc = fmaf(xv.z - dv.z, xv.z - dv.z, acc);
+        acc = fmaf(xv.w - dv.w, xv.w - dv.w, acc);
+    }
+    for (; k < D; ++k) acc = fmaf(x[k] - d[k], x[k] - d[k], acc);
+    return acc;
+}
+
 // aw[u][b] = a_u[b] * wG (the reference's coeff * gaussianKernelWeight), 0 past M.
 __global__ void gram_coeff_kernel(const float* __restrict__ a, size_t a_stride, int users, int M, int Mpad, float wG,
                                   float* __restrict__ aw)
@@ -112,29 +191,46 @@ struct GramArgs {
     const float* xn;      // data norms
     const float* dn;      // dictionary norms (Mpad)
     const float* aw;      // users x Mpad
+    const float* fw;      // fix weights (Mpad)
+    const float* gate;    // per chunk: max fw, max fw |ewl2 dn|, 0, 0
+    const float* xrows;   // data rows (n_samples x Dp, FP32) for the exact recompute
+    const float* drows;   // dictionary rows (M x Dp, FP32)
     float* part;          // splits x users x n_samples partial sums
     int* err;
-    int n_samples, Mpad, users, Kp, N;
+    int n_samples, Mpad, users, Kp, N, Dp, D;
     int chunks_per_split, n_chunks;
     int stages; // dictionary chunks in flight (<= kMaxStages)
     float ewl2; // ew * log2(e)
+    unsigned long long wait_ns; // limit of the bounded waits
 };
 
 // NC accumulator columns of one data row: squared distance from the cross term
 // and the norms, Gaussian value, contraction with every user's coefficients.
-// xs: the stage's norms (xs[0 .. NC)) and coefficient rows (xs[(1 + u) N + ...]).
-template <int NC, int NU>
-__device__ __forceinline__ void epilogue_columns(const float* gv, const float* xs, int N, float xn, float ewl2,
-                                                 int users, float* acc)
+// xs: the stage's norms (xs[0 .. NC)), coefficient rows (xs[(1 + u) N + ...]) and
+// fix weights (xs[(1 + users) N + ...]).  CHECK: entries whose error bound exceeds
+// kFixEps are left out and returned as bits of the mask (column j -> bit j).
+template <int NC, int NU, bool CHECK>
+__device__ __forceinline__ uint32_t epilogue_columns(const float* gv, const float* xs, int N, float xn, float ewl2,
+                                                     int users, float* acc)
 {
+    uint32_t mask = 0u;
 #pragma unroll
     for (int j = 0; j < NC; j += 4) {
         const float4 dn4 = *reinterpret_cast<const float4*>(xs + j);
+        const float t[4] = {xn + dn4.x, xn + dn4.y, xn + dn4.z, xn + dn4.w};
         float kv[4];
-        kv[0] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + 0], xn + dn4.x), 0.f));
-        kv[1] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + 1], xn + dn4.y), 0.f));
-        kv[2] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + 2], xn + dn4.z), 0.f));
-        kv[3] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + 3], xn + dn4.w), 0.f));
+#pragma unroll
+        for (int e = 0; e < 4; ++e) kv[e] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j + e], t[e]), 0.f));
+        if constexpr (CHECK) {
+            const float4 fw4 = *reinterpret_cast<const float4*>(xs + (1 + users) * N + j);
+            const float fw[4] = {fw4.x, fw4.y, fw4.z, fw4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (kv[e] * (ewl2 * t[e]) * fw[e] < -1.f) {
+                    mask |= 1u << (j + e);
+                    kv[e] = 0.f;
+                }
+        }
 #pragma unroll
         for (int u = 0; u < NU; ++u) {
             if (u < users) {
@@ -146,6 +242,16 @@ __device__ __forceinline__ void epilogue_columns(const float* gv, const float* x
             }
         }
     }
+    return mask;
+}
+
+// Largest |ewl2 xn| of the warp's rows.
+__device__ __forceinline__ float warp_exn_max(float ewl2, float xn)
+{
+    float v = fabsf(ewl2 * xn);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
 }
 
 template <int MODE, int NU>
@@ -156,7 +262,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
     const int KE = T::kSplit ? 2 * g.Kp : g.Kp;
     const uint32_t a_bytes = uint32_t(kTileM) * KE * T::kElem;
     const uint32_t b_bytes = uint32_t(g.N) * KE * T::kElem;
-    const uint32_t x_bytes = uint32_t(g.N) * 4 * (1 + g.users); // dn + aw rows
+    const uint32_t x_bytes = uint32_t(g.N) * 4 * (2 + g.users) + 16; // dn, aw rows, fw, chunk gate
     uint8_t* sA = smem;
     uint8_t* sB = sA + a_bytes;
     const int NS = g.stages;
@@ -212,7 +318,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
             int issued = 0;
             for (int i = 0; i < nch; ++i) {
                 const int s = i % NS;
-                if (i >= NS && !mbar_wait(&empty[s], ((i / NS) - 1) & 1, abort_flag)) break;
+                if (i >= NS && !mbar_wait(&empty[s], ((i / NS) - 1) & 1, abort_flag, g.wait_ns)) break;
                 ++issued;
                 const int c = c0 + i;
                 mbar_expect_tx(&full[s], b_bytes + x_bytes);
@@ -221,6 +327,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
                 bulk_g2s(xs, g.dn + size_t(c) * N, N * 4, &full[s]);
                 for (int u = 0; u < g.users; ++u)
                     bulk_g2s(xs + (1 + u) * N, g.aw + size_t(u) * g.Mpad + size_t(c) * N, N * 4, &full[s]);
+                bulk_g2s(xs + (1 + g.users) * N, g.fw + size_t(c) * N, N * 4, &full[s]);
+                bulk_g2s(xs + (2 + g.users) * N, g.gate + size_t(c) * 4, 16, &full[s]);
             }
             // no bulk copy may still be writing shared memory when the CTA exits
             mbar_drain(afull, 0);
@@ -228,15 +336,15 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
         }
     } else if (warp == kEpiWarps + 1) {
         // ---------------- MMA issuer ----------------
-        if (lane == 0 && mbar_wait(afull, 0, abort_flag)) {
+        if (lane == 0 && mbar_wait(afull, 0, abort_flag, g.wait_ns)) {
             const uint32_t idesc = instr_desc<MODE>(kTileM, N);
             const uint32_t lbo_a = kTileM * 16, lbo_b = uint32_t(N) * 16;
             const int ksteps = g.Kp / T::kStepK;
             const int lo_off = g.Kp / T::kChunk; // K chunks to the lo half
             for (int i = 0; i < nch; ++i) {
                 const int s = i % NS, buf = i & 1;
-                if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag)) break;
-                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag)) break;
+                if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag, g.wait_ns)) break;
+                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag, g.wait_ns)) break;
                 tc_fence_after();
                 const uint8_t* b = sB + size_t(s) * b_bytes;
                 const uint32_t d = tmem + uint32_t(buf * N);
@@ -266,31 +374,51 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect_kernel(GramArgs g)
         // ---------------- epilogue: 8 warps ----------------
         const int q = warp & 3, h = warp >> 2;
         const int row = tile * kTileM + q * 32 + lane;
-        const float xn = row < g.n_samples ? g.xn[row] : 0.f;
+        const bool valid = row < g.n_samples;
+        const float xn = valid ? g.xn[row] : 0.f;
+        const float exn_max = fix_scale<MODE>() > 0.f ? warp_exn_max(g.ewl2, xn) : 0.f;
         float acc[NU];
 #pragma unroll
         for (int u = 0; u < NU; ++u) acc[u] = 0.f;
         const int half = N / 2;
+        // flagged entries of one batch of columns: exact squared distance from the FP32 rows
+        auto fix = [&](uint32_t mask, const float* xs, int col, int c) {
+            if (!valid) return;
+            while (mask) {
+                const int j = __ffs(mask) - 1;
+                mask &= mask - 1u;
+                const float d2 = row_distance(g.xrows + size_t(row) * g.Dp, g.drows + size_t(c * N + col + j) * g.Dp, g.D);
+                const float kv = ex2(g.ewl2 * d2);
+#pragma unroll
+                for (int u = 0; u < NU; ++u)
+                    if (u < g.users) acc[u] = fmaf(xs[(1 + u) * N + col + j], kv, acc[u]);
+            }
+        };
         for (int i = 0; i < nch; ++i) {
             const int s = i % NS, buf = i & 1;
             // the stage's norms / coefficients (bulk copies) and the accumulator
-            if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag)) break;
-            if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag)) break;
+            if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag, g.wait_ns)) break;
+            if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag, g.wait_ns)) break;
             tc_fence_after();
             const float* xs = reinterpret_cast<const float*>(reinterpret_cast<const uint8_t*>(sX) + size_t(s) * x_bytes);
             const uint32_t trow = tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * N);
+            // can any entry of this chunk exceed the bound for a row of this warp?  (warp-uniform)
+            const float* gate = xs + (2 + g.users) * N;
+            const bool check = fix_scale<MODE>() > 0.f && fmaf(exn_max, gate[0], gate[1]) > 1.f;
             if (half >= 32) {
                 for (int cb = 0; cb < half; cb += 32) {
                     const int col = h * half + cb;
                     float gv[32];
                     tmem_ld32(trow + uint32_t(col), gv);
-                    epilogue_columns<32, NU>(gv, xs + col, N, xn, g.ewl2, g.users, acc);
+                    if (check) fix(epilogue_columns<32, NU, true>(gv, xs + col, N, xn, g.ewl2, g.users, acc), xs, col, c0 + i);
+                    else epilogue_columns<32, NU, false>(gv, xs + col, N, xn, g.ewl2, g.users, acc);
                 }
             } else { // 32-column chunks: 16 columns per half
                 const int col = h * half;
                 float gv[16];
                 tmem_ld16(trow + uint32_t(col), gv);
-                epilogue_columns<16, NU>(gv, xs + col, N, xn, g.ewl2, g.users, acc);
+                if (check) fix(epilogue_columns<16, NU, true>(gv, xs + col, N, xn, g.ewl2, g.users, acc), xs, col, c0 + i);
+                else epilogue_columns<16, NU, false>(gv, xs + col, N, xn, g.ewl2, g.users, acc);
             }
             tc_fence_before();
             __syncwarp();
@@ -379,13 +507,70 @@ struct Gram2Args {
     const uint8_t* w_ops; // per chunk: W, 16 rows x N (K), canonical K-major, hi [| lo]
     const float* xn;      // data norms
     const float* dn;      // dictionary norms (Mpad)
+    const float* fw;      // fix weights (Mpad)
+    const float* gate;    // per chunk: max fw, max fw |ewl2 dn|, 0, 0
+    const float* xrows;   // data rows (n_samples x Dp, FP32) for the exact recompute
+    const float* drows;   // dictionary rows (M x Dp, FP32)
     float* part;          // splits x users x n_samples partial sums
     int* err;
-    int n_samples, users, Kp, N;
+    int n_samples, users, Kp, N, Dp, D;
     int chunks_per_split, n_chunks;
     int stages;
     float ewl2; // ew * log2(e)
+    unsigned long long wait_ns; // limit of the bounded waits
 };
+
+// 16 kernel values of one data row (columns col .. col + 15 of the chunk) into the
+// kernel-value operand P (row r; hi [and lo]).  CHECK: entries whose error bound
+// exceeds kFixEps are returned as bits of the mask (their P entries are rewritten).
+template <int MODE, bool CHECK>
+__device__ __forceinline__ uint32_t kernel_values16(const float* gv, const float* sd, int N, int col, float xn,
+                                                    float ewl2, uint8_t* p, int r)
+{
+    using T = OpTraits<MODE>;
+    uint32_t mask = 0u;
+#pragma unroll
+    for (int j0 = 0; j0 < 16; j0 += T::kChunk) {
+        // one 16-byte K chunk of this row: hi, and lo for split modes
+        uint32_t hw[4] = {0u, 0u, 0u, 0u}, lw[4] = {0u, 0u, 0u, 0u};
+        float kv[T::kChunk];
+#pragma unroll
+        for (int e = 0; e < T::kChunk; ++e) {
+            const int j = j0 + e;
+            const float t = xn + sd[col + j];
+            kv[e] = ex2(ewl2 * fmaxf(fmaf(-2.f, gv[j], t), 0.f));
+            if constexpr (CHECK)
+                if (kv[e] * (ewl2 * t) * sd[N + col + j] < -1.f) mask |= 1u << j;
+        }
+        if constexpr (MODE == kBF16) {
+            // pairs converted by one instruction each (round to nearest)
+#pragma unroll
+            for (int e = 0; e < T::kChunk; e += 2) {
+                const __nv_bfloat162 v2 = __floats2bfloat162_rn(kv[e], kv[e + 1]);
+                hw[e >> 1] = *reinterpret_cast<const uint32_t*>(&v2);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < T::kChunk; ++e) {
+                float hi, lo;
+                split_operand<MODE>(kv[e], &hi, &lo);
+                if constexpr (T::kTF) {
+                    hw[e] = __float_as_uint(hi);
+                    lw[e] = __float_as_uint(lo);
+                } else {
+                    hw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(hi))) << (16 * (e & 1));
+                    lw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(lo))) << (16 * (e & 1));
+                }
+            }
+        }
+        const int kc = (col + j0) / T::kChunk;
+        const size_t off = size_t(kc) * (kTileM * 16) + (r >> 3) * 128 + (r & 7) * 16;
+        *reinterpret_cast<uint4*>(p + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        if constexpr (T::kSplit)
+            *reinterpret_cast<uint4*>(p + size_t(N / T::kChunk) * (kTileM * 16) + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+    return mask;
+}
 
 // W chunks: element (u, k) = a[u][c N + k] * wG (0 past M and for u >= users)
 template <int MODE>
@@ -425,8 +610,9 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect2_kernel(Gram2Args g)
     uint8_t* sB = sA + a_bytes;                          // [NS] chunk rows
     uint8_t* sW = sB + size_t(NS) * b_bytes;             // [NS] chunk coefficients
     uint8_t* sP = sW + size_t(NS) * w_bytes;             // [2] kernel values
-    float* sD = reinterpret_cast<float*>(sP + 2 * size_t(p_bytes)); // [NS][N] chunk norms
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sD + size_t(NS) * N);
+    const int sd_stride = 2 * N + 4;                     // chunk norms, fix weights, gate
+    float* sD = reinterpret_cast<float*>(sP + 2 * size_t(p_bytes)); // [NS][sd_stride]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sD + size_t(NS) * sd_stride);
     uint64_t* full = bars;             // [NS]
     uint64_t* empty = bars + NS;       // [NS]
     uint64_t* tfull = bars + 2 * NS;   // [2]
@@ -481,20 +667,23 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect2_kernel(Gram2Args g)
             int issued = 0;
             for (int i = 0; i < nch; ++i) {
                 const int s = i % NS;
-                if (i >= NS && !mbar_wait(&empty[s], ((i / NS) - 1) & 1, abort_flag)) break;
+                if (i >= NS && !mbar_wait(&empty[s], ((i / NS) - 1) & 1, abort_flag, g.wait_ns)) break;
                 ++issued;
                 const int c = c0 + i;
-                mbar_expect_tx(&full[s], b_bytes + w_bytes + uint32_t(N) * 4);
+                mbar_expect_tx(&full[s], b_bytes + w_bytes + uint32_t(sd_stride) * 4);
                 bulk_g2s(sB + size_t(s) * b_bytes, g.b_ops + size_t(c) * b_bytes, b_bytes, &full[s]);
                 bulk_g2s(sW + size_t(s) * w_bytes, g.w_ops + size_t(c) * w_bytes, w_bytes, &full[s]);
-                bulk_g2s(sD + size_t(s) * N, g.dn + size_t(c) * N, uint32_t(N) * 4, &full[s]);
+                float* sd = sD + size_t(s) * sd_stride;
+                bulk_g2s(sd, g.dn + size_t(c) * N, uint32_t(N) * 4, &full[s]);
+                bulk_g2s(sd + N, g.fw + size_t(c) * N, uint32_t(N) * 4, &full[s]);
+                bulk_g2s(sd + 2 * N, g.gate + size_t(c) * 4, 16, &full[s]);
             }
             mbar_drain(afull, 0);
             for (int i = max(0, issued - NS); i < issued; ++i) mbar_drain(&full[i % NS], (i / NS) & 1);
         }
     } else if (warp == kEpiWarps + 1) {
         // ---------------- MMA issuer: Gram tile of chunk i, then the users' product of chunk i - 1 ----------------
-        if (lane == 0 && mbar_wait(afull, 0, abort_flag)) {
+        if (lane == 0 && mbar_wait(afull, 0, abort_flag, g.wait_ns)) {
             const uint32_t idesc = instr_desc<MODE>(kTileM, N);
             const uint32_t idesc2 = instr_desc<MODE>(kTileM, kUsers2);
             const uint32_t lbo_a = kTileM * 16, lbo_b = uint32_t(N) * 16, lbo_w = kUsers2 * 16;
@@ -503,7 +692,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect2_kernel(Gram2Args g)
             bool ok = true;
             auto product2 = [&](int j) {
                 const int pb = j & 1, sj = j % NS;
-                if (!mbar_wait(&pfull[pb], (j >> 1) & 1, abort_flag)) {
+                if (!mbar_wait(&pfull[pb], (j >> 1) & 1, abort_flag, g.wait_ns)) {
                     ok = false;
                     return;
                 }
@@ -526,8 +715,8 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect2_kernel(Gram2Args g)
             };
             for (int i = 0; i < nch && ok; ++i) {
                 const int s = i % NS, buf = i & 1;
-                if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag)) break;
-                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag)) break;
+                if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag, g.wait_ns)) break;
+                if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag, g.wait_ns)) break;
                 tc_fence_after();
                 const uint8_t* b = sB + size_t(s) * b_bytes;
                 const uint32_t d = tmem + uint32_t(buf * N);
@@ -556,61 +745,43 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect2_kernel(Gram2Args g)
         const int q = warp & 3, h = warp >> 2;
         const int r = q * 32 + lane; // row of the tile (tensor-memory lane)
         const int row = tile * kTileM + r;
-        const float xn = row < g.n_samples ? g.xn[row] : 0.f;
+        const bool valid = row < g.n_samples;
+        const float xn = valid ? g.xn[row] : 0.f;
+        constexpr bool kFix = fix_scale<MODE>() > 0.f && !T::kSplit;
+        const float exn_max = kFix ? warp_exn_max(g.ewl2, xn) : 0.f;
         const int half = N / 2;
         bool ok = true;
         for (int i = 0; i < nch; ++i) {
             const int s = i % NS, buf = i & 1, pb = i & 1;
-            if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag) || !mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag) ||
-                (i >= 2 && !mbar_wait(&pempty[pb], ((i >> 1) - 1) & 1, abort_flag))) {
+            if (!mbar_wait(&full[s], (i / NS) & 1, abort_flag, g.wait_ns) ||
+                !mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag, g.wait_ns) ||
+                (i >= 2 && !mbar_wait(&pempty[pb], ((i >> 1) - 1) & 1, abort_flag, g.wait_ns))) {
                 ok = false;
                 break;
             }
             tc_fence_after();
-            const float* dn = sD + size_t(s) * N;
+            const float* sd = sD + size_t(s) * sd_stride;
             uint8_t* p = sP + size_t(pb) * p_bytes;
             const uint32_t trow = tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * N);
+            // can any entry of this chunk exceed the bound for a row of this warp?  (warp-uniform)
+            const bool check = kFix && fmaf(exn_max, sd[2 * N], sd[2 * N + 1]) > 1.f;
             for (int cb = 0; cb < half; cb += 16) {
                 const int col = h * half + cb;
                 float gv[16];
                 tmem_ld16(trow + uint32_t(col), gv);
-#pragma unroll
-                for (int j0 = 0; j0 < 16; j0 += T::kChunk) {
-                    // one 16-byte K chunk of this row: hi, and lo for split modes
-                    uint32_t hw[4] = {0u, 0u, 0u, 0u}, lw[4] = {0u, 0u, 0u, 0u};
-                    float kv[T::kChunk];
-#pragma unroll
-                    for (int e = 0; e < T::kChunk; ++e) {
-                        const int j = j0 + e;
-                        kv[e] = ex2(g.ewl2 * fmaxf(fmaf(-2.f, gv[j], xn + dn[col + j]), 0.f));
-                    }
-                    if constexpr (MODE == kBF16) {
-                        // pairs converted by one instruction each (round to nearest)
-#pragma unroll
-                        for (int e = 0; e < T::kChunk; e += 2) {
-                            const __nv_bfloat162 v2 = __floats2bfloat162_rn(kv[e], kv[e + 1]);
-                            hw[e >> 1] = *reinterpret_cast<const uint32_t*>(&v2);
-                        }
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < T::kChunk; ++e) {
-                            float hi, lo;
-                            split_operand<MODE>(kv[e], &hi, &lo);
-                            if constexpr (T::kTF) {
-                                hw[e] = __float_as_uint(hi);
-                                lw[e] = __float_as_uint(lo);
-                            } else {
-                                hw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(hi))) << (16 * (e & 1));
-                                lw[e >> 1] |= uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(lo))) << (16 * (e & 1));
-                            }
-                        }
-                    }
-                    const int kc = (col + j0) / T::kChunk;
-                    const size_t off = size_t(kc) * (kTileM * 16) + (r >> 3) * 128 + (r & 7) * 16;
-                    *reinterpret_cast<uint4*>(p + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-                    if constexpr (T::kSplit)
-                        *reinterpret_cast<uint4*>(p + size_t(N / T::kChunk) * (kTileM * 16) + off) =
-                            make_uint4(lw[0], lw[1], lw[2], lw[3]);
+                if (!check) {
+                    kernel_values16<MODE, false>(gv, sd, N, col, xn, g.ewl2, p, r);
+                    continue;
+                }
+                uint32_t mask = kernel_values16<MODE, true>(gv, sd, N, col, xn, g.ewl2, p, r);
+                if (!valid) mask = 0u;
+                // flagged entries: exact squared distance from the FP32 rows, the value rewritten in P
+                while (mask) {
+                    const int j = __ffs(mask) - 1;
+                    mask &= mask - 1u;
+                    const float d2 = row_distance(g.xrows + size_t(row) * g.Dp,
+                                                  g.drows + size_t((c0 + i) * N + col + j) * g.Dp, g.D);
+                    put_operand<MODE>(p, kTileM, r, col + j, ex2(g.ewl2 * d2));
                 }
             }
             tc_fence_before();
@@ -628,7 +799,7 @@ __global__ void __launch_bounds__(kThreads, 1) gram_detect2_kernel(Gram2Args g)
             float acc[kUsers2];
 #pragma unroll
             for (int u = 0; u < kUsers2; ++u) acc[u] = 0.f;
-            const bool have = ok && nch > 0 && mbar_wait(done, 0, abort_flag);
+            const bool have = ok && nch > 0 && mbar_wait(done, 0, abort_flag, g.wait_ns);
             if (__all_sync(0xffffffffu, have)) {
                 tc_fence_after();
                 tmem_ld16(tmem + (uint32_t(q * 32) << 16) + acc2, acc);
@@ -652,7 +823,7 @@ template <int MODE> size_t gram2_smem(int Kp, int N, int stages)
     using T = OpTraits<MODE>;
     const size_t KE = T::kSplit ? 2 * Kp : Kp, KE2 = T::kSplit ? 2 * N : N;
     return size_t(kTileM) * KE * T::kElem + size_t(stages) * (size_t(N) * KE * T::kElem + kUsers2 * KE2 * T::kElem) +
-           2 * size_t(kTileM) * KE2 * T::kElem + size_t(stages) * N * 4 + (2 * stages + 10) * 8 + 16;
+           2 * size_t(kTileM) * KE2 * T::kElem + size_t(stages) * (2 * N + 4) * 4 + (2 * stages + 10) * 8 + 16;
 }
 
 template <int MODE, int NU> void launch_gram(const GramArgs& ga, int n_tiles, int splits, size_t smem, cudaStream_t s,
@@ -668,6 +839,10 @@ template <int MODE>
 apsm_status run_gram2(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s, int Kp, int N, int stages)
 {
     using T = OpTraits<MODE>;
+    if (2 * N + kUsers2 > 512) { // the kernel's tensor memory: 2 N + 16 columns rounded up to a power of two
+        h->last_error = "two-product Gram detection: chunk of " + std::to_string(N) + " rows exceeds tensor memory";
+        return APSM_ERR_UNSUPPORTED;
+    }
     GramWorkspace* gw = h->gram;
     const int ns = int(2 * S);
     const int M = int(h->used);
@@ -691,10 +866,13 @@ apsm_status run_gram2(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s
     GR_CK(gw->w_ops.ensure(size_t(n_chunks) * kUsers2 * KE2 * T::kElem));
     GR_CK(gw->xn.ensure(size_t(n_tiles) * kTileM));
     GR_CK(gw->dn.ensure(Mpad));
+    GR_CK(gw->fw.ensure(Mpad));
+    GR_CK(gw->gate.ensure(size_t(4) * n_chunks));
     GR_CK(gw->part.ensure(size_t(splits) * U * ns));
     GR_CK(gw->err.ensure(1));
     GR_CK(cudaMemsetAsync(gw->err.p, 0, sizeof(int), s));
     GR_CK(cudaMemsetAsync(gw->dn.p, 0, sizeof(float) * Mpad, s));
+    const float ewl2 = h->model_params().ew * 1.4426950408889634f;
 
     const int threads = 256;
     gram_pack_kernel<MODE><<<std::min(4096, (n_tiles * kTileM * Kp + threads - 1) / threads), threads, 0, s>>>(
@@ -702,6 +880,9 @@ apsm_status run_gram2(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s
     GR_CK(cudaGetLastError());
     gram_pack_kernel<MODE><<<std::min(4096, (n_chunks * N * Kp + threads - 1) / threads), threads, 0, s>>>(
         h->dict_X.p, M, Dp, D, Kp, N, n_chunks, gw->b_ops.p, gw->dn.p);
+    GR_CK(cudaGetLastError());
+    gram_fix_kernel<MODE><<<n_chunks, 256, 0, s>>>(h->dict_a.p, h->cap, U, M, N, h->cfg.wG, ewl2, gw->dn.p, gw->fw.p,
+                                                   gw->gate.p);
     GR_CK(cudaGetLastError());
     gram_pack_w_kernel<MODE><<<std::min(4096, (n_chunks * kUsers2 * N + threads - 1) / threads), threads, 0, s>>>(
         h->dict_a.p, h->cap, U, M, N, n_chunks, h->cfg.wG, gw->w_ops.p);
@@ -713,16 +894,23 @@ apsm_status run_gram2(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s
     ga.w_ops = gw->w_ops.p;
     ga.xn = gw->xn.p;
     ga.dn = gw->dn.p;
+    ga.fw = gw->fw.p;
+    ga.gate = gw->gate.p;
+    ga.xrows = h->xs.p;
+    ga.drows = h->dict_X.p;
     ga.part = gw->part.p;
     ga.err = gw->err.p;
     ga.n_samples = ns;
     ga.users = U;
     ga.Kp = Kp;
     ga.N = N;
+    ga.Dp = Dp;
+    ga.D = D;
     ga.chunks_per_split = cps;
     ga.n_chunks = n_chunks;
     ga.stages = stages;
-    ga.ewl2 = h->model_params().ew * 1.4426950408889634f;
+    ga.ewl2 = ewl2;
+    ga.wait_ns = wait_limit_ns();
     // >= 120 KB keeps one CTA per SM: its tensor memory (up to 512 columns) is never contended
     const size_t smem = std::max<size_t>(gram2_smem<MODE>(Kp, N, stages) + 1024, 120 * 1024);
     GR_CK(cudaFuncSetAttribute(gram_detect2_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -754,7 +942,9 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
         // the users' contraction on the tensor cores where its operands fit shared memory; only
         // in the BF16 form, whose kernel values and coefficients may be BF16 too (in the other
         // forms the second product's rounding would cost more accuracy than its time saves)
-        for (int n2 = 256; n2 >= 32; n2 /= 2)
+        // tensor memory: two Gram buffers of n2 columns and the users' 16, rounded up to a power of
+        // two, within the 512 columns of an SM: n2 <= 128
+        for (int n2 = 128; n2 >= 32; n2 /= 2)
             for (int st2 = kMaxStages; st2 >= 2; --st2)
                 if (gram2_smem<MODE>(Kp, n2, st2) + 1024 <= 220 * 1024) return run_gram2<MODE>(h, S, d_out, s, Kp, n2, st2);
     }
@@ -762,7 +952,7 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     // (chunks of 256 down to 64 columns in 3 stages, then 32 columns in 3 or 2 stages)
     int N = 256, stages = kMaxStages;
     auto smem_for = [&](int n, int st) {
-        return size_t(kTileM) * KE * T::kElem + size_t(st) * (size_t(n) * KE * T::kElem + size_t(n) * 4 * (1 + U)) +
+        return size_t(kTileM) * KE * T::kElem + size_t(st) * (size_t(n) * KE * T::kElem + size_t(n) * 4 * (2 + U) + 16) +
                (2 * st + 6) * 8 + 16 + size_t(4 * 32) * U * 4;
     };
     const size_t limit = 220 * 1024;
@@ -790,10 +980,13 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     GR_CK(gw->xn.ensure(size_t(n_tiles) * kTileM));
     GR_CK(gw->dn.ensure(Mpad));
     GR_CK(gw->aw.ensure(size_t(U) * Mpad));
+    GR_CK(gw->fw.ensure(Mpad));
+    GR_CK(gw->gate.ensure(size_t(4) * n_chunks));
     GR_CK(gw->part.ensure(size_t(splits) * U * ns));
     GR_CK(gw->err.ensure(1));
     GR_CK(cudaMemsetAsync(gw->err.p, 0, sizeof(int), s));
     GR_CK(cudaMemsetAsync(gw->dn.p, 0, sizeof(float) * Mpad, s));
+    const float ewl2 = h->model_params().ew * 1.4426950408889634f;
 
     const int threads = 256;
     gram_pack_kernel<MODE><<<std::min(4096, (n_tiles * kTileM * Kp + threads - 1) / threads), threads, 0, s>>>(
@@ -804,6 +997,9 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     GR_CK(cudaGetLastError());
     gram_coeff_kernel<<<(U * Mpad + 255) / 256, 256, 0, s>>>(h->dict_a.p, h->cap, U, M, Mpad, h->cfg.wG, gw->aw.p);
     GR_CK(cudaGetLastError());
+    gram_fix_kernel<MODE><<<n_chunks, 256, 0, s>>>(h->dict_a.p, h->cap, U, M, N, h->cfg.wG, ewl2, gw->dn.p, gw->fw.p,
+                                                   gw->gate.p);
+    GR_CK(cudaGetLastError());
 
     GramArgs ga;
     ga.a_ops = gw->a_ops.p;
@@ -811,6 +1007,10 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     ga.xn = gw->xn.p;
     ga.dn = gw->dn.p;
     ga.aw = gw->aw.p;
+    ga.fw = gw->fw.p;
+    ga.gate = gw->gate.p;
+    ga.xrows = h->xs.p;
+    ga.drows = h->dict_X.p;
     ga.part = gw->part.p;
     ga.err = gw->err.p;
     ga.n_samples = ns;
@@ -818,10 +1018,13 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
     ga.users = U;
     ga.Kp = Kp;
     ga.N = N;
+    ga.Dp = Dp;
+    ga.D = D;
     ga.chunks_per_split = cps;
     ga.n_chunks = n_chunks;
     ga.stages = stages;
-    ga.ewl2 = h->model_params().ew * 1.4426950408889634f;
+    ga.ewl2 = ewl2;
+    ga.wait_ns = wait_limit_ns();
     // >= 120 KB keeps one CTA per SM, so the 2N tensor-memory columns of a CTA never wait for another's
     const size_t smem = std::max<size_t>(smem_for(N, stages) + 1024, 120 * 1024);
     if (U <= 1) launch_gram<MODE, 1>(ga, n_tiles, splits, smem, s, &e);
@@ -843,6 +1046,16 @@ apsm_status run_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
 
 using namespace apsm;
 
+// Expiry of a bounded wait in the last Gram detection, read after its stream
+// synchronised (host calls): reported once, then cleared.
+apsm_status detect_gram_check(apsm_detector* h)
+{
+    if (!h->gram || !h->gram->h_err || !*h->gram->h_err) return APSM_OK;
+    *h->gram->h_err = 0;
+    h->last_error = "Gram detection gave up waiting on the GPU (bounded wait expired); its estimates are invalid";
+    return APSM_ERR_CUDA;
+}
+
 apsm_status detect_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t s)
 {
     if (!h->gram) {
@@ -854,8 +1067,9 @@ apsm_status detect_gram(apsm_detector* h, uint32_t S, float* d_out, cudaStream_t
         }
         *h->gram->h_err = 0;
     }
-    if (*h->gram->h_err) {
-        h->last_error = "a previous Gram detection timed out waiting on the GPU";
+    if (*h->gram->h_err) { // an earlier call on this stream (device mode) gave up: reported once
+        *h->gram->h_err = 0;
+        h->last_error = "a previous Gram detection gave up waiting on the GPU (bounded wait expired)";
         return APSM_ERR_CUDA;
     }
     switch (h->cfg.detect_mode) {

@@ -8,7 +8,8 @@ outputs are compared with the FP64 oracle holding the same state
 soft-output magnitude of the frame, follows from its operand precision: the
 cross term x.d carries a relative error of about 2^-8 (bf16), 2^-11 (tf32),
 2^-16 (bf16x3) or 2^-21 (tf32x3) of |x||d|, which reaches the Gaussian term
-scaled by 2 |ew| |x||d|."""
+scaled by 2 |ew| |x||d|; the single-product forms recompute the entries where
+that bound is large exactly, which keeps them within 2e-3."""
 import numpy as np
 import pytest
 
@@ -19,7 +20,7 @@ pytestmark = pytest.mark.gpu
 
 BASE = {"otype": "APSM", "windowSize": 20, "gaussianKernelVariance": 0.5, "eB": 0.01}
 # relative soft-output bound of each form (the exact form is its own FP32 bar)
-BOUNDS = {"balanced": 1e-5, "gram_tf32x3": 2e-5, "gram_bf16x3": 1e-4, "gram_tf32": 2e-3, "gram_bf16": 2e-2}
+BOUNDS = {"balanced": 1e-5, "gram_tf32x3": 2e-5, "gram_bf16x3": 1e-4, "gram_tf32": 2e-3, "gram_bf16": 2e-3}
 
 CASES = [  # name, (seed, K users, N, P, S, modulation), users detected, extra config
     ("N8-u1", (40, 3, 8, 150, 300, "QPSK"), 1, {}),

@@ -74,8 +74,9 @@ def test_pool_matches_oracle_per_detector(native_lib, oracle_mod, cfg):
 
 # Operand precision of the pool's other tensor-core forms: the cross term y^H x
 # carries ~2^-8 (bf16), ~2^-11 (tf32) or ~2^-16 (bf16x3) relative error of
-# |y||x|, which reaches each Gaussian term scaled by |ew|.
-GRAM_TOL = {"gram_bf16": 1e-2, "gram_tf32": 2e-3, "gram_bf16x3": 1e-4}
+# |y||x|, which reaches each Gaussian term scaled by |ew|; the single-product
+# forms recompute the pairs where that bound is large exactly (2e-3 bar).
+GRAM_TOL = {"gram_bf16": 2e-3, "gram_tf32": 2e-3, "gram_bf16x3": 1e-4}
 
 
 @pytest.mark.parametrize("narrow", [False, True], ids=["wide", "narrow"])
