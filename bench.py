@@ -145,6 +145,58 @@ def sweep_algorithmic_bytes(dets, window: int, dict_size: int) -> int:
     return total
 
 
+def sweep_column_entries(dets, dict_size: int) -> int:
+    """Kernel-column entries of a batch (pair n against the min(n, capacity)
+    pairs before it): each is written once by the column launch and read
+    once by the sweep, 16 bytes each way."""
+    return sum(sum(min(n, dict_size) for n in range(d.P)) for d in dets)
+
+
+def latency_roofline(pool, L, dets, ids, dev_in, sweep_ms: float, slots: int, sm_mhz: float | None) -> dict:
+    """Step-latency bound of the batched training sweep.  Every job is a chain
+    of P dependent steps (one complex pilot enters per step, sampleStep 2); the
+    launch runs `slots` chains at once (CTAs per SM x SMs).  The per-step
+    latency of a chain running alone on the idle GPU (the longest job, one
+    CTA) is measured here; from it follow the longest chain's floor and the
+    throughput floor of all steps spread over the slots."""
+    k = max(range(len(dets)), key=lambda i: dets[i].P)
+    job = pool.prepare([L.PoolJob(ids[k], dev_in[k][0], dev_in[k][1], fresh=True)], device=True)
+    alone = []
+    for _ in range(4):
+        pool.run_prepared(job, mode=1)
+        pool.wait()
+        alone.append(pool.last_sweep_ms())
+    alone_ms = min(alone[1:])
+    steps_longest = dets[k].P
+    step_us = alone_ms * 1e3 / steps_longest
+    total_steps = sum(d.P for d in dets)
+    floor_ms = max(steps_longest * step_us, total_steps * step_us / slots) * 1e-3
+    out = {"kernel": "batch_sweep_kernel", "sweep_ms": sweep_ms, "steps_total": total_steps,
+           "longest_chain_steps": steps_longest, "slots": slots, "step_us_alone": step_us,
+           "chain_floor_ms": steps_longest * step_us * 1e-3,
+           "throughput_floor_ms": total_steps * step_us / slots * 1e-3,
+           "floor_ms": floor_ms, "frac": floor_ms / sweep_ms,
+           "step_us_in_batch": sweep_ms * 1e3 * slots / total_steps,
+           "note": "floor = max(longest chain, all steps / slots) at the step latency of a chain running alone; "
+                   "frac < 1 is what sharing an SM between chains costs"}
+    if sm_mhz:
+        out["cycles_per_step_alone"] = step_us * sm_mhz
+        out["cycles_per_step_in_batch"] = out["step_us_in_batch"] * sm_mhz
+    return out
+
+
+def sfu_roofline(dets, dict_size: int, detect_ms: float, sms: int, sm_mhz: float | None) -> dict:
+    """Exponential-unit bound of the batch's detection: per (data symbol,
+    dictionary pair) the pair form needs 3 exponentials (ex2 on the SFU, 16
+    per clock per SM); the stage time includes the operand packing."""
+    pairs = sum(d.S * min(d.P, dict_size) for d in dets)
+    mhz = sm_mhz or 1965.0
+    floor_ms = 3.0 * pairs / (sms * 16 * mhz * 1e6) * 1e3
+    return {"kernel": "batch_gram_kernel + operand packing (detection stage)", "pair_evaluations": pairs,
+            "exponentials": 3 * pairs, "floor_ms": floor_ms, "stage_ms": detect_ms, "frac": floor_ms / detect_ms,
+            "clock_mhz": mhz}
+
+
 def run_batched(args, rank: int, world: int) -> dict | None:
     import torch
 
@@ -204,7 +256,12 @@ def run_batched(args, rank: int, world: int) -> dict | None:
     total_ms = sum(a.elapsed_time(b) for a, b in ev)
 
     # SER of the estimates (hard decisions of the reference's Gray map)
-    sers = [L.symbol_error_rate(x[3].cpu().numpy(), d.tx_data, d.modulation) for d, x in zip(dets, dev_in)]
+    est_batched = [x[3].cpu().numpy() for x in dev_in]
+    sers = [L.symbol_error_rate(e, d.tx_data, d.modulation) for d, e in zip(dets, est_batched)]
+    sweep = float(np.median(stage["sweep"]))
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    slots = sms * (shape["sweep_ctas_per_sm"] or 2)
+    lat = latency_roofline(pool, L, dets, ids, dev_in, sweep, slots, clk.get("sm_mhz"))
 
     # ---- e2e: host buffers through the C ABI (staging + copies inside) ----
     pinned = []  # page-locked host copies of the frames (the e2e inputs and outputs)
@@ -232,16 +289,35 @@ def run_batched(args, rank: int, world: int) -> dict | None:
     h2d = sum(d.rx_train.nbytes + d.tx_train.nbytes + d.rx_data.nbytes for d in dets)
     d2h = sum(8 * d.S for d in dets)
 
+    # ---- e2e with pageable host buffers (ordinary numpy arrays, as the reference's std::vector) ----
+    page_jobs = ([L.PoolJob(i, np.ascontiguousarray(d.rx_train), np.ascontiguousarray(d.tx_train), fresh=True)
+                  for i, d in zip(ids, dets)] +
+                 [L.PoolJob(i, np.ascontiguousarray(d.rx_data), est=np.zeros(d.S, np.complex64))
+                  for i, d in zip(ids, dets)])
+    prepared_pg = pool.prepare(page_jobs)
+    for _ in range(2):
+        pool.run_prepared(prepared_pg)
+    pg_ms = []
+    for _ in range(max(2, args.steps // 2)):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pool.run_prepared(prepared_pg)
+        pg_ms.append((time.perf_counter() - t0) * 1e3)
+
     symbols, total_ms, e2e_total = replica_totals(sum(d.S for d in dets), total_ms, sum(e2e_ms), world, "cuda")
     if rank != 0:
         return None
 
     ms_step = total_ms / args.steps
-    sweep = float(np.median(stage["sweep"]))
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak_gbs = float(peaks.get("hbm_gbs", 6650.0))
     alg = sweep_algorithmic_bytes(dets, 80, 2000)
     achieved = alg / (sweep * 1e-3) / 1e9
+    col_entries = sweep_column_entries(dets, 2000)
+    pilots = sum(d.P for d in dets)
+    plain_same = run_plain_same(dets, dev_in, est_batched) if not args.no_extras else None
     return {
         "metric": METRIC, "value": symbols / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -250,7 +326,14 @@ def run_batched(args, rank: int, world: int) -> dict | None:
                        launch_shape=dict(shape, chosen_by="built-in (0 = built-in choice)" if args.no_autotune
                                          else "apsm_pool_autotune")),
         "e2e": {"value": symbols / (e2e_total / args.steps * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_total / args.steps},
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_total / args.steps,
+                "host_buffers": "page-locked"},
+        "e2e_pageable": {"value": symbols / (float(np.median(pg_ms)) * 1e-3), "unit": UNIT,
+                         "ms_per_step": float(np.median(pg_ms)), "h2d_bytes_per_step": int(h2d),
+                         "d2h_bytes_per_step": int(d2h),
+                         "host_buffers": "pageable numpy arrays (staged by the pool's helper threads)"},
+        "training_samples_per_s": pilots / (ms_step * 1e-3),
+        "training_samples_per_s_train_stage": pilots / (float(np.median(stage["train"])) * 1e-3),
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "batch_sweep_kernel (training sweep, all 512 jobs)",
                      "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
@@ -259,25 +342,36 @@ def run_batched(args, rank: int, world: int) -> dict | None:
                      "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of an ncu capture of the "
                                        "32-detector case (373.0 MB for 361.3 MB algorithmic), scaled to this "
                                        "launch by its algorithmic bytes",
-                     "note": "a chain of P dependent steps per detector: latency / shared-memory bound, "
-                             "not HBM; see profiles/",
+                     "note": "a chain of P dependent steps per detector: bound by step latency (see "
+                             "roofline_latency), not HBM; see profiles/",
+                     "self_inflicted_bytes": {"kernel_columns_written": 16 * col_entries,
+                                              "kernel_columns_read_by_sweep": 16 * col_entries,
+                                              "what": "the column launch writes every (pair, earlier pair) "
+                                                      "kernel value once and the sweep reads it back: traffic "
+                                                      "of the precomputed-column design, not of the algorithm's "
+                                                      "inputs"},
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+        "roofline_latency": lat,
+        "roofline_sfu": sfu_roofline(dets, 2000, float(np.median(stage["detect"])), sms, clk.get("sm_mhz")),
         "stage_ms": {k: float(np.median(v)) for k, v in stage.items()},
         "ser_mean": float(np.mean(sers)), "clocks": clk,
+        "plain_same_workload": plain_same,
     }
 
 
 # -------------------------------------------------- plain per-detector form --
-def run_plain(steps: int = 5, warmup: int = 3) -> dict:
+def run_plain(steps: int = 5, warmup: int = 3, detect_version: str = "balanced", compare: bool = True) -> dict:
     """The reference's per-detector API (NomaDetector per user) on one
-    config-1 frame: 8 users, N=16, 1000 pilots, 8000 symbols, FP32."""
+    config-1 frame: 8 users, N=16, 1000 pilots, 8000 symbols, FP32 (or the
+    detection form `detect_version`); with `compare`, the LLS baselines and
+    the reference library's own kernels on the same frame."""
     import torch
 
     import libapsm_b200 as L
     from libapsm_b200 import synth
 
     frame = synth.config1_frame(seed=1)
-    cfg = dict(synth.CONFIG1_ALGORITHM)
+    cfg = dict(synth.CONFIG1_ALGORITHM, detectVersion=detect_version)
     U, N = frame.tx_train.shape[0], frame.rx_train.shape[0]
     S = frame.rx_data.shape[1]
     det = L.NomaDetectorFactory.build(cfg, N, num_users=U)
@@ -302,9 +396,126 @@ def run_plain(steps: int = 5, warmup: int = 3) -> dict:
             ev[i][1].record(stream)
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in ev) / steps
-    return {"value": U * S / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
-            "workload": "16QAM K=8 users N=16 P=1000 S=8000 window=80 dictionary=1000, NomaDetector per user "
-                        "(exact FP32 sweep + BALANCED-order detect)"}
+    mod = frame.modulation
+
+    def ser(est_users):
+        return float(np.mean([L.symbol_error_rate(est_users[u], frame.tx_data[u], mod) for u in range(U)]))
+
+    out = {"value": U * S / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "ser": ser(est.cpu().numpy()),
+           "detect": detect_version,
+           "workload": "16QAM K=8 users N=16 P=1000 S=8000 window=80 dictionary=1000, NomaDetector per user "
+                       "(exact FP32 sweep + BALANCED-order detect), all 8 users"}
+    if not compare:
+        det.close()
+        return out
+
+    # LLS linear baseline on our own kernels (FP64 normal equations + Cholesky), same frame
+    lls = L.NomaDetectorFactory.build({"otype": "LLS"}, N, num_users=U)
+    lls.train(frame.rx_train, frame.tx_train)
+    lls.detect(frame.rx_data)
+    t0 = time.perf_counter()
+    lls.train(frame.rx_train, frame.tx_train)
+    e_lls, _ = lls.detect(frame.rx_data)
+    out["lls"] = {"ser": ser(e_lls.reshape(U, S)), "ms_wall": (time.perf_counter() - t0) * 1e3,
+                  "what": "LLS detector on this library's kernels, host buffers, train + detect of all 8 users"}
+    lls.close()
+    det.close()
+    out["reference_cuda"] = reference_cuda_config1(frame, dict(synth.CONFIG1_ALGORITHM))
+    return out
+
+
+def reference_cuda_config1(frame, cfg) -> dict | None:
+    """The reference library itself (built from its sources for sm_100a) on the
+    same config-1 frame: one NomaDetector per user, as its CLI runs them, with
+    the reference's own CUDA-event times (train / detect, noma_detect.cpp:136-138)
+    and its cuBLAS LLS baseline (lls_detector.cu:175,217)."""
+    import libapsm_b200 as L
+    from oracle import oracle as O
+
+    if not O.reference_available():
+        return None
+    U, N = frame.tx_train.shape[0], frame.rx_train.shape[0]
+    mod = frame.modulation
+    r = O.ReferenceDetector(cfg, N)  # warm-up (context, module load)
+    r.train(frame.rx_train[:, :64], frame.tx_train[0, :64])
+    del r
+    train_ms = detect_ms = 0.0
+    sers = []
+    t0 = time.perf_counter()
+    for u in range(U):
+        r = O.ReferenceDetector(cfg, N)
+        train_ms += r.train(frame.rx_train, frame.tx_train[u])
+        e, dms = r.detect(frame.rx_data)
+        detect_ms += dms
+        sers.append(L.symbol_error_rate(e, frame.tx_data[u], mod))
+        del r
+    wall = time.perf_counter() - t0
+    S = frame.rx_data.shape[1]
+    out = {"train_ms": train_ms, "detect_ms": detect_ms, "wall_ms": wall * 1e3, "ser": float(np.mean(sers)),
+           "value_events": U * S / ((train_ms + detect_ms) * 1e-3), "value_wall": U * S / wall, "unit": UNIT,
+           "what": "reference NomaDetector per user (8 users, one after the other); train/detect ms are its own "
+                   "CUDA-event times summed over the users"}
+    lls_ms, lls_sers = 0.0, []
+    for u in range(U):
+        r = O.ReferenceDetector({"otype": "LLS"}, N)
+        lls_ms += r.train(frame.rx_train, frame.tx_train[u])
+        e, dms = r.detect(frame.rx_data)
+        lls_ms += dms
+        lls_sers.append(L.symbol_error_rate(e, frame.tx_data[u], mod))
+        del r
+    out["lls"] = {"ser": float(np.mean(lls_sers)), "ms_events": lls_ms,
+                  "what": "reference cuBLAS LLS detector (Sgels train, Sgemm detect), 8 users, its own event times"}
+    return out
+
+
+def run_plain_same(dets, dev_in, est_batched) -> dict:
+    """The plain per-detector FP32 form on the batched workload itself: one
+    NomaDetector (the reference's API) per detector, fresh train + detect of
+    the same 512 frames, device-resident inputs, one detector after the
+    other (the reference's calls return when their GPU work is done).  SER of
+    both forms on the same frames."""
+    import torch
+
+    import libapsm_b200 as L
+    from libapsm_b200 import synth
+
+    cfg = dict(synth.CONFIG2_ALGORITHM)
+    handles = {N: L.NomaDetectorFactory.build(cfg, N) for N in sorted({d.N for d in dets})}
+    outs = [torch.empty(d.S, dtype=torch.complex64, device="cuda") for d in dets]
+
+    def one(i):
+        h = handles[dets[i].N]
+        h.reset_state()
+        h.train_device(dev_in[i][0], dev_in[i][1])
+        h.detect_device(dev_in[i][2], outs[i])
+        h.synchronize()
+
+    for i in range(4):  # warm-up (workspaces of each antenna count)
+        one(i)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(len(dets)):
+        one(i)
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    symbols = sum(d.S for d in dets)
+    err_p = err_b = diff = 0
+    for d, o, eb in zip(dets, outs, est_batched):
+        ep = o.cpu().numpy()
+        true = d.modulation.hard_decode_int(d.tx_data)
+        dp, db = d.modulation.hard_decode_int(ep), d.modulation.hard_decode_int(eb)
+        err_p += int(np.sum(dp != true))
+        err_b += int(np.sum(db != true))
+        diff += int(np.sum(dp != db))
+    for h in handles.values():
+        h.close()
+    ser_p, ser_b = err_p / symbols, err_b / symbols
+    return {"value": symbols / secs, "unit": UNIT, "seconds": secs, "ser_plain": ser_p, "ser_batched": ser_b,
+            "ser_rel_diff": abs(ser_b - ser_p) / ser_p if ser_p else 0.0, "decisions_differing": diff,
+            "symbols": symbols,
+            "what": "NomaDetector per detector (exact FP32 sweep + BALANCED-order detect), the 512 frames of the "
+                    "batched workload one after the other, device-resident inputs, wall clock with the GPU "
+                    "synchronised per detector"}
 
 
 # ------------------------------------------------- large-detect precision --
@@ -500,14 +711,29 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
 
 
 # ----------------------------------------------------------- reference arm --
-def cpu_baseline(n_sample: int = 2) -> dict:
-    """The FP32 restatement of the reference algorithm on the host cores, on
-    a bounded sample of the batched workload (the first n_sample detectors)."""
+def cpu_sample(per_class: int = 6) -> list:
+    """A bounded sample of the batched workload stratified by antenna count:
+    the first `per_class` detectors of each antenna class {4, 8, 16, 32} in
+    the 512-detector draw (their pilot and data lengths as drawn)."""
+    from libapsm_b200 import synth
+
+    dets = synth.config2_detectors(N_DET, seed=2)
+    out = []
+    for N in (4, 8, 16, 32):
+        out += [d for d in dets if d.N == N][:per_class]
+    return out
+
+
+def cpu_baseline(per_class: int = 6) -> dict:
+    """The FP32 restatement of the reference algorithm on the host cores
+    (OpenMP over all host threads), on a bounded, antenna-stratified sample of
+    the batched workload.  Also the share of the full batch's work the sample
+    holds, so that its time can be set against the batch's."""
     from libapsm_b200 import synth
     from oracle import oracle as O
 
     threads = O.set_threads(os.cpu_count() or 1)
-    dets = synth.config2_detectors(n_sample, seed=2)
+    dets = cpu_sample(per_class)
     cfg = dict(synth.CONFIG2_ALGORITHM)
     t0 = time.perf_counter()
     syms = 0
@@ -517,8 +743,11 @@ def cpu_baseline(n_sample: int = 2) -> dict:
         o.detect(d.rx_data)
         syms += d.S
     dt = time.perf_counter() - t0
+    P = sum(d.P for d in dets)
     return {"value": syms / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n_sample} of the 512 detectors (train + detect each, {syms} symbols), {dt:.2f} s"}
+            "training_samples_per_s": P / dt,
+            "sample": f"{len(dets)} of the 512 detectors, the first {per_class} of each antenna class "
+                      f"(4/8/16/32), train + detect each: {P} pilots, {syms} symbols, {dt:.2f} s"}
 
 
 def reference_cuda(n_sample: int = 16) -> dict | None:
@@ -592,9 +821,17 @@ def main():
                     help="run only the large-detect precision study (N=64, dictionary 8192) and print it")
     ap.add_argument("--serving-only", action="store_true",
                     help="run only the served form (FP32 pair form and BF16 Gram detection) and print it")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="run only the plain per-detector form on the config-1 frame (8 users, N=16) and print it")
+    ap.add_argument("--plain-detect-version", default="balanced",
+                    help="detection form of --plain-only (balanced, gram_bf16, gram_bf16x3, gram_tf32, gram_tf32x3)")
     args = ap.parse_args()
     if args.precision_only:
         print(json.dumps({"precision": run_precision_study()}), flush=True)
+        return
+    if args.plain_only:
+        print(json.dumps({"plain": run_plain(steps=max(1, args.steps), warmup=max(1, args.warmup),
+                                             detect_version=args.plain_detect_version, compare=False)}), flush=True)
         return
     if args.serving_only:
         print(json.dumps({"serving": run_serving(), "serving_gram_bf16": run_serving(detect_version="gram_bf16")}),
@@ -626,6 +863,12 @@ def main():
         line["serving"] = run_serving()
         os.environ.pop("APSM_POOL_TRACE", None)
         line["serving_gram_bf16"] = run_serving(detect_version="gram_bf16")
+        line["serving_p50_us"] = line["serving"]["p50_us"]
+        line["serving_p99_us"] = line["serving"]["p99_us"]
+        line["serving_deadline_met"] = line["serving"]["deadline_500us_met"]
+        ps = line.get("plain_same_workload") or {}
+        if ps.get("value"):
+            line["batched_over_plain"] = line["value"] / ps["value"]
         line["precision"] = run_precision_study()
     if line is not None and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
