@@ -621,7 +621,7 @@ def run_precision_study(reps: int = 3, sample: int = 2048) -> dict:
 
 # ------------------------------------------------------------ serving form --
 def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = N_DET, lanes: int = 8,
-                max_batch: int = 16, detect_version: str = "balanced") -> dict:
+                max_batch: int = 16, detect_version: str = "balanced", deadline_s: float = 500e-6) -> dict:
     """Poisson per-TTI requests against resident detectors through the
     request server (continuous batching over `lanes` streams, at most
     `max_batch` requests of one kind per batch), detection in the FP32
@@ -629,7 +629,9 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
     Request samples sit in
     page-locked host buffers, as a radio front end's DMA buffers would; the
     latency of a request runs from its submission to its completion as the
-    server's clock sees them (host samples in, estimates back in host memory)."""
+    server's clock sees them (host samples in, estimates back in host memory).
+    Each request carries the 500 us deadline: one not admitted into a batch by
+    then is dropped (counted, and as a missed deadline in the percentiles)."""
     import torch
 
     import libapsm_b200 as L
@@ -677,6 +679,7 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
         srv.wait(t)
     prepared = [(ta, kind, n, srv.make_job(job(d, kind, n))) for (ta, d, kind, n) in reqs]
     b0, j0 = srv.stats()
+    srv.set_deadline(deadline_s)  # a request not admitted within the deadline is dropped
     start = clock() + 0.01
     tickets = []
     for (ta, kind, n, prep) in prepared:
@@ -684,10 +687,16 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
         while clock() < target:
             pass
         tickets.append(srv.submit_prepared(prep))
-    lat, kinds, syms, done = [], [], 0, []
+    lat, kinds, syms, done, dropped, failed = [], [], 0, [], 0, 0
     for (ta, kind, n, prep), tk in zip(prepared, tickets):
-        srv.wait(tk)
+        st = srv.wait_status(tk)
         s0, s1, s2 = srv.times(tk)
+        if st != 0:
+            dropped += st == L._native.APSM_ERR_DEADLINE
+            failed += st != L._native.APSM_ERR_DEADLINE
+            lat.append(float("inf"))
+            kinds.append(kind)
+            continue
         lat.append(s2 - s0)
         kinds.append(kind)
         done.append(s2)
@@ -701,6 +710,7 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
     return {"p50_us": pct(lat_us, 50), "p99_us": pct(lat_us, 99),
             "train_p99_us": pct(lat_us[is_train], 99), "detect_p99_us": pct(lat_us[~is_train], 99),
             "deadline_500us_met": float(np.mean(lat_us <= 500.0)), "symbols_per_s": syms / (max(done) - start),
+            "deadline_s": deadline_s, "dropped_at_deadline": int(dropped), "failed": int(failed),
             "requests": len(reqs), "rate_hz": rate_hz, "duration_s": duration_s, "batches": int(b - b0),
             "avg_batch": float((jb - j0) / max(1, b - b0)), "lanes": lanes, "max_batch": max_batch,
             "detect": "FP32 CUDA-core pair form" if detect_version == "balanced" else

@@ -35,7 +35,9 @@ typedef enum {
     APSM_ERR_OUT_OF_MEMORY = 4,    /* device allocation failed or would exceed the handle's memory budget */
     APSM_ERR_UNSUPPORTED = 5,      /* valid config the B200 kernels do not implement (e.g. antenna count above the maximum) */
     APSM_ERR_NO_DEVICE = 6,        /* no usable sm_100 device */
-    APSM_ERR_TIMEOUT = 7           /* a host-side wait ran out of time */
+    APSM_ERR_TIMEOUT = 7,          /* a host-side wait ran out of time */
+    APSM_ERR_DEADLINE = 8,         /* a served request was not admitted into a batch by its deadline (dropped) */
+    APSM_ERR_CANCELLED = 9         /* a served request was cancelled before it was admitted */
 } apsm_status;
 
 typedef struct apsm_detector apsm_detector;
@@ -147,7 +149,10 @@ apsm_status apsm_detect_device(apsm_detector* h, const float* d_rx, uint32_t S, 
  * the reference's detectVersion values only (else APSM_ERR_UNSUPPORTED).  The
  * first call on a device looks up the array's address (make it before any
  * stream capture); the array is shared by all handles on the device, so calls
- * that overlap on a device race and must be serialised by the caller.
+ * that overlap on a device race and must be serialised by the caller.  The
+ * looked-up address is kept for the life of the process: cudaDeviceReset on a
+ * device that has used this entry point is not supported (the library's
+ * module would load again, possibly at another address).
  */
 apsm_status apsm_detect_device_noalloc(apsm_detector* h, const float* d_rx, uint32_t S, float* d_est, void* stream);
 
@@ -256,20 +261,33 @@ apsm_status apsm_pool_reset(apsm_pool* p, uint32_t detector);
 
 /* Runs a batch on a lane: all training jobs first (in one sweep launch; a
  * detector may be trained at most once per batch), then all detection jobs,
- * which see this batch's training.  Host modes stage every input through one
- * pinned buffer (one host-to-device copy with the job descriptors) and bring
- * every estimate back in one device-to-host copy; the caller keeps its
- * buffers alive until the batch finished.  A detector must not be in batches
- * on two lanes at once. */
+ * which see this batch's training.  Host modes, inputs: a batch with 4 MB or
+ * more of training inputs whose buffers are page-locked and mapped for the
+ * device has them read in place by the packing kernel; detection samples in
+ * page-locked buffers are copied to the device straight from them on a second
+ * stream while the batch trains; everything else (pageable buffers, small
+ * batches) is staged by host helper threads through the lane's pinned buffer
+ * and uploaded with the job descriptors.  Estimates: into page-locked,
+ * device-mapped caller buffers (batches with 4 MB of estimates or more) the
+ * detection kernels write them in place, so such buffers hold partial
+ * estimates while the batch runs; otherwise each launch's estimates come
+ * back in one device-to-host copy and are scattered to the callers' buffers
+ * when the batch is finished.  The caller keeps its buffers alive until the
+ * batch finished.  A later run (or reserve / autotune) on the lane finishes
+ * a lane's pending APSM_RUN_HOST_ASYNC batch first and returns its status if
+ * it failed.  A detector must not be in batches on two lanes at once. */
 apsm_status apsm_pool_run(apsm_pool* p, uint32_t lane, const apsm_job* jobs, uint32_t n_jobs, int mode);
 /* Waits for the lane's last batch and, for APSM_RUN_HOST_ASYNC, writes its
- * estimates to the caller's buffers. */
+ * estimates to the caller's buffers; returns the batch's status (an expired
+ * bounded wait of a tensor-core kernel: APSM_ERR_CUDA). */
 apsm_status apsm_pool_wait(apsm_pool* p, uint32_t lane);
 
 /*
  * Grows the lane's device scratch and page-locked buffers to what this batch
  * (same arguments as apsm_pool_run) needs, without running it or changing any
- * detector; returns once the memory is in place.  A lane grows its buffers on
+ * detector; returns once the memory is in place.  A pending
+ * APSM_RUN_HOST_ASYNC batch of the lane is finished first (its estimates are
+ * written, its failure is returned): growth retires the buffers it reads.  A lane grows its buffers on
  * demand otherwise, and growing them (mapping device memory, page-locking
  * host memory) stalls the batch that needs it for milliseconds: a request
  * server reserves every lane for its largest batch before taking requests.
@@ -316,6 +334,22 @@ apsm_status apsm_pool_last_sweep_ms(apsm_pool* p, uint32_t lane, float* sweep_ms
 /* Kernels the lane's last batch launched (its own kernels; memsets and copies excluded). */
 int apsm_pool_last_launches(apsm_pool* p, uint32_t lane);
 
+/* The checks apsm_pool_run applies to one job on its own: known detector and
+ * kind, buffers present (APSM_ERR_INVALID_ARGUMENT otherwise).  Reads the
+ * detector table without locking: not concurrently with apsm_pool_add /
+ * apsm_pool_remove.  No counterpart in the reference. */
+apsm_status apsm_pool_check_job(const apsm_pool* p, const apsm_job* job);
+
+/* Host-side fault injection, for tests of the failure paths (no counterpart in
+ * the reference, whose CUDA errors end the process).  APSM_FAULT_LANE_ALLOC:
+ * the pool's next `count` lane-scratch growths fail as an allocation would
+ * (the batch returns APSM_ERR_OUT_OF_MEMORY; the lane grows again on a later
+ * batch).  APSM_FAULT_DROP_REQUEST (server): the next `count` submitted
+ * requests are lost on their way into the queue; they end only by their
+ * deadline (APSM_ERR_DEADLINE) or apsm_server_cancel.  Nothing faults the GPU. */
+typedef enum { APSM_FAULT_LANE_ALLOC = 1, APSM_FAULT_DROP_REQUEST = 2 } apsm_fault;
+apsm_status apsm_pool_inject_fault(apsm_pool* p, int fault, uint32_t count);
+
 /* Snapshot of a detector: rows in use, a (rows), w (2N); pointers may be NULL. */
 apsm_status apsm_pool_get_state(apsm_pool* p, uint32_t detector, uint32_t* rows, float* a, float* w);
 const char* apsm_pool_last_error(const apsm_pool* p);
@@ -337,9 +371,30 @@ const char* apsm_pool_last_error(const apsm_pool* p);
 typedef struct apsm_server apsm_server;
 
 apsm_status apsm_server_create(apsm_pool* pool, uint32_t lanes, uint32_t max_batch, apsm_server** out);
-/* Finishes every submitted request, then stops the worker. */
+/* Finishes every queued request, then stops the worker. */
 void apsm_server_destroy(apsm_server* s);
+/* Queues a request (deadline: the server's default).  A malformed request
+ * (apsm_pool_check_job) or one whose scratch alone exceeds the pool's HBM
+ * budget is rejected here (APSM_ERR_INVALID_ARGUMENT / APSM_ERR_OUT_OF_MEMORY,
+ * no ticket), so it cannot fail the batch it would join. */
 apsm_status apsm_server_submit(apsm_server* s, const apsm_job* job, uint64_t* ticket);
+/* As apsm_server_submit, with a deadline deadline_s seconds after submission
+ * (0: none; < 0: the server's default).  A request not admitted into a batch
+ * by its deadline ends with APSM_ERR_DEADLINE without running; one admitted
+ * in time runs to completion (its completion time, apsm_server_times, may be
+ * later than the deadline).  A dropped training request leaves the detector's
+ * state as it was; the detector's later requests proceed. */
+apsm_status apsm_server_submit_deadline(apsm_server* s, const apsm_job* job, double deadline_s, uint64_t* ticket);
+/* Default deadline (seconds after submission, 0: none) of later submissions. */
+apsm_status apsm_server_set_deadline(apsm_server* s, double seconds);
+/* Ends a request that is not admitted yet with APSM_ERR_CANCELLED.  A request
+ * already on the GPU runs to completion (APSM_ERR_UNSUPPORTED); a finished or
+ * unknown one: APSM_ERR_INVALID_ARGUMENT. */
+apsm_status apsm_server_cancel(apsm_server* s, uint64_t ticket);
+/* Requests dropped at their deadline, cancelled, and rejected at submission. */
+apsm_status apsm_server_counts(apsm_server* s, uint64_t* dropped, uint64_t* cancelled, uint64_t* rejected);
+/* See apsm_pool_inject_fault (APSM_FAULT_DROP_REQUEST). */
+apsm_status apsm_server_inject_fault(apsm_server* s, int fault, uint32_t count);
 /* 1 when the request finished (*status its result), 0 while pending, -1 unknown ticket. */
 int apsm_server_poll(apsm_server* s, uint64_t ticket, apsm_status* status);
 /* Blocks until the request finished (its status) or timeout_s passed (APSM_ERR_TIMEOUT). */

@@ -20,6 +20,10 @@ APSM_ERR_OUT_OF_MEMORY = 4
 APSM_ERR_UNSUPPORTED = 5
 APSM_ERR_NO_DEVICE = 6
 APSM_ERR_TIMEOUT = 7
+APSM_ERR_DEADLINE = 8
+APSM_ERR_CANCELLED = 9
+APSM_FAULT_LANE_ALLOC = 1
+APSM_FAULT_DROP_REQUEST = 2
 
 STATUS_NAMES = {
     APSM_OK: "APSM_OK",
@@ -30,6 +34,8 @@ STATUS_NAMES = {
     APSM_ERR_UNSUPPORTED: "APSM_ERR_UNSUPPORTED",
     APSM_ERR_NO_DEVICE: "APSM_ERR_NO_DEVICE",
     APSM_ERR_TIMEOUT: "APSM_ERR_TIMEOUT",
+    APSM_ERR_DEADLINE: "APSM_ERR_DEADLINE",
+    APSM_ERR_CANCELLED: "APSM_ERR_CANCELLED",
 }
 
 # (name, restype, argtypes) of every exported entry point
@@ -82,10 +88,18 @@ SIGNATURES = [
     ("apsm_pool_last_launches", ctypes.c_int, [_P, _U32]),
     ("apsm_pool_last_sweep_ms", ctypes.c_int, [_P, _U32, _F]),
     ("apsm_pool_set_timing", ctypes.c_int, [_P, ctypes.c_int]),
+    ("apsm_pool_check_job", ctypes.c_int, [_P, _P]),
+    ("apsm_pool_inject_fault", ctypes.c_int, [_P, ctypes.c_int, _U32]),
     # request server (continuous batching over a pool)
     ("apsm_server_create", ctypes.c_int, [_P, _U32, _U32, ctypes.POINTER(_P)]),
     ("apsm_server_destroy", None, [_P]),
     ("apsm_server_submit", ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    ("apsm_server_submit_deadline", ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64)]),
+    ("apsm_server_set_deadline", ctypes.c_int, [_P, ctypes.c_double]),
+    ("apsm_server_cancel", ctypes.c_int, [_P, ctypes.c_uint64]),
+    ("apsm_server_counts", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.POINTER(ctypes.c_uint64)]),
+    ("apsm_server_inject_fault", ctypes.c_int, [_P, ctypes.c_int, _U32]),
     ("apsm_server_poll", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int)]),
     ("apsm_server_wait", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_double]),
     ("apsm_server_times", ctypes.c_int, [_P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double),

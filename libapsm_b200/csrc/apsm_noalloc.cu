@@ -14,7 +14,9 @@
 //     names) of an APSM handle; other handles get APSM_ERR_UNSUPPORTED;
 //   * the array's device address is looked up once per device, by the first
 //     call on that device, with the handle's device current; make that first
-//     call before any stream capture;
+//     call before any stream capture.  The address is kept for the life of
+//     the process: cudaDeviceReset of such a device is not supported (the
+//     module would be loaded again, possibly at another address);
 //   * nothing in the scratch must start at zero: pack_rows_kernel writes every
 //     element of every packed row (padding columns included) before the
 //     detection kernel reads it;

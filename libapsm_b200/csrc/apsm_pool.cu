@@ -74,6 +74,7 @@ struct Lane {
     int* err = nullptr;           // error flag of the last batch (in the scratch)
     int* err_host = nullptr;      // its copy in page-locked memory, written by the batch's last copy
     bool err_copied = false;      // the last batch copies the flag (it has kernels that can set it)
+    bool unfinished = false;      // an APSM_RUN_HOST_ASYNC batch whose finish() has not run yet
     int launches = 0;             // kernels launched by the last batch
     // batch timeline (APSM_POOL_TRACE): stream start, inputs copied, packed, kernel columns, swept,
     // trained (dictionary copied back), detected
@@ -284,6 +285,7 @@ struct apsm_pool {
     std::mutex mu;
     std::FILE* trace = nullptr; // batch timeline lines (env APSM_POOL_TRACE = file path)
     bool timing = true;         // per-stage GPU events of each batch (apsm_pool_last_ms)
+    uint32_t fault_lane_alloc = 0; // lane-scratch growths still to fail (apsm_pool_inject_fault)
     cudaMemPool_t mempool = nullptr; // lane scratch (stream-ordered; keeps its memory mapped)
     Stager stager;                   // host-input staging (helper threads for large batches)
     std::map<uint32_t, std::vector<int>> perms;
@@ -336,6 +338,30 @@ struct apsm_pool {
     // reserve_only: plan the batch and grow the lane's buffers to its needs, run nothing
     apsm_status run(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode, bool reserve_only = false);
     apsm_status check_lane(uint32_t lane);
+    // Checks of one job that need no other job of its batch (touches no pool state).
+    apsm_status job_error(const apsm_job& j, std::string* msg) const
+    {
+        if (j.detector >= dets.size() || !dets[j.detector].live) {
+            *msg = "unknown detector";
+            return APSM_ERR_INVALID_ARGUMENT;
+        }
+        if (j.kind != APSM_JOB_TRAIN && j.kind != APSM_JOB_DETECT) {
+            *msg = "unknown kind";
+            return APSM_ERR_INVALID_ARGUMENT;
+        }
+        if (j.length == 0) return APSM_OK;
+        if (!j.rx) *msg = "null rx";
+        else if (j.kind == APSM_JOB_TRAIN && !j.tx) *msg = "null tx";
+        else if (j.kind == APSM_JOB_DETECT && !j.est) *msg = "null est";
+        else return APSM_OK;
+        return APSM_ERR_INVALID_ARGUMENT;
+    }
+    apsm_status check_job(const apsm_job& j, const std::string& what)
+    {
+        std::string msg;
+        const apsm_status st = job_error(j, &msg);
+        return st == APSM_OK ? st : fail(st, what + ": " + msg);
+    }
     apsm_status finish(uint32_t lane); // wait for the lane, hand out estimates, check its error flag
     apsm_status autotune(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode, std::string* report);
 };
@@ -468,8 +494,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     Lane& L = lanes[lane_id];
     const bool host = mode != APSM_RUN_DEVICE;
     const double t_run0 = trace ? host_us() : 0.0;
-    if (!L.pending.empty()) {
-        apsm_status st = finish(lane_id); // the lane's previous host batch
+    if (!L.pending.empty() || L.unfinished) {
+        apsm_status st = finish(lane_id); // the lane's previous host batch (its estimates, its error flag)
         if (st != APSM_OK) return st;
     }
     const uint32_t cap = 2 * cfg.dict_size;
@@ -479,28 +505,13 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     std::vector<char> trained(dets.size(), 0);
     for (uint32_t i = 0; i < n; ++i) {
         const apsm_job& j = jobs[i];
-        if (j.detector >= dets.size() || !dets[j.detector].live)
-            return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": unknown detector");
-        if (j.kind != APSM_JOB_TRAIN && j.kind != APSM_JOB_DETECT)
-            return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": unknown kind");
-        if (j.length == 0) {
-            if (j.kind == APSM_JOB_TRAIN && (j.flags & APSM_JOB_FRESH)) {
-                if (trained[j.detector])
-                    return fail(APSM_ERR_INVALID_ARGUMENT, "detector " + std::to_string(j.detector) +
-                                                               " is trained twice in one batch");
-                trained[j.detector] = 1;
-            }
-            continue;
-        }
-        if (!j.rx) return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null rx");
-        if (j.kind == APSM_JOB_TRAIN) {
-            if (!j.tx) return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null tx");
+        const apsm_status st = check_job(j, "job " + std::to_string(i));
+        if (st != APSM_OK) return st;
+        if (j.kind == APSM_JOB_TRAIN && (j.length > 0 || (j.flags & APSM_JOB_FRESH))) {
             if (trained[j.detector])
                 return fail(APSM_ERR_INVALID_ARGUMENT, "detector " + std::to_string(j.detector) +
                                                            " is trained twice in one batch");
             trained[j.detector] = 1;
-        } else if (!j.est) {
-            return fail(APSM_ERR_INVALID_ARGUMENT, "job " + std::to_string(i) + ": null est");
         }
     }
 
@@ -767,6 +778,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         if (L.scratch) POOL_CK(cudaFreeAsync(L.scratch, L.stream));
         L.scratch = nullptr;
         L.scratch_bytes = 0;
+        if (fault_lane_alloc > 0) { // injected (tests): this growth fails as an allocation would
+            --fault_lane_alloc;
+            return fail(APSM_ERR_OUT_OF_MEMORY, "lane scratch growth failed (injected fault)");
+        }
         POOL_CK(cudaMallocFromPoolAsync(&L.scratch, want, mempool, L.stream));
         L.scratch_bytes = want;
     }
@@ -1141,6 +1156,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     }
     POOL_CK(cudaEventRecord(L.done, s));
     if (mode == APSM_RUN_HOST) return finish(lane_id);
+    L.unfinished = mode == APSM_RUN_HOST_ASYNC;
     return APSM_OK;
 }
 
@@ -1155,7 +1171,7 @@ apsm_status apsm_pool::autotune(uint32_t lane_id, const apsm_job* jobs, uint32_t
 {
     apsm_pool* p = this;
     Lane& L = lanes[lane_id];
-    if (!L.pending.empty()) {
+    if (!L.pending.empty() || L.unfinished) {
         apsm_status st = finish(lane_id);
         if (st != APSM_OK) return st;
     }
@@ -1274,6 +1290,7 @@ apsm_status apsm_pool::finish(uint32_t lane_id)
     Lane& L = lanes[lane_id];
     const double t0 = trace ? host_us() : 0.0;
     POOL_CK(cudaEventSynchronize(L.done));
+    L.unfinished = false;
     const double t1 = trace ? host_us() : 0.0;
     {
         std::vector<Stager::Range> pieces;
@@ -1587,6 +1604,21 @@ extern "C" uint64_t apsm_pool_job_bytes(const apsm_pool* p, const apsm_job* job)
     if (!p || !job || job->detector >= p->dets.size() || !p->dets[job->detector].live) return 0;
     const PoolDet& d = p->dets[job->detector];
     return job->kind == APSM_JOB_TRAIN ? p->train_bytes(d, job->length, true) : p->detect_bytes(d, job->length, true);
+}
+
+extern "C" apsm_status apsm_pool_check_job(const apsm_pool* p, const apsm_job* job)
+{
+    if (!p || !job) return APSM_ERR_INVALID_ARGUMENT;
+    std::string msg;
+    return p->job_error(*job, &msg);
+}
+
+extern "C" apsm_status apsm_pool_inject_fault(apsm_pool* p, int fault, uint32_t count)
+{
+    if (!p || fault != APSM_FAULT_LANE_ALLOC) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(p->mu);
+    p->fault_lane_alloc = count;
+    return APSM_OK;
 }
 
 extern "C" uint64_t apsm_pool_budget(const apsm_pool* p) { return p ? p->budget : 0; }

@@ -19,6 +19,23 @@
 //     batch, keeping its order).
 // Batches on different lanes overlap on the device.  Request times are taken
 // with a monotonic host clock: submission, admission and completion.
+//
+// Failure model (the reference's is CUDA_CHECK: print and exit, cpp/lib/cuda/
+// cuda_errorhandling.cuh:98-134).  Every ticket ends with a status:
+//   * a request that is not admitted into a batch by its deadline is dropped
+//     (APSM_ERR_DEADLINE); one admitted in time runs to completion, and its
+//     completion time tells whether it finished late;
+//   * apsm_server_cancel ends a request that is not admitted yet
+//     (APSM_ERR_CANCELLED);
+//   * a malformed request (unknown detector or kind, missing buffer) or one
+//     whose scratch alone exceeds the pool's HBM budget is rejected at
+//     submission: no ticket, so it can never fail the batch it would join;
+//   * a batch whose launch fails (e.g. its lane's scratch cannot grow) ends
+//     its requests with that status; the pool and the server stay usable.
+// Fault injection for tests of these paths is host-side only: the pool can
+// fail its next lane-scratch growths (apsm_pool_inject_fault) and the server
+// can lose its next submitted requests (apsm_server_inject_fault), which then
+// end only by their deadline or a cancel.
 #include "apsm_b200.h"
 
 #include <algorithm>
@@ -43,8 +60,10 @@ double now_s()
 struct ServerReq {
     apsm_job job;
     double t_submit = 0, t_start = 0, t_done = 0;
+    double deadline = 0; // server clock, 0: none
     apsm_status st = APSM_OK;
     int state = 0; // 0 waiting, 1 running, 2 done
+    bool lost = false; // dropped on the way in (fault injection): never queued
 };
 
 } // namespace
@@ -64,11 +83,65 @@ struct apsm_server {
     std::unordered_set<uint32_t> busy_dets;
     uint64_t next_ticket = 1;
     uint64_t batches = 0, batched = 0;
+    uint64_t dropped = 0, cancelled = 0, rejected = 0;
+    double default_deadline = 0; // seconds after submission, 0: none
+    uint32_t fault_drop = 0;     // requests still to lose on submission (fault injection)
+    std::unordered_set<uint64_t> lost;
 
     void run();
     void complete(uint32_t lane, apsm_status st);
+    void finish_one(uint64_t tk, apsm_status st, double t);
+    void expire(double t);
+    double next_deadline() const;
     bool admit(uint32_t lane);
 };
+
+void apsm_server::finish_one(uint64_t tk, apsm_status st, double t)
+{
+    auto it = reqs.find(tk);
+    if (it == reqs.end()) return;
+    it->second.state = 2;
+    it->second.st = st;
+    it->second.t_done = t;
+    cv_done.notify_all();
+}
+
+// Drops the waiting (and lost) requests whose deadline passed; called with mu held.
+void apsm_server::expire(double t)
+{
+    for (auto it = queue.begin(); it != queue.end();) {
+        const ServerReq& r = reqs[*it];
+        if (r.deadline > 0 && t > r.deadline) {
+            finish_one(*it, APSM_ERR_DEADLINE, t);
+            ++dropped;
+            it = queue.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    for (auto it = lost.begin(); it != lost.end();) {
+        const ServerReq& r = reqs[*it];
+        if (r.deadline > 0 && t > r.deadline) {
+            finish_one(*it, APSM_ERR_DEADLINE, t);
+            ++dropped;
+            it = lost.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+double apsm_server::next_deadline() const
+{
+    double d = 0;
+    auto take = [&](uint64_t tk) {
+        auto it = reqs.find(tk);
+        if (it != reqs.end() && it->second.deadline > 0 && (d == 0 || it->second.deadline < d)) d = it->second.deadline;
+    };
+    for (uint64_t tk : queue) take(tk);
+    for (uint64_t tk : lost) take(tk);
+    return d;
+}
 
 void apsm_server::complete(uint32_t lane, apsm_status st)
 {
@@ -89,6 +162,7 @@ void apsm_server::complete(uint32_t lane, apsm_status st)
 // Builds and launches a batch on an idle lane; called with mu held.
 bool apsm_server::admit(uint32_t lane)
 {
+    expire(now_s());
     if (queue.empty()) return false;
     const uint64_t budget = apsm_pool_budget(pool);
     uint64_t cap = ~0ull;
@@ -145,6 +219,7 @@ void apsm_server::run()
 {
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
+        expire(now_s());
         bool any_busy = false, progress = false;
         for (uint32_t l = 0; l < n_lanes; ++l) {
             if (!lane_busy[l]) continue;
@@ -172,7 +247,11 @@ void apsm_server::run()
             std::this_thread::yield(); // poll the lanes again
             lk.lock();
         } else {
-            cv_submit.wait_for(lk, std::chrono::milliseconds(1));
+            // idle: wake for a submission, the next deadline, or after 1 ms
+            double wait_s = 1e-3;
+            const double nd = next_deadline();
+            if (nd > 0) wait_s = std::max(0.0, std::min(wait_s, nd - now_s()));
+            cv_submit.wait_for(lk, std::chrono::duration<double>(wait_s));
         }
     }
 }
@@ -207,22 +286,94 @@ extern "C" void apsm_server_destroy(apsm_server* s)
     delete s;
 }
 
-extern "C" apsm_status apsm_server_submit(apsm_server* s, const apsm_job* job, uint64_t* ticket)
+extern "C" apsm_status apsm_server_submit_deadline(apsm_server* s, const apsm_job* job, double deadline_s,
+                                                   uint64_t* ticket)
 {
     if (!s || !job || !ticket) return APSM_ERR_INVALID_ARGUMENT;
-    if (job->kind != APSM_JOB_TRAIN && job->kind != APSM_JOB_DETECT) return APSM_ERR_INVALID_ARGUMENT;
+    // malformed or oversized requests are rejected here, so they never join (and fail) a batch
+    apsm_status chk = apsm_pool_check_job(s->pool, job);
+    if (chk == APSM_OK) {
+        const uint64_t budget = apsm_pool_budget(s->pool);
+        if (budget && apsm_pool_job_bytes(s->pool, job) > budget) chk = APSM_ERR_OUT_OF_MEMORY;
+    }
     {
         std::lock_guard<std::mutex> g(s->mu);
+        if (chk != APSM_OK) {
+            ++s->rejected;
+            return chk;
+        }
         if (s->stop) return APSM_ERR_INVALID_ARGUMENT;
         const uint64_t tk = s->next_ticket++;
         ServerReq r;
         r.job = *job;
         r.t_submit = now_s();
+        const double rel = deadline_s < 0 ? s->default_deadline : deadline_s;
+        r.deadline = rel > 0 ? r.t_submit + rel : 0;
+        if (s->fault_drop > 0) { // injected: the request is lost on its way into the queue
+            --s->fault_drop;
+            r.lost = true;
+            s->lost.insert(tk);
+        } else {
+            s->queue.push_back(tk);
+        }
         s->reqs.emplace(tk, r);
-        s->queue.push_back(tk);
         *ticket = tk;
     }
     s->cv_submit.notify_one();
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_server_submit(apsm_server* s, const apsm_job* job, uint64_t* ticket)
+{
+    return apsm_server_submit_deadline(s, job, -1.0, ticket);
+}
+
+extern "C" apsm_status apsm_server_set_deadline(apsm_server* s, double seconds)
+{
+    if (!s || !(seconds >= 0)) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(s->mu);
+    s->default_deadline = seconds;
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_server_cancel(apsm_server* s, uint64_t ticket)
+{
+    if (!s) return APSM_ERR_INVALID_ARGUMENT;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return APSM_ERR_INVALID_ARGUMENT;
+        ServerReq& r = it->second;
+        if (r.state == 1) return APSM_ERR_UNSUPPORTED; // on the GPU already: runs to completion
+        if (r.state == 2) return APSM_ERR_INVALID_ARGUMENT;
+        if (r.lost) {
+            s->lost.erase(ticket);
+        } else {
+            auto q = std::find(s->queue.begin(), s->queue.end(), ticket);
+            if (q != s->queue.end()) s->queue.erase(q);
+        }
+        s->finish_one(ticket, APSM_ERR_CANCELLED, now_s());
+        ++s->cancelled;
+    }
+    s->cv_submit.notify_one();
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_server_counts(apsm_server* s, uint64_t* dropped, uint64_t* cancelled, uint64_t* rejected)
+{
+    if (!s) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(s->mu);
+    if (dropped) *dropped = s->dropped;
+    if (cancelled) *cancelled = s->cancelled;
+    if (rejected) *rejected = s->rejected;
+    return APSM_OK;
+}
+
+extern "C" apsm_status apsm_server_inject_fault(apsm_server* s, int fault, uint32_t count)
+{
+    if (!s || fault != APSM_FAULT_DROP_REQUEST) return APSM_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> g(s->mu);
+    s->fault_drop = count;
     return APSM_OK;
 }
 

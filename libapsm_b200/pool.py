@@ -98,6 +98,11 @@ class DetectorPool:
     def reset(self, detector: int) -> None:
         self._check(self._lib.apsm_pool_reset(self._h, int(detector)))
 
+    def inject_fault(self, fault: int, count: int = 1) -> None:
+        """Host-side fault injection (tests): APSM_FAULT_LANE_ALLOC fails the next
+        `count` lane-scratch growths as an allocation would."""
+        self._check(self._lib.apsm_pool_inject_fault(self._h, int(fault), int(count)))
+
     def get_state(self, detector: int) -> tuple[int, np.ndarray, np.ndarray]:
         """(rows in use, a[rows], w[2N])."""
         n = self.antennas[detector]

@@ -67,16 +67,54 @@ class DetectorServer:
                    tx.ctypes.data if tx is not None else None, est.ctypes.data if est is not None else None)
         return cj, rx, tx, est
 
-    def submit_prepared(self, prepared: tuple) -> int:
+    def submit_prepared(self, prepared: tuple, deadline: float | None = None) -> int:
+        """Queue a request; `deadline` seconds after submission (None: the server's
+        default, 0: none).  Malformed or oversized requests raise here (no ticket)."""
         t = ctypes.c_uint64()
-        st = self._lib.apsm_server_submit(self._h, ctypes.byref(prepared[0]), ctypes.byref(t))
+        dl = -1.0 if deadline is None else float(deadline)
+        st = self._lib.apsm_server_submit_deadline(self._h, ctypes.byref(prepared[0]), dl, ctypes.byref(t))
         if st != _native.APSM_OK:
-            raise ApsmError(st, "apsm_server_submit failed")
+            raise ApsmError(st, "request rejected at submission")
         self._keep[t.value] = prepared
         return t.value
 
-    def submit(self, job: PoolJob) -> int:
-        return self.submit_prepared(self.make_job(job))
+    def submit(self, job: PoolJob, deadline: float | None = None) -> int:
+        return self.submit_prepared(self.make_job(job), deadline)
+
+    def set_deadline(self, seconds: float) -> None:
+        """Default deadline of later submissions (0: none)."""
+        st = self._lib.apsm_server_set_deadline(self._h, float(seconds))
+        if st != _native.APSM_OK:
+            raise ApsmError(st, "apsm_server_set_deadline")
+
+    def cancel(self, ticket: int) -> int:
+        """Cancel a request not admitted yet; the native status (APSM_OK when cancelled)."""
+        return int(self._lib.apsm_server_cancel(self._h, ctypes.c_uint64(ticket)))
+
+    def status(self, ticket: int) -> int | None:
+        """The finished request's status, None while it is pending."""
+        s = ctypes.c_int()
+        r = self._lib.apsm_server_poll(self._h, ctypes.c_uint64(ticket), ctypes.byref(s))
+        if r < 0:
+            raise ValueError(f"unknown ticket {ticket}")
+        return s.value if r == 1 else None
+
+    def wait_status(self, ticket: int, timeout: float = 30.0) -> int:
+        """Block until the request finished (or timeout): its status, APSM_ERR_TIMEOUT."""
+        return int(self._lib.apsm_server_wait(self._h, ctypes.c_uint64(ticket), float(timeout)))
+
+    def counts(self) -> tuple[int, int, int]:
+        """Requests dropped at their deadline, cancelled, rejected at submission."""
+        d, c, r = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._lib.apsm_server_counts(self._h, ctypes.byref(d), ctypes.byref(c), ctypes.byref(r))
+        return d.value, c.value, r.value
+
+    def inject_fault(self, fault: int, count: int = 1) -> None:
+        """Host-side fault injection (tests): APSM_FAULT_DROP_REQUEST loses the next
+        `count` submitted requests on their way into the queue."""
+        st = self._lib.apsm_server_inject_fault(self._h, int(fault), int(count))
+        if st != _native.APSM_OK:
+            raise ApsmError(st, "apsm_server_inject_fault")
 
     def wait(self, ticket: int, timeout: float = 30.0) -> np.ndarray | None:
         st = self._lib.apsm_server_wait(self._h, ctypes.c_uint64(ticket), float(timeout))

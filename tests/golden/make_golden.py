@@ -39,7 +39,19 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
-REF_DATA = Path("/root/reference/cpp/data/offline")
+def _reference_dir() -> Path:
+    """The fraunhoferhhi/libapsm checkout whose captured data and library this
+    script runs (environment variable APSM_REFERENCE_DIR)."""
+    import os
+
+    d = os.environ.get("APSM_REFERENCE_DIR")
+    if not d:
+        raise SystemExit("make_golden.py: set APSM_REFERENCE_DIR to the libapsm checkout (its cpp/data/offline "
+                         "holds the captured frames)")
+    p = Path(d) / "cpp" / "data" / "offline"
+    if not p.is_dir():
+        raise SystemExit(f"make_golden.py: {p} not found: APSM_REFERENCE_DIR must be the libapsm checkout")
+    return p
 
 CASES = {
     "qpsk_small": (dict(seed=101, K=2, N=4, P=64, S=64, modulation="QPSK"),
@@ -73,8 +85,8 @@ def capture() -> None:
     (loadData with Modulation::getScale, binary_load.cpp:55-81)."""
     from libapsm_b200 import binfile
 
-    rx = binfile.read(REF_DATA / "rx" / "time" / "rxData_QPSK_alltx_converted.bin")
-    tx = binfile.read(REF_DATA / "tx" / "NOMA_signals_qpsk_complex.bin")
+    rx = binfile.read(_reference_dir() / "rx" / "time" / "rxData_QPSK_alltx_converted.bin")
+    tx = binfile.read(_reference_dir() / "tx" / "NOMA_signals_qpsk_complex.bin")
     ant = [i * 16 // 8 for i in range(8)]  # antennaPatternEquidistant(8), util.cpp:264-272
     scale = np.float32(1.0 / np.sqrt(2.0))
     rxt = binfile.complex_matrix(rx["rxSigTraining"])[ant, :160]
