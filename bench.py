@@ -197,6 +197,9 @@ def sfu_roofline(dets, dict_size: int, detect_ms: float, sms: int, sm_mhz: float
             "clock_mhz": mhz}
 
 
+batched_est_host: list = []  # the last batched run's estimates (rank 0), for the CPU sample's SER
+
+
 def run_batched(args, rank: int, world: int) -> dict | None:
     import torch
 
@@ -318,6 +321,7 @@ def run_batched(args, rank: int, world: int) -> dict | None:
     col_entries = sweep_column_entries(dets, 2000)
     pilots = sum(d.P for d in dets)
     plain_same = run_plain_same(dets, dev_in, est_batched) if not args.no_extras else None
+    batched_est_host[:] = est_batched
     return {
         "metric": METRIC, "value": symbols / (ms_step * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -724,17 +728,18 @@ def run_serving(rate_hz: float = 20000.0, duration_s: float = 0.3, n_det: int = 
 def cpu_sample(per_class: int = 6) -> list:
     """A bounded sample of the batched workload stratified by antenna count:
     the first `per_class` detectors of each antenna class {4, 8, 16, 32} in
-    the 512-detector draw (their pilot and data lengths as drawn)."""
+    the 512-detector draw (their pilot and data lengths as drawn), as
+    (index in the draw, detector) pairs."""
     from libapsm_b200 import synth
 
     dets = synth.config2_detectors(N_DET, seed=2)
     out = []
     for N in (4, 8, 16, 32):
-        out += [d for d in dets if d.N == N][:per_class]
+        out += [(i, d) for i, d in enumerate(dets) if d.N == N][:per_class]
     return out
 
 
-def cpu_baseline(per_class: int = 6) -> dict:
+def cpu_baseline(per_class: int = 6, batched_est: list | None = None) -> dict:
     """The FP32 restatement of the reference algorithm on the host cores
     (OpenMP over all host threads), on a bounded, antenna-stratified sample of
     the batched workload.  Also the share of the full batch's work the sample
@@ -743,21 +748,36 @@ def cpu_baseline(per_class: int = 6) -> dict:
     from oracle import oracle as O
 
     threads = O.set_threads(os.cpu_count() or 1)
-    dets = cpu_sample(per_class)
+    sample = cpu_sample(per_class)
+    dets = [d for _, d in sample]
     cfg = dict(synth.CONFIG2_ALGORITHM)
     t0 = time.perf_counter()
     syms = 0
+    ests = []
     for d in dets:
         o = O.OracleDetector(cfg, d.N, O.F32)
         o.train(d.rx_train, d.tx_train)
-        o.detect(d.rx_data)
+        ests.append(o.detect(d.rx_data))
         syms += d.S
     dt = time.perf_counter() - t0
     P = sum(d.P for d in dets)
-    return {"value": syms / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "training_samples_per_s": P / dt,
-            "sample": f"{len(dets)} of the 512 detectors, the first {per_class} of each antenna class "
-                      f"(4/8/16/32), train + detect each: {P} pilots, {syms} symbols, {dt:.2f} s"}
+    out = {"value": syms / dt, "unit": UNIT, "cores": threads, "kind": "port",
+           "training_samples_per_s": P / dt,
+           "sample": f"{len(dets)} of the 512 detectors, the first {per_class} of each antenna class "
+                     f"(4/8/16/32), train + detect each: {P} pilots, {syms} symbols, {dt:.2f} s"}
+    if batched_est is not None:
+        # the same frames' SER in the oracle and in the batched run (hard decisions of the Gray map)
+        err_o = err_b = diff = 0
+        for (i, d), eo in zip(sample, ests):
+            true = d.modulation.hard_decode_int(d.tx_data)
+            do, db = d.modulation.hard_decode_int(eo), d.modulation.hard_decode_int(batched_est[i])
+            err_o += int(np.sum(do != true))
+            err_b += int(np.sum(db != true))
+            diff += int(np.sum(do != db))
+        out["ser_oracle"] = err_o / syms
+        out["ser_batched_same_frames"] = err_b / syms
+        out["decisions_differing_from_oracle"] = diff
+    return out
 
 
 def reference_cuda(n_sample: int = 16) -> dict | None:
@@ -881,7 +901,7 @@ def main():
             line["batched_over_plain"] = line["value"] / ps["value"]
         line["precision"] = run_precision_study()
     if line is not None and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline()
+        line["cpu_baseline"] = cpu_baseline(batched_est=batched_est_host if len(batched_est_host) == N_DET else None)
     if world > 1:
         import torch
 

@@ -120,6 +120,21 @@ struct BatchGramJob {
     float ew2;          // ew * log2(e)
 };
 
+// One training job of a tensor-core kernel-column launch (kernels_batch_kcol_tc.cu): its
+// universe pairs as UMMA operands (TF32 hi | lo, canonical K-major): row tiles of 128 pairs
+// b in [0, nP) and column chunks of 64 pairs n in [n_first, nP) (two rows per pair).
+struct BatchKcolTcJob {
+    const float2* Y;    // nP x Np universe pairs
+    const float* nrm;   // nP pair norms
+    float4* Kc;         // the job's kernel columns (as BatchTrainJob::Kc)
+    uint8_t* a_ops;     // a_tiles row tiles
+    uint8_t* b_ops;     // b_chunks column chunks
+    float* a_nrm;       // a_tiles x 128 row norms (0 past nP)
+    int nP, N, Np, Kp, capP, n_first, a_tiles, b_chunks;
+    long long kc_base;  // column_prefix(n_first)
+    float ewl2;         // ew log2(e)
+};
+
 // Packing of complex samples: antenna-major rx (N x L complex) -> L x Np pairs + norms.
 struct BatchPackJob {
     const float2* rx;   // N x L
@@ -151,6 +166,17 @@ cudaError_t launch_batch_kcol(const BatchTrainJob* d_jobs, const int* order, int
                               int row_split, BatchCommon cm, cudaStream_t s);
 int batch_kcol_group(); // columns per block
 int batch_kcol_rows();  // column entries per block pass
+// The same columns with the cross terms y_b^H y_n on the tensor cores (TF32 split, FP32
+// accuracy), for jobs without old-pair sums (pro == null) and N <= 32: operand packing, then
+// one CTA per chunk of 64 columns (chunk_prefix[j] = first CTA of job j), Kpmax the largest Kp
+// of the launch.
+int batch_kcol_tc_kp(int N);
+int batch_kcol_tc_row_tile();  // pairs per row tile
+int batch_kcol_tc_col_pairs(); // columns per chunk (CTA)
+size_t batch_kcol_tc_a_bytes(int Kp);
+size_t batch_kcol_tc_b_bytes(int Kp);
+cudaError_t launch_batch_kcol_tc(const BatchKcolTcJob* d_jobs, int n_jobs, int max_units, const int* d_chunk_prefix,
+                                 int total_chunks, int Kpmax, BatchCommon cm, int* d_err, cudaStream_t s);
 size_t batch_sweep_smem(const BatchCommon& cm);
 int batch_sweep_threads();
 cudaError_t batch_sweep_occupancy(const BatchCommon& cm, int* ctas_per_sm);

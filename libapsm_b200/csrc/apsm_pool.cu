@@ -286,6 +286,12 @@ struct apsm_pool {
     std::FILE* trace = nullptr; // batch timeline lines (env APSM_POOL_TRACE = file path)
     bool timing = true;         // per-stage GPU events of each batch (apsm_pool_last_ms)
     uint32_t fault_lane_alloc = 0; // lane-scratch growths still to fail (apsm_pool_inject_fault)
+    // Form of the kernel columns of a training job, decided by the job alone (so a job's result
+    // never depends on its batch): tensor cores for fresh sweeps (no old-pair sums) with
+    // kcol_tc_min_n <= N <= 32 antennas, the CUDA-core kernel otherwise.  APSM_POOL_KCOL=cuda
+    // or =tensor (read at creation) forces one form where it applies.
+    int kcol_tc_min_n = 8;
+    bool kcol_tc_off = false;
     cudaMemPool_t mempool = nullptr; // lane scratch (stream-ordered; keeps its memory mapped)
     Stager stager;                   // host-input staging (helper threads for large batches)
     std::map<uint32_t, std::vector<int>> perms;
@@ -439,6 +445,10 @@ struct TrainPlan {
     // prologue sums of the first window's pairs over the old pairs (launch_batch_kcol)
     int pro_n = 0, pro_w = 0, pro_lo = 0, pro_stride = 0; // pro_n: columns with sums
     size_t off_pro = 0;
+    // kernel columns on the tensor cores (launch_batch_kcol_tc): operand scratch
+    bool kc_tc = false;
+    int kc_Kp = 0, kc_a_tiles = 0, kc_b_chunks = 0;
+    size_t off_kca = 0, off_kcb = 0, off_kcn = 0;
 };
 
 struct DetectPlan {
@@ -545,6 +555,13 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             const uint32_t fhP = uint32_t(t.final_hi) / 2;
             t.usedP_new = std::min(fhP, t.det->capP);
             t.lo_new = fhP - t.usedP_new;
+            t.kc_tc = !kcol_tc_off && t.pro_n == 0 && t.nP > t.n_first && int(t.det->N) >= kcol_tc_min_n &&
+                      t.det->N <= 32;
+            if (t.kc_tc) {
+                t.kc_Kp = batch_kcol_tc_kp(int(t.det->N));
+                t.kc_a_tiles = int((t.nP + batch_kcol_tc_row_tile() - 1) / batch_kcol_tc_row_tile());
+                t.kc_b_chunks = int((t.nP - t.n_first + batch_kcol_tc_col_pairs() - 1) / batch_kcol_tc_col_pairs());
+            }
             tp.push_back(std::move(t));
         }
     // step lists of a large batch from the device arena (new ones uploaded now)
@@ -678,6 +695,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     const size_t off_ci = o; o = align_up(o + sizeof(BatchCopyJob) * nCopyIn, 256);
     const size_t off_co = o; o = align_up(o + sizeof(BatchCopyJob) * nT, 256);
     const size_t off_ko = o; o = align_up(o + sizeof(int) * nT, 256); // training jobs by antenna class
+    const size_t off_kt = o; o = align_up(o + sizeof(BatchKcolTcJob) * nT, 256); // tensor-core column jobs
+    const size_t off_ktp = o; o = align_up(o + sizeof(int) * (nT + 5), 256);     // their chunk prefixes
     const size_t off_gj = o; o = align_up(o + sizeof(BatchGramJob) * nG, 256);
     const size_t off_gp = o; o = align_up(o + sizeof(int) * (nG + nGcls), 256);
     if (!arena)
@@ -730,6 +749,11 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         t.off_y = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
         t.off_a = o; o = align_up(o + sizeof(float) * 2 * t.nP, 256);
         t.off_kc = o; o = align_up(o + sizeof(float4) * size_t(std::max<long long>(t.n_kc, 1)), 256);
+        if (t.kc_tc) {
+            t.off_kca = o; o = align_up(o + batch_kcol_tc_a_bytes(t.kc_Kp) * t.kc_a_tiles, 256);
+            t.off_kcb = o; o = align_up(o + batch_kcol_tc_b_bytes(t.kc_Kp) * t.kc_b_chunks, 256);
+            t.off_kcn = o; o = align_up(o + sizeof(float) * batch_kcol_tc_row_tile() * t.kc_a_tiles, 256);
+        }
         if (t.pro_n > 0) {
             t.off_pro = o;
             o = align_up(o + sizeof(float2) * size_t(t.pro_n) * t.pro_stride, 256);
@@ -911,24 +935,69 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     }
     for (auto& kv : perm_off) std::memcpy(hst + kv.second, perms[kv.first].data(), sizeof(int) * kv.first);
     const size_t pack_train = ipack;
-    // kernel-column launches, one per antenna class (rows of the class's size in registers)
+    // kernel-column launches, one per antenna class and form: the CUDA-core kernel (rows of the
+    // class's size in registers) and the tensor-core kernel (operands of the class's Kp)
     struct KcolClass {
         int first = 0, count = 0, max_cols = 0, max_n = 1;
+        int tc_first = 0, tc_count = 0, tc_units = 0, tc_chunks = 0, tc_kp = 0, tc_prefix = 0;
     };
     KcolClass kcls[5];
     {
         auto cls_of = [](int n) { return n <= 4 ? 0 : n <= 8 ? 1 : n <= 16 ? 2 : n <= 32 ? 3 : 4; };
-        for (size_t k = 0; k < nT; ++k) ++kcls[cls_of(int(tp[k].det->N))].count;
-        for (int c = 1; c < 5; ++c) kcls[c].first = kcls[c - 1].first + kcls[c - 1].count;
-        int fill[5];
-        for (int c = 0; c < 5; ++c) fill[c] = kcls[c].first;
-        auto* h_ko = reinterpret_cast<int*>(hst + off_ko);
         for (size_t k = 0; k < nT; ++k) {
             KcolClass& kc = kcls[cls_of(int(tp[k].det->N))];
-            h_ko[fill[cls_of(int(tp[k].det->N))]++] = int(k);
-            kc.max_cols = std::max(kc.max_cols, int(tp[k].nP - tp[k].n_first));
-            kc.max_n = std::max(kc.max_n, int(tp[k].det->N));
+            ++(tp[k].kc_tc ? kc.tc_count : kc.count);
         }
+        for (int c = 1; c < 5; ++c) {
+            kcls[c].first = kcls[c - 1].first + kcls[c - 1].count;
+            kcls[c].tc_first = kcls[c - 1].tc_first + kcls[c - 1].tc_count;
+            kcls[c].tc_prefix = kcls[c - 1].tc_prefix + kcls[c - 1].tc_count + 1;
+        }
+        int fill[5], tc_fill[5];
+        for (int c = 0; c < 5; ++c) {
+            fill[c] = kcls[c].first;
+            tc_fill[c] = kcls[c].tc_first;
+        }
+        auto* h_ko = reinterpret_cast<int*>(hst + off_ko);
+        auto* h_kt = reinterpret_cast<BatchKcolTcJob*>(hst + off_kt);
+        auto* h_ktp = reinterpret_cast<int*>(hst + off_ktp);
+        for (size_t k = 0; k < nT; ++k) {
+            const int c = cls_of(int(tp[k].det->N));
+            KcolClass& kc = kcls[c];
+            const TrainPlan& t = tp[k];
+            if (!t.kc_tc) {
+                h_ko[fill[c]++] = int(k);
+                kc.max_cols = std::max(kc.max_cols, int(t.nP - t.n_first));
+                kc.max_n = std::max(kc.max_n, int(t.det->N));
+                continue;
+            }
+            const int i = tc_fill[c]++;
+            BatchKcolTcJob kj{};
+            kj.Y = reinterpret_cast<const float2*>(D(t.off_Y));
+            kj.nrm = reinterpret_cast<const float*>(D(t.off_nrm));
+            kj.Kc = reinterpret_cast<float4*>(D(t.off_kc));
+            kj.a_ops = reinterpret_cast<uint8_t*>(D(t.off_kca));
+            kj.b_ops = reinterpret_cast<uint8_t*>(D(t.off_kcb));
+            kj.a_nrm = reinterpret_cast<float*>(D(t.off_kcn));
+            kj.nP = int(t.nP);
+            kj.N = int(t.det->N);
+            kj.Np = int(t.det->Np);
+            kj.Kp = t.kc_Kp;
+            kj.capP = int(t.det->capP);
+            kj.n_first = int(t.n_first);
+            kj.a_tiles = t.kc_a_tiles;
+            kj.b_chunks = t.kc_b_chunks;
+            kj.kc_base = t.kc_base;
+            kj.ewl2 = t.det->ew * 1.4426950408889634f;
+            h_kt[i] = kj;
+            // chunk prefix of the class: one entry per job plus the total
+            h_ktp[kc.tc_prefix + (i - kc.tc_first)] = kc.tc_chunks;
+            kc.tc_chunks += t.kc_b_chunks;
+            kc.tc_units = std::max(kc.tc_units, t.kc_a_tiles + t.kc_b_chunks);
+            kc.tc_kp = std::max(kc.tc_kp, t.kc_Kp);
+        }
+        for (int c = 0; c < 5; ++c)
+            if (kcls[c].tc_count > 0) h_ktp[kcls[c].tc_prefix + kcls[c].tc_count] = kcls[c].tc_chunks;
     }
     for (size_t k = 0; k < nD; ++k) {
         DetectPlan& q = dp[k];
@@ -1034,7 +1103,14 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     if (nT > 0) {
         const auto* d_tj = reinterpret_cast<const BatchTrainJob*>(D(off_tj));
         const int* d_ko = reinterpret_cast<const int*>(D(off_ko));
+        const auto* d_kt = reinterpret_cast<const BatchKcolTcJob*>(D(off_kt));
+        const int* d_ktp = reinterpret_cast<const int*>(D(off_ktp));
         for (const KcolClass& kc : kcls) {
+            if (kc.tc_count > 0) {
+                POOL_CK(launch_batch_kcol_tc(d_kt + kc.tc_first, kc.tc_count, kc.tc_units, d_ktp + kc.tc_prefix,
+                                             kc.tc_chunks, kc.tc_kp, cm, d_err, s));
+                L.launches += 2;
+            }
             if (kc.count == 0 || kc.max_cols <= 0) continue;
             // small launches (single train requests): spread each column group's rows over blocks
             int row_split = 1;
@@ -1141,7 +1217,9 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     }
     // the error flag of kernels with bounded waits (tensor-core detection) travels back with the
     // batch: finish() reads it without a synchronous copy
-    L.err_copied = nG > 0; // only the tensor-core kernels wait on barriers (bounded, flagging expiry)
+    bool any_kc_tc = false;
+    for (const auto& t : tp) any_kc_tc = any_kc_tc || t.kc_tc;
+    L.err_copied = nG > 0 || any_kc_tc; // only the tensor-core kernels wait on barriers (bounded, flagging expiry)
     if (L.err_copied) POOL_CK(cudaMemcpyAsync(L.err_host, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (trace) {
         POOL_CK(cudaEventRecord(L.tr[6], s));
@@ -1434,6 +1512,10 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
         *l.err_host = 0;
         cudaEventRecord(l.done, l.stream);
         cudaEventRecord(l.desc_copied, l.stream);
+    }
+    if (const char* f = std::getenv("APSM_POOL_KCOL")) {
+        if (std::strcmp(f, "cuda") == 0) p->kcol_tc_off = true;
+        if (std::strcmp(f, "tensor") == 0) p->kcol_tc_min_n = 1;
     }
     if (const char* path = std::getenv("APSM_POOL_TRACE")) {
         p->trace = std::fopen(path, "w");
