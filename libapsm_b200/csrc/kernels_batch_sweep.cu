@@ -65,7 +65,15 @@ struct Entry {
     int n;    // pair, -1 when no pair enters at that step
     int lo, F, top;
     int slow; // served by direct loads when consumed
+    int fl;   // first frozen entry staged by this thread block's loads (entries [fl, F))
 };
+
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 
 __device__ __forceinline__ float hyperslab(float e, float eB)
 {
@@ -215,9 +223,10 @@ __global__ void __launch_bounds__(kThreads, 2)
             KP[qn * XSPp + sb] = kt.z;
             KM[qn * XSPp + sb] = kt.y;
         };
-        // diagonal block of pair n with squared norm nv: r = nv, m = 0
+        // diagonal block of pair n with squared norm nv: r = nv, m = 0 (the Gaussian values as the
+        // kernel-column launches form them: 2^(ew log2(e) x) on the SFU)
         auto fill_diag = [&](int qn, float nv) {
-            const float b = wG * expf(ew * (2.f * nv));
+            const float b = wG * ex2_approx(ew * 1.4426950408889634f * (2.f * nv));
             KA[qn * XSPp + qn] = fmaf(wL, nv, wG);
             KP[qn * XSPp + qn] = b;
             KM[qn * XSPp + qn] = b;
@@ -302,7 +311,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     yw[2 * q + 1] = js.y[2 * j + 1];
                     aw[2 * q] = ag[2 * j];
                     aw[2 * q + 1] = ag[2 * j + 1];
-                    rd[q] = 1.f / fmaf(wL, js.nrm[j], wG);
+                    rd[q] = __frcp_rn(fmaf(wL, js.nrm[j], wG));
                     nws[q] = js.nrm[j];
                 }
                 for (int b = max(e_lo, j - LB + 1) + lane; b <= j; b += 32) fill_band(b % XSP, q, col[b]);
@@ -310,10 +319,12 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
 
         // ---- the entering-pair pipeline (see the header) ----
-        Entry e_cur{-1, 0, 0, 0, 0}, e_nxt{-1, 0, 0, 0, 0};
+        Entry e_cur{-1, 0, 0, 0, 0, 0}, e_nxt{-1, 0, 0, 0, 0, 0};
         float4 colbuf[kPf];
         float2 abuf[kPf];
         const int et = tid - kRowThreads; // index among the entering warps' threads (< 0: row warps)
+        // the pair features d = et and et + kEntThreads of the entering warps' threads (y_n[d mod N])
+        const int fk0 = et >= 0 ? et % N : 0, fk1 = et >= 0 ? (et + kEntThreads) % N : 0;
         float4 win_cur0 = make_float4(0.f, 0.f, 0.f, 0.f), win_cur1 = win_cur0, win_nxt0 = win_cur0, win_nxt1 = win_cur0;
         float2 y_cur0 = make_float2(0.f, 0.f), y_cur1 = y_cur0, y_nxt0 = y_cur0, y_nxt1 = y_cur0;
         float t_cur0 = 0.f, t_cur1 = 0.f, n_cur = 0.f, t_nxt0 = 0.f, t_nxt1 = 0.f, n_nxt = 0.f;
@@ -359,19 +370,21 @@ __global__ void __launch_bounds__(kThreads, 2)
                     wpr[2 * (tt & 3) + 1] = p1;
                 }
             }
+            // loads of the later steps: every address clamped into the column / the pair (the entries
+            // past its end are masked where they are used), so no instruction here waits for a load
+            e_nxt.fl = fl;
+            const int fmax = max(fl, e_nxt.F - 1), tmax = max(e_nxt.lo, e_nxt.top - 1);
 #pragma unroll
             for (int k = 0; k < kPf; ++k) {
-                const int b = fl + tid + k * kThreads;
-                const bool ok = b < e_nxt.F;
-                colbuf[k] = ok ? __ldg(col + b) : make_float4(0.f, 0.f, 0.f, 0.f);
-                abuf[k] = ok ? *reinterpret_cast<const float2*>(ag + 2 * b) : make_float2(0.f, 0.f);
+                const int b = min(fl + tid + k * kThreads, fmax);
+                colbuf[k] = __ldg(col + b);
+                abuf[k] = *reinterpret_cast<const float2*>(ag + 2 * b);
             }
             if (et >= 0) {
-                const int b0 = e_nxt.F + et, b1 = b0 + kEntThreads;
-                win_nxt0 = b0 < e_nxt.top ? __ldg(col + b0) : make_float4(0.f, 0.f, 0.f, 0.f);
-                win_nxt1 = b1 < e_nxt.top ? __ldg(col + b1) : make_float4(0.f, 0.f, 0.f, 0.f);
-                if (et < D) y_nxt0 = Y[size_t(n) * Np + et % N];
-                if (et + kEntThreads < D) y_nxt1 = Y[size_t(n) * Np + (et + kEntThreads) % N];
+                win_nxt0 = __ldg(col + min(e_nxt.F + et, tmax));
+                win_nxt1 = __ldg(col + min(e_nxt.F + et + kEntThreads, tmax));
+                y_nxt0 = Y[size_t(n) * Np + fk0];
+                y_nxt1 = Y[size_t(n) * Np + fk1];
             }
             if (et == 0) {
                 t_nxt0 = js.y[2 * n];
@@ -384,7 +397,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             gf0 = gf1 = 0.f;
             if (e_nxt.n >= 0 && !e_nxt.slow) {
 #pragma unroll
-                for (int k = 0; k < kPf; ++k) acc_pair(abuf[k], colbuf[k], gf0, gf1);
+                for (int k = 0; k < kPf; ++k)
+                    if (e_nxt.fl + tid + k * kThreads < e_nxt.F) acc_pair(abuf[k], colbuf[k], gf0, gf1);
                 warp_sum2(gf0, gf1);
                 if (lane == 0) {
                     wpf[(buf * kWarps + warp) * 2] = gf0;
@@ -463,7 +477,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     yw[2 * qn] = t_cur0;
                     yw[2 * qn + 1] = t_cur1;
                     aw[2 * qn] = aw[2 * qn + 1] = 0.f;
-                    rd[qn] = 1.f / fmaf(wL, n_cur, wG);
+                    rd[qn] = __frcp_rn(fmaf(wL, n_cur, wG));
                     nws[qn] = n_cur;
                     fill_diag(qn, n_cur);
                 }
@@ -492,7 +506,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                         yw[2 * qn] = js.y[2 * n];
                         yw[2 * qn + 1] = js.y[2 * n + 1];
                         aw[2 * qn] = aw[2 * qn + 1] = 0.f;
-                        rd[qn] = 1.f / fmaf(wL, js.nrm[n], wG);
+                        rd[qn] = __frcp_rn(fmaf(wL, js.nrm[n], wG));
                         nws[qn] = js.nrm[n];
                         fill_diag(qn, js.nrm[n]);
                     }
