@@ -68,6 +68,15 @@ struct Entry {
     int fl;   // first frozen entry staged by this thread block's loads (entries [fl, F))
 };
 
+// Bulk prefetch of a global range into L2 (16-byte aligned, size a multiple of 16): a hint, no
+// shared memory and no register is involved.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+constexpr int kPrefetchPairs = 4; // kernel columns brought into L2 this many pairs before their loads
+
 __device__ __forceinline__ float ex2_approx(float x)
 {
     float y;
@@ -320,8 +329,13 @@ __global__ void __launch_bounds__(kThreads, 2)
 
         // ---- the entering-pair pipeline (see the header) ----
         Entry e_cur{-1, 0, 0, 0, 0, 0}, e_nxt{-1, 0, 0, 0, 0, 0};
+        // frozen part of an entering pair's sum: thread tid takes the pairs b = tid + 256 k (mod 2048)
+        // of the frozen range; their final coefficients stay in registers (abuf[k] holds a_b of the
+        // pair currently in slot k; loaded once, when b first becomes frozen: pairs below cache_F are
+        // cached), and only the column entries are loaded for every entering pair
         float4 colbuf[kPf];
         float2 abuf[kPf];
+        int cache_F = 0;
         const int et = tid - kRowThreads; // index among the entering warps' threads (< 0: row warps)
         // the pair features d = et and et + kEntThreads of the entering warps' threads (y_n[d mod N])
         const int fk0 = et >= 0 ? et % N : 0, fk1 = et >= 0 ? (et + kEntThreads) % N : 0;
@@ -350,6 +364,15 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
             const int n = e_lo;
             const float4* col = col_ptr(n);
+            if (tid == 32) {
+                // a later pair's column into L2 (it was written long before: in DRAM by now), so that
+                // its loads, kPrefetchPairs steps from now, find it there
+                const int n2 = n + kPrefetchPairs;
+                if (n2 < nP) {
+                    const int b0 = col_begin(n2, capP), b1 = col_end(n2, qP, nP);
+                    if (b1 > b0) prefetch_l2(col_ptr(n2) + b0, uint32_t(16 * (b1 - b0)));
+                }
+            }
             if (warp == 5) {
                 // the pair's old-pair sums (one per kernel-column pass): lanes take passes, shuffle sum
                 float p0 = 0.f, p1 = 0.f;
@@ -376,17 +399,18 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int fmax = max(fl, e_nxt.F - 1), tmax = max(e_nxt.lo, e_nxt.top - 1);
 #pragma unroll
             for (int k = 0; k < kPf; ++k) {
-                const int b = min(fl + tid + k * kThreads, fmax);
-                colbuf[k] = __ldg(col + b);
-                abuf[k] = *reinterpret_cast<const float2*>(ag + 2 * b);
+                const int b = fl + ((tid + k * kThreads - fl) & (kThreads * kPf - 1)); // slot k's pair
+                colbuf[k] = __ldg(col + min(b, fmax));
+                if (b < e_nxt.F && b >= cache_F) abuf[k] = *reinterpret_cast<const float2*>(ag + 2 * b);
             }
+            cache_F = max(cache_F, e_nxt.F);
             if (et >= 0) {
                 win_nxt0 = __ldg(col + min(e_nxt.F + et, tmax));
                 win_nxt1 = __ldg(col + min(e_nxt.F + et + kEntThreads, tmax));
                 y_nxt0 = Y[size_t(n) * Np + fk0];
                 y_nxt1 = Y[size_t(n) * Np + fk1];
             }
-            if (et == 0) {
+            if (tid == 0) {
                 t_nxt0 = js.y[2 * n];
                 t_nxt1 = js.y[2 * n + 1];
                 n_nxt = js.nrm[n];
@@ -397,8 +421,10 @@ __global__ void __launch_bounds__(kThreads, 2)
             gf0 = gf1 = 0.f;
             if (e_nxt.n >= 0 && !e_nxt.slow) {
 #pragma unroll
-                for (int k = 0; k < kPf; ++k)
-                    if (e_nxt.fl + tid + k * kThreads < e_nxt.F) acc_pair(abuf[k], colbuf[k], gf0, gf1);
+                for (int k = 0; k < kPf; ++k) {
+                    const int b = e_nxt.fl + ((tid + k * kThreads - e_nxt.fl) & (kThreads * kPf - 1));
+                    if (b < e_nxt.F) acc_pair(abuf[k], colbuf[k], gf0, gf1);
+                }
                 warp_sum2(gf0, gf1);
                 if (lane == 0) {
                     wpf[(buf * kWarps + warp) * 2] = gf0;
@@ -432,6 +458,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
             STEP_MARK(0);
             // ================= phase 1 =================
+            const bool fast = ne == 1 && e_cur.n == e_lo && !e_cur.slow;
             // (1a) window rows: fold the last update in; corrections of the active rows
             for (int r = tid; r < 2 * XSP && tid < kRowThreads; r += kRowThreads) {
                 const int q = r >> 1;
@@ -447,8 +474,18 @@ __global__ void __launch_bounds__(kThreads, 2)
                 }
                 cs[r] = c;
             }
+            if (fast && tid == 0) {
+                // the entering pair's target, coefficient, projection scale, norm and diagonal block
+                // (thread 0 has the slack here; warps 6-7 take the window part below)
+                const int qn = e_cur.n % XSP;
+                yw[2 * qn] = t_cur0;
+                yw[2 * qn + 1] = t_cur1;
+                aw[2 * qn] = aw[2 * qn + 1] = 0.f;
+                rd[qn] = __frcp_rn(fmaf(wL, n_cur, wG));
+                nws[qn] = n_cur;
+                fill_diag(qn, n_cur);
+            }
             // (1b) pairs entering at t+1: data, window kernel, start of their predictions
-            const bool fast = ne == 1 && e_cur.n == e_lo && !e_cur.slow;
             if (fast) {
               if (et >= 0) {
                 const int n = e_cur.n, qn = n % XSP;
@@ -473,14 +510,6 @@ __global__ void __launch_bounds__(kThreads, 2)
                     wpe[2 * (warp - kRowThreads / 32) + 1] = g1;
                 }
                 if (et < Np) Yw[qn * YP + et] = et < N ? y_cur0 : make_float2(0.f, 0.f);
-                if (et == 0) {
-                    yw[2 * qn] = t_cur0;
-                    yw[2 * qn + 1] = t_cur1;
-                    aw[2 * qn] = aw[2 * qn + 1] = 0.f;
-                    rd[qn] = __frcp_rn(fmaf(wL, n_cur, wG));
-                    nws[qn] = n_cur;
-                    fill_diag(qn, n_cur);
-                }
               }
             } else if (ne > 0) {
                 // direct loads (several pairs per step, or columns longer than the pipeline holds)
