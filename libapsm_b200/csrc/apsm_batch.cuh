@@ -154,6 +154,15 @@ struct BatchCopyJob {
     int pairs, Np;
 };
 
+// A pool detector's state (pairs Y (pitch Np), row-form targets and coefficients, `rows` =
+// 2 x pairs) as the single detector's Dedup rows (pitch Dp, with their squared norms), and
+// back: the pool runs training jobs of normConstraint configs with the single detector's
+// exact sweep.
+cudaError_t launch_pool_to_rows(const float2* Y, int Np, const float* y, const float* a, int rows, int N, int Dp,
+                                float* X, float* nrm, float* dy, float* da, cudaStream_t s);
+cudaError_t launch_rows_to_pool(const float* X, const float* nrm, const float* dy, const float* da, int rows, int N,
+                                int Dp, int Np, float2* Y, float* pn, float* y, float* a, cudaStream_t s);
+
 // max_n: largest antenna count of the jobs (sizes the kernel's shared memory)
 cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s);
 cudaError_t launch_batch_copy(const BatchCopyJob* d_jobs, int n_jobs, int max_pairs, int max_np, cudaStream_t s);

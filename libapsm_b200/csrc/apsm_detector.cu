@@ -70,10 +70,6 @@ apsm_status apsm_detector::init(const Config& c, uint32_t num_antennas, uint32_t
     Dp = row_pitch(D);
     U = num_users;
     is_lls = cfg.otype == "LLS";
-    if (cfg.norm_constraint > 0.f && cfg.train_incremental) {
-        last_error = "normConstraint > 0 runs with the exact training sweep only (trainVersion \"exact\")";
-        return APSM_ERR_UNSUPPORTED;
-    }
     cap = 2 * cfg.dict_size;
     // ApsmNomaDetector constructor (apsm_noma_detector.cu:79-80)
     variance_eff = cfg.variance;
@@ -300,7 +296,9 @@ apsm_status apsm_detector::train(const float2* d_rx, const float2* d_tx, uint32_
         ta.prof = prof_buffer;
         ta.NS = 0;
 
-        if (cfg.train_incremental) {
+        // normConstraint rescales every coefficient after each step, which the incremental sweep's
+        // running sums do not follow: such detectors train with the exact sweep
+        if (cfg.train_incremental && !(cfg.norm_constraint > 0.f)) {
             // rows resident at once: window(t) and the rows entering at t+1 (and t+2 prefetched)
             int xs = 1;
             for (int t = 0; t < T; ++t) {

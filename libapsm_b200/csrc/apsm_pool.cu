@@ -292,6 +292,12 @@ struct apsm_pool {
     // or =tensor (read at creation) forces one form where it applies.
     int kcol_tc_min_n = 8;
     bool kcol_tc_off = false;
+    // normConstraint > 0: training jobs run the single detector's exact sweep, which applies the
+    // constraint after every step (apsm_train.cu:142-145, 168-256); one such detector per antenna
+    // count, created on first use, holds a pool detector's state while it trains
+    std::map<uint32_t, apsm_detector*> exact_by_n;
+    apsm_status exact_handle(uint32_t N, apsm_detector** out);
+    apsm_status train_exact(uint32_t lane, const apsm_job* jobs, uint32_t n, int mode, std::vector<apsm_job>* rest);
     cudaMemPool_t mempool = nullptr; // lane scratch (stream-ordered; keeps its memory mapped)
     Stager stager;                   // host-input staging (helper threads for large batches)
     std::map<uint32_t, std::vector<int>> perms;
@@ -380,6 +386,7 @@ struct apsm_pool {
 
 apsm_pool::~apsm_pool()
 {
+    for (auto& kv : exact_by_n) delete kv.second;
     for (auto& l : lanes) {
         if (l.stream) cudaStreamSynchronize(l.stream);
         if (l.scratch) cudaFree(l.scratch);
@@ -523,6 +530,16 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                                                            " is trained twice in one batch");
             trained[j.detector] = 1;
         }
+    }
+
+    // normConstraint: the training jobs first, each with the exact sweep; the batch then holds the
+    // detection jobs (which see this training, as in every batch)
+    std::vector<apsm_job> rest;
+    if (cfg.norm_constraint > 0.f && !reserve_only) {
+        const apsm_status st = train_exact(lane_id, jobs, n, mode, &rest);
+        if (st != APSM_OK) return st;
+        jobs = rest.data();
+        n = uint32_t(rest.size());
     }
 
     // ---------- plan (sizes and offsets) ----------
@@ -1238,6 +1255,83 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     return APSM_OK;
 }
 
+apsm_status apsm_pool::exact_handle(uint32_t N, apsm_detector** out)
+{
+    auto it = exact_by_n.find(N);
+    if (it == exact_by_n.end()) {
+        auto* h = new apsm_detector();
+        const apsm_status st = h->init(cfg, N, 1);
+        if (st != APSM_OK) {
+            const std::string msg = h->last_error;
+            delete h;
+            return fail(st, "normConstraint training detector: " + msg);
+        }
+        it = exact_by_n.emplace(N, h).first;
+    }
+    *out = it->second;
+    return APSM_OK;
+}
+
+// Training jobs of a normConstraint pool, in the batch's order, each on the lane's stream with the
+// exact sweep of a single detector of its antenna count: the pool detector's state is converted to
+// Dedup rows, trained, and converted back (same dictionary semantics: rows oldest first, a full
+// dictionary evicts its oldest rows, a second call continues the window).  The detection jobs are
+// returned in `rest`.
+apsm_status apsm_pool::train_exact(uint32_t lane_id, const apsm_job* jobs, uint32_t n, int mode,
+                                   std::vector<apsm_job>* rest)
+{
+    apsm_pool* p = this;
+    cudaStream_t s = lanes[lane_id].stream;
+    const bool host = mode != APSM_RUN_DEVICE;
+    rest->clear();
+    for (uint32_t i = 0; i < n; ++i) {
+        const apsm_job& j = jobs[i];
+        if (j.kind != APSM_JOB_TRAIN) {
+            rest->push_back(j);
+            continue;
+        }
+        PoolDet& d = dets[j.detector];
+        if (j.flags & APSM_JOB_FRESH) {
+            POOL_CK(cudaMemsetAsync(d.w, 0, sizeof(float) * 2 * d.N, s));
+            POOL_CK(cudaMemsetAsync(d.r, 0, sizeof(float) * 2 * d.N, s));
+            d.used = 0;
+        }
+        if (j.length == 0) continue;
+        apsm_detector* h = nullptr;
+        apsm_status st = exact_handle(d.N, &h);
+        if (st != APSM_OK) return st;
+        const int N = int(d.N), Dp = int(h->Dp), Np = int(d.Np);
+        // pool state -> rows of the detector
+        h->used = d.used;
+        POOL_CK(launch_pool_to_rows(d.Y, Np, d.y, d.a, int(d.used), N, Dp, h->dict_X.p, h->dict_nrm.p, h->dict_y.p,
+                                    h->dict_a.p, s));
+        POOL_CK(cudaMemcpyAsync(h->w.p, d.w, sizeof(float) * 2 * d.N, cudaMemcpyDeviceToDevice, s));
+        const float2* rx = reinterpret_cast<const float2*>(j.rx);
+        const float2* tx = reinterpret_cast<const float2*>(j.tx);
+        if (host) {
+            POOL_CK(h->rx_stage.ensure(size_t(d.N) * j.length));
+            POOL_CK(h->tx_stage.ensure(j.length));
+            POOL_CK(cudaMemcpyAsync(h->rx_stage.p, rx, sizeof(float2) * size_t(d.N) * j.length,
+                                    cudaMemcpyHostToDevice, s));
+            POOL_CK(cudaMemcpyAsync(h->tx_stage.p, tx, sizeof(float2) * j.length, cudaMemcpyHostToDevice, s));
+            rx = h->rx_stage.p;
+            tx = h->tx_stage.p;
+        }
+        st = h->train(rx, tx, j.length, s, nullptr);
+        if (st != APSM_OK) return fail(st, "normConstraint training: " + h->last_error);
+        POOL_CK(cudaStreamSynchronize(s));
+        st = h->check_train_error();
+        if (st != APSM_OK) return fail(st, h->last_error);
+        // rows -> pool state (the residual weights of the incremental sweep are not used by
+        // normConstraint pools)
+        POOL_CK(launch_rows_to_pool(h->dict_X.p, h->dict_nrm.p, h->dict_y.p, h->dict_a.p, int(h->used), N, Dp, Np,
+                                    d.Y, d.nrm, d.y, d.a, s));
+        POOL_CK(cudaMemcpyAsync(d.w, h->w.p, sizeof(float) * 2 * d.N, cudaMemcpyDeviceToDevice, s));
+        d.used = h->used;
+    }
+    return APSM_OK;
+}
+
 // Launch-shape autotuner: the batch is run once per candidate of each knob
 // that it exercises (one knob at a time, the others at their current values),
 // the GPU time from its first to its last kernel compared, and the fastest
@@ -1439,7 +1533,6 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
     std::string why;
     if (cfg.otype != "APSM") why = "the detector pool runs APSM detectors only";
     else if (cfg.lls_init) why = "llsInitialization is not available in the detector pool";
-    else if (cfg.norm_constraint > 0.f) why = "normConstraint > 0 is not available in this build";
     else if (!(cfg.variance > 0.f)) why = "the detector pool needs gaussianKernelVariance > 0";
     else if (cfg.step % 2 != 0 || cfg.step == 0 || cfg.step > 8) why = "the detector pool needs an even sampleStep <= 8";
     else if (cfg.dict_size < cfg.window + cfg.step / 2) why = "the detector pool needs dictionarySize >= windowSize + sampleStep / 2";

@@ -89,3 +89,72 @@ cudaError_t launch_batch_copy(const BatchCopyJob* d_jobs, int n_jobs, int max_pa
 }
 
 } // namespace apsm
+
+namespace apsm {
+
+namespace {
+
+// rows 2b = [Re y_b; Im y_b], 2b+1 = [Im y_b; -Re y_b] of pair b (Dedup embedding,
+// cpp/lib/cuda/cuda_matrix_device.cuh:180-188), feature d < Dp (0 past 2N)
+__device__ __forceinline__ float dedup_feature(const float2* __restrict__ yb, int N, int odd, int d)
+{
+    if (d < N) return odd ? yb[d].y : yb[d].x;
+    if (d < 2 * N) return odd ? -yb[d - N].x : yb[d - N].y;
+    return 0.f;
+}
+
+__global__ void pool_to_rows_kernel(const float2* __restrict__ Y, int Np, const float* __restrict__ y,
+                                    const float* __restrict__ a, int rows, int N, int Dp, float* __restrict__ X,
+                                    float* __restrict__ nrm, float* __restrict__ dy, float* __restrict__ da)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+        const float2* yb = Y + size_t(i >> 1) * Np;
+        const int odd = i & 1;
+        float acc = 0.f;
+        for (int d = 0; d < Dp; ++d) {
+            const float v = dedup_feature(yb, N, odd, d);
+            X[size_t(i) * Dp + d] = v;
+            if (d < 2 * N) acc = fmaf(v, v, acc); // the packing kernels' sequential chain
+        }
+        nrm[i] = acc;
+        dy[i] = y[i];
+        da[i] = a[i];
+    }
+}
+
+__global__ void rows_to_pool_kernel(const float* __restrict__ X, const float* __restrict__ nrm,
+                                    const float* __restrict__ dy, const float* __restrict__ da, int rows, int N,
+                                    int Dp, int Np, float2* __restrict__ Y, float* __restrict__ pn,
+                                    float* __restrict__ y, float* __restrict__ a)
+{
+    const int pairs = rows / 2;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < pairs; b += gridDim.x * blockDim.x) {
+        const float* x = X + size_t(2 * b) * Dp; // row 2b = [Re y_b; Im y_b]
+        for (int k = 0; k < Np; ++k) Y[size_t(b) * Np + k] = k < N ? make_float2(x[k], x[N + k]) : make_float2(0.f, 0.f);
+        pn[b] = nrm[2 * b]; // the pair norm is row 2b's (same chain: real parts, then imaginary parts)
+        y[2 * b] = dy[2 * b];
+        y[2 * b + 1] = dy[2 * b + 1];
+        a[2 * b] = da[2 * b];
+        a[2 * b + 1] = da[2 * b + 1];
+    }
+}
+
+} // namespace
+
+cudaError_t launch_pool_to_rows(const float2* Y, int Np, const float* y, const float* a, int rows, int N, int Dp,
+                                float* X, float* nrm, float* dy, float* da, cudaStream_t s)
+{
+    if (rows <= 0) return cudaSuccess;
+    pool_to_rows_kernel<<<(rows + 127) / 128, 128, 0, s>>>(Y, Np, y, a, rows, N, Dp, X, nrm, dy, da);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rows_to_pool(const float* X, const float* nrm, const float* dy, const float* da, int rows, int N,
+                                int Dp, int Np, float2* Y, float* pn, float* y, float* a, cudaStream_t s)
+{
+    if (rows <= 0) return cudaSuccess;
+    rows_to_pool_kernel<<<(rows / 2 + 127) / 128, 128, 0, s>>>(X, nrm, dy, da, rows, N, Dp, Np, Y, pn, y, a);
+    return cudaGetLastError();
+}
+
+} // namespace apsm

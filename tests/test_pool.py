@@ -22,7 +22,6 @@ def _create(native_lib, cfg: str):
     ('{"otype":"APSM","sampleStep":3}', 5, "even sampleStep"),
     ('{"otype":"APSM","sampleStep":10}', 5, "even sampleStep"),
     ('{"otype":"APSM","windowSize":90,"dictionarySize":80}', 5, "dictionarySize"),
-    ('{"otype":"APSM","normConstraint":0.5}', 5, "normConstraint"),
 ])
 def test_pool_config_restrictions(native_lib, cfg, status, msg):
     st, err = _create(native_lib, cfg)

@@ -377,3 +377,41 @@ def test_pool_page_locked_estimates_written_in_place(native_lib):
         outs[mode] = [np.array(r) for r in res]
     for a, b in zip(outs["pageable"], outs["page-locked"]):
         np.testing.assert_array_equal(a, b)
+
+
+NORM_CFGS = {  # bounds below every detector's unconstrained norm (the test checks that they bind)
+    "norm-w10": dict(CFG, windowSize=10, normConstraint=0.01, dictionarySize=400),
+    "norm-wrap": dict(CFG, windowSize=20, normConstraint=0.01, dictionarySize=60),
+    "norm-w80": dict(CFG, windowSize=80, normConstraint=0.003, dictionarySize=400, detectVersion="gram_tf32x3"),
+}
+
+
+@pytest.mark.parametrize("name", sorted(NORM_CFGS))
+def test_pool_norm_constraint_matches_oracle(native_lib, oracle_mod, name):
+    """normConstraint (apsm_train.cu:142-145, 168-256: after every step the
+    Gaussian part's RKHS norm is bounded by rescaling the coefficients) in the
+    pool: each detector's training runs the exact sweep, the detections the
+    pool's kernels; per detector the FP32 oracle (adapt_coeffs_f32 after each
+    step) at 1e-4, including a dictionary that wraps (60 entries, 150
+    pilots) and a second train call that appends."""
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    cfg = NORM_CFGS[name]
+    pool = DetectorPool(cfg)
+    specs = [(3, 150, 200), (8, 120, 96), (16, 100, 130), (32, 80, 64)]
+    dets, frames = [], []
+    for i, (N, P, S) in enumerate(specs):
+        dets.append(pool.add(N))
+        frames.append((N,) + _frame(700 + i, N, P, S, "QAM16"))
+    half = [(d, f[1][:, : f[1].shape[1] // 2], f[2][: f[1].shape[1] // 2]) for d, f in zip(dets, frames)]
+    rest = [(d, f[1][:, f[1].shape[1] // 2:], f[2][f[1].shape[1] // 2:]) for d, f in zip(dets, frames)]
+    pool.run([PoolJob(d, rx, tx) for d, rx, tx in half])
+    outs = pool.run([PoolJob(d, rx, tx) for d, rx, tx in rest] + [PoolJob(d, f[3]) for d, f in zip(dets, frames)])
+    for k, ((N, rx, tx, rxd), h, r) in enumerate(zip(frames, half, rest)):
+        ref = _oracle_run(oracle_mod, cfg, N, [(h[1], h[2]), (r[1], r[2])], rxd)
+        free = _oracle_run(oracle_mod, {k: v for k, v in cfg.items() if k != "normConstraint"}, N,
+                           [(h[1], h[2]), (r[1], r[2])], rxd)
+        assert _rel(free, ref) > 10 * TOL, (name, N, "the bound does not bind")
+        err = _rel(outs[len(specs) + k], ref)
+        print(f"{name} N={N}: {err:.3e}")
+        assert err < TOL, (name, N, err)
