@@ -179,6 +179,13 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float wL = cm.wL, wG = cm.wG, eB = cm.eB;
     const int Lp = (XSP + kParts - 1) / kParts; // row slots per part
     const int ncp = (XSP + 1) / 2;              // column-slot pairs
+    // n mod XSP without an integer division: q = floor(n M / 2^32) with M = ceil(2^32 / XSP) is
+    // floor(n / XSP) for every n < 2^32 / XSP (pair indices are far below); one fixup as a guard
+    const uint32_t xsp_magic = uint32_t((0x100000000ull + uint32_t(XSP) - 1) / uint32_t(XSP));
+    auto slot_of = [&](int n) {
+        int r = n - int(__umulhi(uint32_t(n), xsp_magic)) * XSP;
+        return r >= XSP ? r - XSP : r;
+    };
 
     float* KA = smem;                                        // [XSP][XSPp]
     float* KP = KA + XSP * XSPp;                             // [XSP][XSPp]
@@ -454,7 +461,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             const int e_lo = has_next ? max(pc.hiP, pn.sP) : 0;
             const int ne = has_next ? max(0, pn.hiP - e_lo) : 0; // pairs entering at t+1
             const int4 st_4 = t + 4 < n_steps ? steps[t + 4] : st_3;
-            const float inv_wk = 1.f / float(pc.wk);
+            const float inv_wk = __frcp_rn(float(pc.wk));
 
             STEP_MARK(0);
             // ================= phase 1 =================
@@ -477,7 +484,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (fast && tid == 0) {
                 // the entering pair's target, coefficient, projection scale, norm and diagonal block
                 // (thread 0 has the slack here; warps 6-7 take the window part below)
-                const int qn = e_cur.n % XSP;
+                const int qn = slot_of(e_cur.n);
                 yw[2 * qn] = t_cur0;
                 yw[2 * qn + 1] = t_cur1;
                 aw[2 * qn] = aw[2 * qn + 1] = 0.f;
@@ -488,9 +495,9 @@ __global__ void __launch_bounds__(kThreads, 2)
             // (1b) pairs entering at t+1: data, window kernel, start of their predictions
             if (fast) {
               if (et >= 0) {
-                const int n = e_cur.n, qn = n % XSP;
+                const int n = e_cur.n, qn = slot_of(n);
                 float g0 = 0.f, g1 = 0.f;
-                const int Fs = e_cur.F % XSP;
+                const int Fs = slot_of(e_cur.F);
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const int i = et + h * kEntThreads;
@@ -515,12 +522,12 @@ __global__ void __launch_bounds__(kThreads, 2)
                 // direct loads (several pairs per step, or columns longer than the pipeline holds)
                 const int top = pc.hiP, lo = pn.loP, fb = pc.sP;
                 for (int e = 0; e < min(ne, kMaxEnter); ++e) {
-                    const int n = e_lo + e, qn = n % XSP;
+                    const int n = e_lo + e, qn = slot_of(n);
                     const float4* col = col_ptr(n);
                     float g0 = 0.f, g1 = 0.f;
                     for (int b = lo + tid; b < top; b += kThreads) {
                         const float2 ab = b < fb ? *reinterpret_cast<const float2*>(ag + 2 * b)
-                                                 : *reinterpret_cast<const float2*>(aw + 2 * (b % XSP));
+                                                 : *reinterpret_cast<const float2*>(aw + 2 * slot_of(b));
                         acc_pair(ab, col[b], g0, g1);
                     }
                     if (tid < D) lin_feature(tid, r_s[tid], Y[size_t(n) * Np + tid % N], g0, g1);
@@ -529,7 +536,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                         wp[(e * kWarps + warp) * 2] = g0;
                         wp[(e * kWarps + warp) * 2 + 1] = g1;
                     }
-                    for (int b = max(0, n - LB + 1) + tid; b < n; b += kThreads) fill_band(b % XSP, qn, col[b]);
+                    for (int b = max(0, n - LB + 1) + tid; b < n; b += kThreads) fill_band(slot_of(b), qn, col[b]);
                     for (int k = tid; k < Np; k += kThreads) Yw[qn * YP + k] = Y[size_t(n) * Np + k];
                     if (tid == 0) {
                         yw[2 * qn] = js.y[2 * n];
@@ -550,7 +557,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             const bool evict = has_next && pn.loP > pc.loP;
             const int nev = evict ? pn.loP - pc.loP : 0;
             const bool ev1 = nev == 1;
-            const int lons = pn.sP % XSP;
+            const int lons = slot_of(pn.sP);
             if (ev1) { // copied into shared memory in the background
                 if (tid < Np) cp_async8(ev_y + tid, Y + size_t(pc.loP) * Np + tid);
                 if (tid == Np) cp_async8(ev_a, ag + 2 * pc.loP);
@@ -659,7 +666,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             // (2d) entering pairs: predictions start from the reduced partial sums (plus wL <x_n, dr>
             //      after an eviction: their partial sums used r from before it)
             for (int i = kThreads - 1 - tid; i < 2 * min(ne, kMaxEnter) && i >= 0; i += kThreads) {
-                const int e = i >> 1, row = i & 1, qn = (e_lo + e) % XSP;
+                const int e = i >> 1, row = i & 1, qn = slot_of(e_lo + e);
                 float s = 0.f;
                 if (fast) {
                     const int fb = (t + 1) & 1; // frozen partials of the pair entering at t+1
