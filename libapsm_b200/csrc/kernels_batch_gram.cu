@@ -52,6 +52,9 @@ constexpr int kThreads = (kEpiWarps + 2) * 32;
 // max fw and max fw * |ew log2(e) * pair norm| (padded to 4)
 constexpr int kBxAw = 0, kBxNrm = 2 * kChunkPairs, kBxFw = 3 * kChunkPairs, kBxGate = 4 * kChunkPairs;
 constexpr int kBx = 4 * kChunkPairs + 4;
+// chunk data ring: the epilogue releases a chunk's data on its own, so an operand stage is free again
+// as soon as its products are done (the epilogue never reads the operands)
+constexpr int kXRing = 4;
 // per-pair error a flagged pair would exceed (soft-output units) in the single-product forms
 constexpr float kFixEps = 1.0f / 8192.0f;
 
@@ -233,7 +236,7 @@ __device__ __forceinline__ uint32_t epilogue_pairs16(const float* gv, const floa
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
     batch_gram_kernel(const BatchGramJob* __restrict__ jobs, int n_jobs, const int* __restrict__ tile_prefix, int Kpmax,
                       int stages, int* err, unsigned long long wait_ns)
 {
@@ -255,11 +258,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t b_stride = uint32_t(tile_bytes<MODE>(kChunkN, Kpmax));
     uint8_t* sA = smem;
     uint8_t* sB = sA + tile_bytes<MODE>(kTileM, Kpmax);
-    float* sX = reinterpret_cast<float*>(sB + size_t(stages) * b_stride); // [stages][kBx]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sX + size_t(stages) * kBx);
+    float* sX = reinterpret_cast<float*>(sB + size_t(stages) * b_stride); // [kXRing][kBx]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sX + size_t(kXRing) * kBx);
     uint64_t* full = bars;                // [stages]
     uint64_t* empty = bars + stages;      // [stages]
-    uint64_t* tfull = bars + 2 * stages;  // [2]
+    uint64_t* xfull = bars + 2 * stages;  // [kXRing]
+    uint64_t* xempty = xfull + kXRing;    // [kXRing]
+    uint64_t* tfull = xempty + kXRing;    // [2]
     uint64_t* tempty = tfull + 2;         // [2]
     uint64_t* afull = tempty + 2;         // [1]
     uint64_t* done = afull + 1;           // [1]
@@ -273,7 +278,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1 + kEpiWarps);
+            mbar_init(&empty[s], 1);
+        }
+        for (int j = 0; j < kXRing; ++j) {
+            mbar_init(&xfull[j], 1);
+            mbar_init(&xempty[j], kEpiWarps);
         }
         for (int s = 0; s < 2; ++s) {
             mbar_init(&tfull[s], 1);
@@ -299,17 +308,21 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             mbar_expect_tx(afull, a_bytes);
             bulk_g2s(sA, jb.a_ops + size_t(tile) * a_bytes, a_bytes, afull);
-            int issued = 0;
+            int issued = 0, xissued = 0;
             for (int i = 0; i < nch; ++i) {
-                const int s = i % stages;
+                const int s = i % stages, j = i % kXRing;
                 if (i >= stages && !mbar_wait(&empty[s], ((i / stages) - 1) & 1, abort_flag, wait_ns)) break;
                 ++issued;
-                mbar_expect_tx(&full[s], b_bytes + kBx * 4);
+                mbar_expect_tx(&full[s], b_bytes);
                 bulk_g2s(sB + size_t(s) * b_stride, jb.b_ops + size_t(i) * b_bytes, b_bytes, &full[s]);
-                bulk_g2s(sX + size_t(s) * kBx, jb.bx + size_t(i) * kBx, kBx * 4, &full[s]);
+                if (i >= kXRing && !mbar_wait(&xempty[j], ((i / kXRing) - 1) & 1, abort_flag, wait_ns)) break;
+                ++xissued;
+                mbar_expect_tx(&xfull[j], kBx * 4);
+                bulk_g2s(sX + size_t(j) * kBx, jb.bx + size_t(i) * kBx, kBx * 4, &xfull[j]);
             }
             mbar_drain(afull, 0);
             for (int i = max(0, issued - stages); i < issued; ++i) mbar_drain(&full[i % stages], (i / stages) & 1);
+            for (int i = max(0, xissued - kXRing); i < xissued; ++i) mbar_drain(&xfull[i % kXRing], (i / kXRing) & 1);
         }
     } else if (warp == kEpiWarps + 1) {
         // ---------------- MMA issuer ----------------
@@ -362,11 +375,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         float f0 = 0.f, f1 = 0.f;
         for (int i = 0; i < nch; ++i) {
-            const int s = i % stages, buf = i & 1;
-            if (!mbar_wait(&full[s], (i / stages) & 1, abort_flag, wait_ns)) break;
+            const int j = i % kXRing, buf = i & 1;
+            if (!mbar_wait(&xfull[j], (i / kXRing) & 1, abort_flag, wait_ns)) break;
             if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag, wait_ns)) break;
             tc_fence_after();
-            const float* xs = sX + size_t(s) * kBx;
+            const float* xs = sX + size_t(j) * kBx;
             // can any pair of this chunk exceed the bound for a sample of this warp?  (warp-uniform)
             const bool check = fix_scale<MODE>() > 0.f && fmaf(exn_max, xs[kBxGate], xs[kBxGate + 1]) > 1.f;
 #pragma unroll 1
@@ -406,7 +419,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive(&tempty[buf]);
-                mbar_arrive(&empty[s]);
+                mbar_arrive(&xempty[j]);
             }
         }
         asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");
@@ -431,7 +444,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 template <int MODE> size_t gram_smem(int Kpmax, int stages)
 {
     return tile_bytes<MODE>(kTileM, Kpmax) + size_t(stages) * tile_bytes<MODE>(kChunkN, Kpmax) +
-           size_t(stages) * kBx * 4 + sizeof(uint64_t) * (2 * stages + 6) + 16 + sizeof(float2) * kTileM + 1024;
+           size_t(kXRing) * kBx * 4 + sizeof(uint64_t) * (2 * stages + 2 * kXRing + 6) + 16 + sizeof(float2) * kTileM +
+           1024;
 }
 
 template <int MODE>
