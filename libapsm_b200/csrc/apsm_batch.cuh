@@ -164,7 +164,9 @@ cudaError_t launch_rows_to_pool(const float* X, const float* nrm, const float* d
                                 int Dp, int Np, float2* Y, float* pn, float* y, float* a, cudaStream_t s);
 
 // max_n: largest antenna count of the jobs (sizes the kernel's shared memory)
-cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s);
+// max_blocks > 0 bounds the grid (blocks then loop over the (job, chunk) units)
+cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s,
+                              int max_blocks = 0);
 cudaError_t launch_batch_copy(const BatchCopyJob* d_jobs, int n_jobs, int max_pairs, int max_np, cudaStream_t s);
 // row_split: blocks per column group, each taking every row_split-th pass of
 // kColRows column entries (entries are computed alike whatever the split).

@@ -58,6 +58,9 @@ struct Lane {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_start = nullptr;
     std::vector<cudaEvent_t> seg_ev; // per detection segment: its samples arrived
+    // training samples packed on the copy stream, one launch per antenna class (the kernel
+    // columns of a class wait for its pack only)
+    cudaEvent_t ev_pack[5] = {};
     bool have_train = false, have_detect = false;
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -97,31 +100,30 @@ double host_us()
 const void* device_view(const void* p, size_t bytes)
 {
     if (!p || bytes == 0) return nullptr;
-    // the driver's pointer query, looked up through the runtime (the library links no libcuda)
-    using PtrAttrFn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
-    static PtrAttrFn cuPointerGetAttribute = [] {
+    // the driver's pointer query (all four attributes in one call; a batch asks for every
+    // input and output buffer), looked up through the runtime (the library links no libcuda)
+    using PtrAttrsFn = CUresult (*)(unsigned int, CUpointer_attribute*, void**, CUdeviceptr);
+    static PtrAttrsFn cuPointerGetAttributes = [] {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        if (cudaGetDriverEntryPoint("cuPointerGetAttributes", &fn, cudaEnableDefault, &q) != cudaSuccess ||
             q != cudaDriverEntryPointSuccess) {
             cudaGetLastError();
             fn = nullptr;
         }
-        return reinterpret_cast<PtrAttrFn>(fn);
+        return reinterpret_cast<PtrAttrsFn>(fn);
     }();
-    if (!cuPointerGetAttribute) return nullptr;
+    if (!cuPointerGetAttributes) return nullptr;
     const CUdeviceptr a = CUdeviceptr(reinterpret_cast<uintptr_t>(p));
     unsigned int type = 0;
     CUdeviceptr start = 0, dptr = 0;
     size_t size = 0;
-    if (cuPointerGetAttribute(&type, CU_POINTER_ATTRIBUTE_MEMORY_TYPE, a) != CUDA_SUCCESS || type != CU_MEMORYTYPE_HOST)
-        return nullptr;
-    if (cuPointerGetAttribute(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, a) != CUDA_SUCCESS ||
-        cuPointerGetAttribute(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, a) != CUDA_SUCCESS)
-        return nullptr;
-    if (a < start || a - start > size || bytes > size - (a - start)) return nullptr;
-    if (cuPointerGetAttribute(&dptr, CU_POINTER_ATTRIBUTE_DEVICE_POINTER, a) != CUDA_SUCCESS || dptr == 0)
-        return nullptr;
+    CUpointer_attribute attrs[4] = {CU_POINTER_ATTRIBUTE_MEMORY_TYPE, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR,
+                                    CU_POINTER_ATTRIBUTE_RANGE_SIZE, CU_POINTER_ATTRIBUTE_DEVICE_POINTER};
+    void* data[4] = {&type, &start, &size, &dptr};
+    // (memory the driver does not know reads as type 0: not page-locked)
+    if (cuPointerGetAttributes(4, attrs, data, a) != CUDA_SUCCESS || type != CU_MEMORYTYPE_HOST) return nullptr;
+    if (a < start || a - start > size || bytes > size - (a - start) || dptr == 0) return nullptr;
     return reinterpret_cast<const void*>(dptr);
 }
 
@@ -399,6 +401,8 @@ apsm_pool::~apsm_pool()
         if (l.desc_copied) cudaEventDestroy(l.desc_copied);
         if (l.copy_stream) cudaStreamSynchronize(l.copy_stream);
         if (l.ev_start) cudaEventDestroy(l.ev_start);
+        for (auto& e : l.ev_pack)
+            if (e) cudaEventDestroy(e);
         for (auto& e : l.seg_ev)
             if (e) cudaEventDestroy(e);
         if (l.copy_stream) cudaStreamDestroy(l.copy_stream);
@@ -898,6 +902,17 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     auto* h_co = reinterpret_cast<BatchCopyJob*>(hst + off_co);
     size_t ipack = 0, icopy = 0;
     int max_len = 0, max_np = 1, max_n = 1, max_pairs_in = 0, max_pairs_out = 0;
+    // antenna classes of the kernel-column launches; the training samples are packed in class
+    // order, so that each class's pack is one contiguous launch
+    auto cls_of = [](int n) { return n <= 4 ? 0 : n <= 8 ? 1 : n <= 16 ? 2 : n <= 32 ? 3 : 4; };
+    struct PackClass {
+        int first = 0, count = 0, max_len = 0, max_n = 1;
+    };
+    PackClass pcls[5];
+    for (size_t k = 0; k < nT; ++k) ++pcls[cls_of(int(tp[k].det->N))].count;
+    for (int c = 1; c < 5; ++c) pcls[c].first = pcls[c - 1].first + pcls[c - 1].count;
+    int pfill[5];
+    for (int c = 0; c < 5; ++c) pfill[c] = pcls[c].first;
     for (size_t k = 0; k < nT; ++k) {
         TrainPlan& t = tp[k];
         PoolDet& d = *t.det;
@@ -916,8 +931,15 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             max_pairs_in = std::max(max_pairs_in, int(t.usedP));
         }
         const int* perm = cfg.shuffle ? reinterpret_cast<const int*>(D(t.perm_off)) : nullptr;
-        h_pj[ipack++] = BatchPackJob{rx, tx, perm, Y + size_t(t.usedP) * d.Np, nrm + t.usedP, yv + 2 * t.usedP,
-                                     av + 2 * t.usedP, int(t.P), int(d.N), int(d.Np)};
+        {
+            PackClass& pc = pcls[cls_of(int(d.N))];
+            h_pj[pfill[cls_of(int(d.N))]++] =
+                BatchPackJob{rx, tx, perm, Y + size_t(t.usedP) * d.Np, nrm + t.usedP, yv + 2 * t.usedP,
+                             av + 2 * t.usedP, int(t.P), int(d.N), int(d.Np)};
+            pc.max_len = std::max(pc.max_len, int(t.P));
+            pc.max_n = std::max(pc.max_n, int(d.N));
+            ++ipack;
+        }
         max_len = std::max(max_len, int(t.P));
         max_np = std::max(max_np, int(d.Np));
         max_n = std::max(max_n, int(d.N));
@@ -960,7 +982,6 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     };
     KcolClass kcls[5];
     {
-        auto cls_of = [](int n) { return n <= 4 ? 0 : n <= 8 ? 1 : n <= 16 ? 2 : n <= 32 ? 3 : 4; };
         for (size_t k = 0; k < nT; ++k) {
             KcolClass& kc = kcls[cls_of(int(tp[k].det->N))];
             ++(tp[k].kc_tc ? kc.tc_count : kc.count);
@@ -1112,8 +1133,26 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         POOL_CK(launch_batch_copy(reinterpret_cast<const BatchCopyJob*>(D(off_ci)), int(nCopyIn), max_pairs_in, max_np, s));
         L.launches += nCopyIn > 0 && max_pairs_in > 0;
     }
-    if (pack_train > 0) { // training samples (detection reads its samples as the caller holds them)
-        POOL_CK(launch_batch_pack(reinterpret_cast<const BatchPackJob*>(D(off_pj)), int(pack_train), max_len, max_n, s));
+    // training samples (detection reads its samples as the caller holds them).  With host inputs
+    // on the copy stream (overlap), each class is packed there -- from page-locked buffers the
+    // pack reads over the link -- while the previous class's kernel columns run, and the detection
+    // samples follow the packs on that stream, so they do not share the link with them
+    const auto* d_pj = reinterpret_cast<const BatchPackJob*>(D(off_pj));
+    bool packed_on_copy[5] = {};
+    if (pack_train > 0 && overlap) {
+        POOL_CK(cudaStreamWaitEvent(L.copy_stream, L.ev_start, 0));
+        for (int c = 0; c < 5; ++c) {
+            if (pcls[c].count == 0 || pcls[c].max_len <= 0) continue;
+            // (two blocks per SM: reads over the link need few blocks in flight, and the kernel
+            // columns of the classes packed before run beside them)
+            POOL_CK(launch_batch_pack(d_pj + pcls[c].first, pcls[c].count, pcls[c].max_len, pcls[c].max_n,
+                                      L.copy_stream, 2 * sms));
+            POOL_CK(cudaEventRecord(L.ev_pack[c], L.copy_stream));
+            packed_on_copy[c] = true;
+            ++L.launches;
+        }
+    } else if (pack_train > 0) {
+        POOL_CK(launch_batch_pack(d_pj, int(pack_train), max_len, max_n, s));
         L.launches += max_len > 0;
     }
     if (trace) POOL_CK(cudaEventRecord(L.tr[2], s));
@@ -1122,7 +1161,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         const int* d_ko = reinterpret_cast<const int*>(D(off_ko));
         const auto* d_kt = reinterpret_cast<const BatchKcolTcJob*>(D(off_kt));
         const int* d_ktp = reinterpret_cast<const int*>(D(off_ktp));
-        for (const KcolClass& kc : kcls) {
+        for (int c = 0; c < 5; ++c) {
+            const KcolClass& kc = kcls[c];
+            if (packed_on_copy[c] && (kc.tc_count > 0 || (kc.count > 0 && kc.max_cols > 0)))
+                POOL_CK(cudaStreamWaitEvent(s, L.ev_pack[c], 0));
             if (kc.tc_count > 0) {
                 POOL_CK(launch_batch_kcol_tc(d_kt + kc.tc_first, kc.tc_count, kc.tc_units, d_ktp + kc.tc_prefix,
                                              kc.tc_chunks, kc.tc_kp, cm, d_err, s));
@@ -1140,6 +1182,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             ++L.launches;
         }
         if (trace) POOL_CK(cudaEventRecord(L.tr[3], s));
+        for (int c = 0; c < 5; ++c) // (a class without kernel columns to compute)
+            if (packed_on_copy[c]) POOL_CK(cudaStreamWaitEvent(s, L.ev_pack[c], 0));
         const int per_sm = shape.sweep_per_sm > 0 ? std::min(shape.sweep_per_sm, sweep_ctas) : sweep_ctas;
         const int grid = int(std::min<size_t>(nT, size_t(per_sm) * sms));
         if (timing) POOL_CK(cudaEventRecord(L.ev[4], s));
@@ -1598,6 +1642,9 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
             return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         if (cudaStreamCreateWithFlags(&l.copy_stream, cudaStreamNonBlocking) != cudaSuccess)
             return failp("cudaStreamCreate failed", APSM_ERR_CUDA);
+        for (auto& e : l.ev_pack)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+                return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         for (auto& e : l.tr)
             if (cudaEventCreate(&e) != cudaSuccess) return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         if (cudaMallocHost(reinterpret_cast<void**>(&l.err_host), sizeof(int)) != cudaSuccess)

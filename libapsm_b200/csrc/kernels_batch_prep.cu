@@ -16,40 +16,48 @@ namespace {
 
 constexpr int kPackChunk = 64;
 
-__global__ void __launch_bounds__(256) batch_pack_kernel(const BatchPackJob* __restrict__ jobs, int smem_n)
+// Units (job, chunk of kPackChunk pairs) of a gx-wide grid over the jobs; a block takes units
+// blockIdx.x, + gridDim.x, ... (a bounded grid leaves the SMs to concurrent work while the pack
+// waits on reads over the host link)
+__global__ void __launch_bounds__(256) batch_pack_kernel(const BatchPackJob* __restrict__ jobs, int n_jobs, int gx,
+                                                          int smem_n)
 {
-    const BatchPackJob jb = jobs[blockIdx.y];
-    const int i0 = blockIdx.x * kPackChunk;
-    if (i0 >= jb.L || jb.N > smem_n) return; // shared memory is sized for smem_n antennas
-    const int n = min(kPackChunk, jb.L - i0);
     extern __shared__ float2 sm[]; // [kPackChunk][N + 1]
-    const int N = jb.N, Np = jb.Np, pitch = N + 1;
-    for (int idx = threadIdx.x; idx < N * kPackChunk; idx += blockDim.x) {
-        const int k = idx / kPackChunk, i = idx % kPackChunk;
-        if (i < n) {
-            const int src = jb.perm ? jb.perm[i0 + i] : i0 + i;
-            sm[i * pitch + k] = jb.rx[size_t(k) * jb.L + src];
+    const long long units = (long long)n_jobs * gx;
+    for (long long u = blockIdx.x; u < units; u += gridDim.x) {
+        const BatchPackJob jb = jobs[u / gx];
+        const int i0 = int(u % gx) * kPackChunk;
+        if (i0 >= jb.L || jb.N > smem_n) continue; // shared memory is sized for smem_n antennas
+        const int n = min(kPackChunk, jb.L - i0);
+        const int N = jb.N, Np = jb.Np, pitch = N + 1;
+        __syncthreads(); // the previous unit's reads of sm are done
+        for (int idx = threadIdx.x; idx < N * kPackChunk; idx += blockDim.x) {
+            const int k = idx / kPackChunk, i = idx % kPackChunk;
+            if (i < n) {
+                const int src = jb.perm ? jb.perm[i0 + i] : i0 + i;
+                sm[i * pitch + k] = jb.rx[size_t(k) * jb.L + src];
+            }
         }
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < n * Np; idx += blockDim.x) {
-        const int i = idx / Np, k = idx % Np;
-        jb.Y[size_t(i0 + i) * Np + k] = k < N ? sm[i * pitch + k] : make_float2(0.f, 0.f);
-    }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        float s = 0.f;
-        for (int k = 0; k < N; ++k) s = fmaf(sm[i * pitch + k].x, sm[i * pitch + k].x, s);
-        for (int k = 0; k < N; ++k) s = fmaf(sm[i * pitch + k].y, sm[i * pitch + k].y, s);
-        jb.nrm[i0 + i] = s;
-        if (jb.y) {
-            const int src = jb.perm ? jb.perm[i0 + i] : i0 + i;
-            const float2 t = jb.tx[src];
-            jb.y[2 * (i0 + i)] = t.x;
-            jb.y[2 * (i0 + i) + 1] = t.y;
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < n * Np; idx += blockDim.x) {
+            const int i = idx / Np, k = idx % Np;
+            jb.Y[size_t(i0 + i) * Np + k] = k < N ? sm[i * pitch + k] : make_float2(0.f, 0.f);
         }
-        if (jb.a) {
-            jb.a[2 * (i0 + i)] = 0.f;
-            jb.a[2 * (i0 + i) + 1] = 0.f;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            float s = 0.f;
+            for (int k = 0; k < N; ++k) s = fmaf(sm[i * pitch + k].x, sm[i * pitch + k].x, s);
+            for (int k = 0; k < N; ++k) s = fmaf(sm[i * pitch + k].y, sm[i * pitch + k].y, s);
+            jb.nrm[i0 + i] = s;
+            if (jb.y) {
+                const int src = jb.perm ? jb.perm[i0 + i] : i0 + i;
+                const float2 t = jb.tx[src];
+                jb.y[2 * (i0 + i)] = t.x;
+                jb.y[2 * (i0 + i) + 1] = t.y;
+            }
+            if (jb.a) {
+                jb.a[2 * (i0 + i)] = 0.f;
+                jb.a[2 * (i0 + i) + 1] = 0.f;
+            }
         }
     }
 }
@@ -71,11 +79,15 @@ __global__ void __launch_bounds__(256) batch_copy_kernel(const BatchCopyJob* __r
 
 } // namespace
 
-cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s)
+cudaError_t launch_batch_pack(const BatchPackJob* d_jobs, int n_jobs, int max_len, int max_n, cudaStream_t s,
+                              int max_blocks)
 {
     if (n_jobs <= 0 || max_len <= 0) return cudaSuccess;
-    dim3 grid((max_len + kPackChunk - 1) / kPackChunk, n_jobs);
-    batch_pack_kernel<<<grid, 256, sizeof(float2) * kPackChunk * (max_n + 1), s>>>(d_jobs, max_n);
+    const int gx = (max_len + kPackChunk - 1) / kPackChunk;
+    long long blocks = (long long)gx * n_jobs;
+    if (max_blocks > 0) blocks = std::min<long long>(blocks, max_blocks);
+    batch_pack_kernel<<<unsigned(blocks), 256, sizeof(float2) * kPackChunk * (max_n + 1), s>>>(d_jobs, n_jobs, gx,
+                                                                                               max_n);
     return cudaGetLastError();
 }
 
