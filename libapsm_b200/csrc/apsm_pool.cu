@@ -82,6 +82,8 @@ struct Lane {
     // batch timeline (APSM_POOL_TRACE): stream start, inputs copied, packed, kernel columns, swept,
     // trained (dictionary copied back), detected
     cudaEvent_t tr[7] = {};
+    cudaEvent_t tr_copy[2] = {}; // copy stream of a host-input batch: training samples packed, detection samples in
+    bool tr_overlap = false;
     double t_run0 = 0, t_run1 = 0;
     double t_mark[3] = {0, 0, 0}; // run(): planned, descriptors written, inputs staged
     int tr_nT = 0, tr_nD = 0;
@@ -407,6 +409,8 @@ apsm_pool::~apsm_pool()
             if (e) cudaEventDestroy(e);
         if (l.copy_stream) cudaStreamDestroy(l.copy_stream);
         for (auto& e : l.tr)
+            if (e) cudaEventDestroy(e);
+        for (auto& e : l.tr_copy)
             if (e) cudaEventDestroy(e);
         if (l.err_host) cudaFreeHost(l.err_host);
         if (l.stream) cudaStreamDestroy(l.stream);
@@ -1151,6 +1155,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             packed_on_copy[c] = true;
             ++L.launches;
         }
+        if (trace) POOL_CK(cudaEventRecord(L.tr_copy[0], L.copy_stream));
     } else if (pack_train > 0) {
         POOL_CK(launch_batch_pack(d_pj, int(pack_train), max_len, max_n, s));
         L.launches += max_len > 0;
@@ -1216,6 +1221,37 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
             k0 = k1;
         }
         for (size_t g = 0; g < gseg.size(); ++g) segs.push_back({size_t(gseg[g][0]), size_t(gseg[g][1]), int(g)});
+        if (overlap && segs.size() > 1) {
+            // Order of the segments when their samples come on the copy stream (which also carries
+            // the training samples first): each detection waits for its own copies, so this is a
+            // two-stage flow shop (copy, then detect) and Johnson's rule orders it -- segments whose
+            // copy is shorter than their detection first, by increasing copy time, then the others
+            // by decreasing detection time.  Times are estimates: bytes at ~45 GB/s; pair
+            // evaluations at ~8e11/s on the tensor cores (the 64-wide operand class at 1.6x the
+            // cost) and a fifth of that for the CUDA-core forms.  The estimates do not depend on
+            // the order (segments are independent).
+            std::vector<std::pair<double, double>> cost(segs.size()); // (copy, detect), seconds
+            for (size_t i = 0; i < segs.size(); ++i) {
+                double bytes = 0.0, pairs = 0.0;
+                for (size_t k = segs[i].k0; k < segs[i].k1; ++k) {
+                    bytes += double(sizeof(float2)) * dp[k].det->N * dp[k].S;
+                    pairs += double(dp[k].S) * double(dp[k].Mp);
+                }
+                const double w = segs[i].g < 0 ? 5.0 : (dp[segs[i].k0].Kp > 32 ? 1.6 : 1.0);
+                cost[i] = {bytes / 45e9, w * pairs / 8e11};
+            }
+            std::vector<size_t> ord(segs.size());
+            for (size_t i = 0; i < ord.size(); ++i) ord[i] = i;
+            std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
+                const bool fx = cost[x].first < cost[x].second, fy = cost[y].first < cost[y].second;
+                if (fx != fy) return fx;
+                return fx ? cost[x].first < cost[y].first : cost[x].second > cost[y].second;
+            });
+            std::vector<Seg> sorted;
+            sorted.reserve(segs.size());
+            for (size_t i : ord) sorted.push_back(segs[i]);
+            segs.swap(sorted);
+        }
         if (overlap) {
             while (L.seg_ev.size() < segs.size()) {
                 cudaEvent_t e = nullptr;
@@ -1231,6 +1267,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                 }
                 POOL_CK(cudaEventRecord(L.seg_ev[i], L.copy_stream));
             }
+            if (trace) POOL_CK(cudaEventRecord(L.tr_copy[1], L.copy_stream));
         }
         // page-locked outputs of a few jobs: one copy each; of many jobs: one copy per segment,
         // scattered by finish() (per-copy cost exceeds a host memcpy then)
@@ -1285,6 +1322,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     if (trace) {
         POOL_CK(cudaEventRecord(L.tr[6], s));
         L.traced = true;
+        L.tr_overlap = overlap && pack_train > 0;
         L.tr_nT = int(nT);
         L.tr_nD = int(nD);
         L.t_run0 = t_run0;
@@ -1521,13 +1559,18 @@ apsm_status apsm_pool::finish(uint32_t lane_id)
         // one line per batch: lane, jobs, host run() time, host gap until finish(), finish's wait and rest,
         // GPU: inputs copied, packed, kernel columns, sweep, dictionary copied back, detected (+ results
         // copied) -- microseconds
-        float g[6] = {0, 0, 0, 0, 0, 0};
+        // (copy stream, host-input batches: training samples packed and detection samples in, from
+        // the batch's first GPU mark; -1 otherwise)
+        float g[6] = {0, 0, 0, 0, 0, 0}, gc[2] = {-1e-3f, -1e-3f};
         for (int k = 0; k < 6; ++k)
             if (cudaEventElapsedTime(&g[k], L.tr[k], L.tr[k + 1]) != cudaSuccess) g[k] = -1e-3f;
+        for (int k = 0; k < 2 && L.tr_overlap; ++k)
+            if (cudaEventElapsedTime(&gc[k], L.tr[0], L.tr_copy[k]) != cudaSuccess) gc[k] = -1e-3f;
         cudaGetLastError();
-        std::fprintf(trace, "%u %d %d %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f\n", lane_id,
-                     L.tr_nT, L.tr_nD, L.t_run1 - L.t_run0, t0 - L.t_run1, t1 - t0, host_us() - t1, 1e3 * g[0],
-                     1e3 * g[1], 1e3 * g[2], 1e3 * g[3], 1e3 * g[4], 1e3 * g[5], L.t_mark[0], L.t_mark[1], L.t_mark[2]);
+        std::fprintf(trace, "%u %d %d %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f %.1f\n",
+                     lane_id, L.tr_nT, L.tr_nD, L.t_run1 - L.t_run0, t0 - L.t_run1, t1 - t0, host_us() - t1,
+                     1e3 * g[0], 1e3 * g[1], 1e3 * g[2], 1e3 * g[3], 1e3 * g[4], 1e3 * g[5], L.t_mark[0], L.t_mark[1],
+                     L.t_mark[2], 1e3 * gc[0], 1e3 * gc[1]);
         L.traced = false;
     }
     return st;
@@ -1647,6 +1690,8 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
                 return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         for (auto& e : l.tr)
             if (cudaEventCreate(&e) != cudaSuccess) return failp("cudaEventCreate failed", APSM_ERR_CUDA);
+        for (auto& e : l.tr_copy)
+            if (cudaEventCreate(&e) != cudaSuccess) return failp("cudaEventCreate failed", APSM_ERR_CUDA);
         if (cudaMallocHost(reinterpret_cast<void**>(&l.err_host), sizeof(int)) != cudaSuccess)
             return failp("cudaMallocHost failed", APSM_ERR_CUDA);
         *l.err_host = 0;
@@ -1662,7 +1707,8 @@ extern "C" apsm_status apsm_pool_create(const char* algorithm_json, uint64_t hbm
         if (p->trace)
             std::fprintf(p->trace, "# lane n_train n_detect run_us gap_us fin_wait_us fin_rest_us gpu_inputs_us "
                                    "gpu_pack_us gpu_kcol_us gpu_sweep_us gpu_copyout_us gpu_detect_us "
-                                   "run_planned_us run_described_us run_staged_us\n");
+                                   "run_planned_us run_described_us run_staged_us gpu_packed_at_us "
+                                   "gpu_detect_inputs_at_us\n");
     }
     if (cudaStreamCreateWithFlags(&p->sched_stream, cudaStreamNonBlocking) != cudaSuccess)
         return failp("cudaStreamCreate failed", APSM_ERR_CUDA);
