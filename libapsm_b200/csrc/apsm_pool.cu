@@ -259,6 +259,7 @@ private:
 
 constexpr size_t kDirectOutJobs = 16; // detection jobs whose estimates are copied to the caller one by one
 constexpr size_t kZeroCopyMin = size_t(4) << 20; // training inputs read in place from this many bytes on
+constexpr size_t kSplitGroup = size_t(32) << 20;  // pageable detection samples staged and uploaded in groups of this size
 constexpr size_t kArenaJobs = 32;     // training jobs from which a batch reads its step lists from the arena
 
 int detect_class(uint32_t N)
@@ -869,6 +870,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     };
     std::vector<HostIn> ins;
     bool direct = false;
+    bool stage_split = false; // pageable detection samples staged and uploaded per segment while the batch trains
     if (host) {
         if (!zc_train)
             for (const auto& t : tp) {
@@ -889,12 +891,21 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                     direct = false;
                     break;
                 }
-        // staged: every input (no direct copies), or the training inputs of a direct batch --
-        // many small copies cost more per byte than helper threads' memcpy plus one upload
+        // a batch that trains and detects from ordinary (pageable) buffers: the training inputs are
+        // staged and uploaded first; the detection samples are staged segment by segment after
+        // the training launches and uploaded on the copy stream while the batch trains
+        if (!direct && nT > 0 && nD > 0) {
+            size_t det_bytes = 0;
+            for (const auto& in : ins) det_bytes += in.detect ? in.bytes : 0;
+            stage_split = det_bytes >= kZeroCopyMin;
+        }
+        // staged: every input (no direct copies), or the training inputs of a direct or split batch
+        // -- many small copies cost more per byte than helper threads' memcpy plus one upload
         std::vector<Stager::Range> pieces;
         pieces.reserve(ins.size());
         for (const auto& in : ins)
-            if (!direct || !in.detect) pieces.push_back({hst + in.off, static_cast<const char*>(in.src), in.bytes});
+            if (!(direct || stage_split) || !in.detect)
+                pieces.push_back({hst + in.off, static_cast<const char*>(in.src), in.bytes});
         stager.begin(pieces); // joined before the upload; the descriptors are written meanwhile
     }
 
@@ -1105,13 +1116,13 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
     stager.wait();
     const double t_stage = trace ? host_us() : 0.0;
     if (trace) POOL_CK(cudaEventRecord(L.tr[0], s));
-    // a batch that trains and detects from page-locked buffers copies the detection samples
-    // on the lane's copy stream while it trains: after the upload of the descriptors and
-    // training inputs (which would otherwise share the link with them and delay the
-    // training) and after the lane's earlier work (the scratch is free); the detections
-    // wait for them
-    const bool overlap = direct && nT > 0 && nD > 0;
-    POOL_CK(cudaMemcpyAsync(dev, hst, direct ? off_det_in : desc_bytes, cudaMemcpyHostToDevice, s));
+    // a batch that trains and detects from page-locked buffers (or stages pageable ones per
+    // segment) copies the detection samples on the lane's copy stream while it trains: after
+    // the upload of the descriptors and training inputs (which would otherwise share the link
+    // with them and delay the training) and after the lane's earlier work (the scratch is
+    // free); the detections wait for them
+    const bool overlap = (direct || stage_split) && nT > 0 && nD > 0;
+    POOL_CK(cudaMemcpyAsync(dev, hst, (direct || stage_split) ? off_det_in : desc_bytes, cudaMemcpyHostToDevice, s));
     if (direct && !overlap)
         for (const auto& in : ins)
             if (in.detect) POOL_CK(cudaMemcpyAsync(dev + in.off, in.src, in.bytes, cudaMemcpyHostToDevice, s));
@@ -1259,16 +1270,38 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                 L.seg_ev.push_back(e);
             }
             POOL_CK(cudaStreamWaitEvent(L.copy_stream, L.ev_start, 0));
-            for (size_t i = 0; i < segs.size(); ++i) {
+        }
+        // segment i's samples onto the copy stream, then its event; issued just before the
+        // segment's detection launches (a detection does not wait for the staging of later segments)
+        auto copy_segment = [&](size_t i) -> apsm_status {
+            if (stage_split) {
+                // the segment's samples (contiguous in the staging layout) in groups of jobs of
+                // ~kSplitGroup bytes: a group is staged by the helper threads, then uploaded in
+                // one copy while the next group is staged
+                std::vector<Stager::Range> pieces;
+                size_t lo = dp[segs[i].k0].off_rx, hi = lo;
+                for (size_t k = segs[i].k0; k < segs[i].k1; ++k) {
+                    const DetectPlan& q = dp[k];
+                    const size_t bytes = sizeof(float2) * size_t(q.det->N) * q.S;
+                    pieces.push_back({hst + q.off_rx, reinterpret_cast<const char*>(jobs[q.job].rx), bytes});
+                    hi = q.off_rx + bytes;
+                    if (hi - lo >= kSplitGroup || k + 1 == segs[i].k1) {
+                        stager.copy(pieces);
+                        POOL_CK(cudaMemcpyAsync(dev + lo, hst + lo, hi - lo, cudaMemcpyHostToDevice, L.copy_stream));
+                        pieces.clear();
+                        if (k + 1 < segs[i].k1) lo = dp[k + 1].off_rx;
+                    }
+                }
+            } else {
                 for (size_t k = segs[i].k0; k < segs[i].k1; ++k) {
                     const DetectPlan& q = dp[k];
                     POOL_CK(cudaMemcpyAsync(dev + q.off_rx, jobs[q.job].rx, sizeof(float2) * size_t(q.det->N) * q.S,
                                             cudaMemcpyHostToDevice, L.copy_stream));
                 }
-                POOL_CK(cudaEventRecord(L.seg_ev[i], L.copy_stream));
             }
-            if (trace) POOL_CK(cudaEventRecord(L.tr_copy[1], L.copy_stream));
-        }
+            POOL_CK(cudaEventRecord(L.seg_ev[i], L.copy_stream));
+            return APSM_OK;
+        };
         // page-locked outputs of a few jobs: one copy each; of many jobs: one copy per segment,
         // scattered by finish() (per-copy cost exceeds a host memcpy then)
         const bool est_out = host && est_bytes > 0;
@@ -1284,7 +1317,11 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         const int* d_gp = reinterpret_cast<const int*>(D(off_gp));
         for (size_t i = 0; i < segs.size(); ++i) {
             const Seg& sg = segs[i];
-            if (overlap) POOL_CK(cudaStreamWaitEvent(s, L.seg_ev[i], 0));
+            if (overlap) {
+                const apsm_status st = copy_segment(i);
+                if (st != APSM_OK) return st;
+                POOL_CK(cudaStreamWaitEvent(s, L.seg_ev[i], 0));
+            }
             if (sg.g < 0) {
                 int tiles = 0;
                 for (size_t k = sg.k0; k < sg.k1; ++k)
@@ -1308,6 +1345,11 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                 POOL_CK(cudaMemcpyAsync(static_cast<char*>(L.pinned_out) + (lo - est_begin), D(lo), hi - lo,
                                         cudaMemcpyDeviceToHost, s));
             }
+        }
+        if (overlap) {
+            // (the staging buffer is consumed once the last upload is done)
+            if (stage_split) POOL_CK(cudaEventRecord(L.desc_copied, L.copy_stream));
+            if (trace) POOL_CK(cudaEventRecord(L.tr_copy[1], L.copy_stream));
         }
         if (est_out && !out_direct)
             for (const auto& q : dp) L.pending.push_back({jobs[q.job].est, q.off_est - est_begin, sizeof(float2) * q.S});

@@ -350,6 +350,30 @@ def test_pool_page_locked_training_inputs_read_in_place(native_lib):
         np.testing.assert_array_equal(a, b)
 
 
+def test_pool_pageable_detection_samples_staged_while_training(native_lib):
+    """A batch that trains and detects from ordinary (pageable) buffers with >= 4 MB of
+    detection samples stages and uploads them per detection segment while it trains; the
+    estimates equal those of the same training and detection run as two batches (the second
+    one stages everything before its upload)."""
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    frames = [(N,) + _frame(800 + i, N, 300, 6000) for i, N in enumerate([4, 8, 16, 32])]
+    outs = {}
+    for mode in ("one batch", "two batches"):
+        pool = DetectorPool(dict(CFG, detectVersion="gram_tf32x3"))
+        dets = [(pool.add(f[0]), f) for _ in range(4) for f in frames]  # 16 detectors, 11.5 MB of samples
+        train = [PoolJob(d, f[1], f[2], fresh=True) for d, f in dets]
+        detect = [PoolJob(d, f[3]) for d, f in dets]
+        if mode == "one batch":
+            res = pool.run(train + detect)[len(train):]
+        else:
+            pool.run(train)
+            res = pool.run(detect)
+        outs[mode] = [np.array(r) for r in res]
+    for a, b in zip(outs["one batch"], outs["two batches"]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_pool_page_locked_estimates_written_in_place(native_lib):
     """Estimates (>= 4 MB) of a host-buffer batch into page-locked buffers are
     written there by the detection kernels; they equal those of the same batch
