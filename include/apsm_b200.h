@@ -263,11 +263,17 @@ apsm_status apsm_pool_reset(apsm_pool* p, uint32_t detector);
  * detector may be trained at most once per batch), then all detection jobs,
  * which see this batch's training.  Host modes, inputs: a batch with 4 MB or
  * more of training inputs whose buffers are page-locked and mapped for the
- * device has them read in place by the packing kernel; detection samples in
- * page-locked buffers are copied to the device straight from them on a second
- * stream while the batch trains; everything else (pageable buffers, small
- * batches) is staged by host helper threads through the lane's pinned buffer
- * and uploaded with the job descriptors.  Estimates: into page-locked,
+ * device has them read in place by the packing kernel (one launch per antenna
+ * class on a second stream, beside the kernel columns of the classes packed
+ * before); detection samples in page-locked buffers are copied to the device
+ * straight from them on that stream while the batch trains; in a batch that
+ * trains and has 4 MB or more of detection samples in pageable buffers, those
+ * are staged by host helper threads and uploaded on that stream in groups of
+ * about 32 MB while the batch trains (the call returns once they are staged);
+ * everything else (small batches, training inputs in pageable buffers) is
+ * staged through the lane's pinned buffer and uploaded with the job
+ * descriptors.  Detection runs in segments of one launch shape, each waiting
+ * for its own samples only.  Estimates: into page-locked,
  * device-mapped caller buffers (batches with 4 MB of estimates or more) the
  * detection kernels write them in place, so such buffers hold partial
  * estimates while the batch runs; otherwise each launch's estimates come
