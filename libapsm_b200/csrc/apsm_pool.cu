@@ -1158,10 +1158,10 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         POOL_CK(cudaStreamWaitEvent(L.copy_stream, L.ev_start, 0));
         for (int c = 0; c < 5; ++c) {
             if (pcls[c].count == 0 || pcls[c].max_len <= 0) continue;
-            // (two blocks per SM: reads over the link need few blocks in flight, and the kernel
-            // columns of the classes packed before run beside them)
+            // (inputs read over the link: two blocks per SM -- few blocks in flight saturate the
+            // link, and the kernel columns of the classes packed before run beside them)
             POOL_CK(launch_batch_pack(d_pj + pcls[c].first, pcls[c].count, pcls[c].max_len, pcls[c].max_n,
-                                      L.copy_stream, 2 * sms));
+                                      L.copy_stream, zc_train ? 2 * sms : 0));
             POOL_CK(cudaEventRecord(L.ev_pack[c], L.copy_stream));
             packed_on_copy[c] = true;
             ++L.launches;
