@@ -374,6 +374,38 @@ def test_pool_pageable_detection_samples_staged_while_training(native_lib):
         np.testing.assert_array_equal(a, b)
 
 
+def test_pool_page_locked_training_with_pageable_detection_samples(native_lib):
+    """Training inputs (>= 4 MB) in page-locked buffers, read in place and packed per antenna
+    class beside the kernel columns, with the detection samples in pageable buffers staged per
+    segment while the batch trains: the estimates equal those of the same training and
+    detection from pageable buffers run as two batches."""
+    import torch
+
+    from libapsm_b200 import DetectorPool, PoolJob
+
+    frames = [(N,) + _frame(900 + i, N, 1500, 3000) for i, N in enumerate([8, 16, 32, 32])]
+    keep = []
+
+    def pin(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        keep.append(t)
+        return t.numpy()
+
+    outs = {}
+    for mode in ("mixed", "two batches"):
+        pool = DetectorPool(dict(CFG, windowSize=40, dictionarySize=1500, detectVersion="gram_tf32x3"))
+        dets = [(pool.add(f[0]), f) for _ in range(4) for f in frames]  # 16 detectors, 4.4 MB of training inputs
+        if mode == "mixed":
+            train = [PoolJob(d, pin(f[1]), pin(f[2]), fresh=True) for d, f in dets]
+            res = pool.run(train + [PoolJob(d, f[3]) for d, f in dets])[len(train):]
+        else:
+            pool.run([PoolJob(d, f[1], f[2], fresh=True) for d, f in dets])
+            res = pool.run([PoolJob(d, f[3]) for d, f in dets])
+        outs[mode] = [np.array(r) for r in res]
+    for a, b in zip(outs["mixed"], outs["two batches"]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_pool_page_locked_estimates_written_in_place(native_lib):
     """Estimates (>= 4 MB) of a host-buffer batch into page-locked buffers are
     written there by the detection kernels; they equal those of the same batch
