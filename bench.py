@@ -233,14 +233,29 @@ def latency_roofline(pool, L, dets, ids, dev_in, sweep_ms: float, slots: int, sm
 
 def sfu_roofline(dets, dict_size: int, detect_ms: float, sms: int, sm_mhz: float | None) -> dict:
     """Exponential-unit bound of the batch's detection: per (data symbol,
-    dictionary pair) the pair form needs 3 exponentials (ex2 on the SFU, 16
-    per clock per SM); the stage time includes the operand packing."""
+    dictionary pair) the pair form needs 3 exponentials (one ex2.approx each);
+    the denominator is the SFU rate measured on this device by
+    apsm_measure_ex2_rate (a kernel of nothing but independent ex2 chains),
+    with the nominal 16 per clock per SM beside it.  The stage time includes
+    the operand packing."""
+    import ctypes
+
+    from libapsm_b200 import _native
+
     pairs = sum(d.S * min(d.P, dict_size) for d in dets)
     mhz = sm_mhz or 1965.0
-    floor_ms = 3.0 * pairs / (sms * 16 * mhz * 1e6) * 1e3
+    nominal = sms * 16 * mhz * 1e6
+    rate, ms = ctypes.c_double(0.0), ctypes.c_float(0.0)
+    measured = None
+    if _native.load().apsm_measure_ex2_rate(ctypes.byref(rate), ctypes.byref(ms)) == 0 and rate.value > 0:
+        measured = rate.value
+    peak = measured or nominal
+    floor_ms = 3.0 * pairs / peak * 1e3
     return {"kernel": "batch_gram_kernel + operand packing (detection stage)", "pair_evaluations": pairs,
             "exponentials": 3 * pairs, "floor_ms": floor_ms, "stage_ms": detect_ms, "frac": floor_ms / detect_ms,
-            "clock_mhz": mhz}
+            "peak_ex2_per_s": peak, "peak_source": "measured (apsm_measure_ex2_rate)" if measured else "nominal",
+            "measured_ex2_per_clk_per_sm": (measured / (sms * mhz * 1e6)) if measured else None,
+            "nominal_ex2_per_s": nominal, "clock_mhz": mhz}
 
 
 batched_est_host: list = []  # the last batched run's estimates (rank 0), for the CPU sample's SER

@@ -206,6 +206,14 @@ const char* apsm_last_error(const apsm_detector* h);
 void apsm_set_wait_limit_ns(uint64_t ns);
 uint64_t apsm_wait_limit_ns(void);
 
+/* Measured exponential throughput of the current device's SFUs
+ * (ex2.approx.ftz.f32 per second, all SMs; the detection kernels' every
+ * exponential is one such instruction): the denominator of the detection
+ * stage's roofline.  Runs a warm-up and a timed launch of ~2 ms on its own
+ * stream; ms (optional) receives the timed launch's duration.  No counterpart
+ * in the reference. */
+apsm_status apsm_measure_ex2_rate(double* per_second, float* ms);
+
 /* ======================================================================
  * Detector pool: many resident detectors (users x cells), batched jobs.
  *

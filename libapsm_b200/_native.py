@@ -66,6 +66,7 @@ SIGNATURES = [
     ("apsm_last_error", ctypes.c_char_p, [_P]),
     ("apsm_set_wait_limit_ns", None, [ctypes.c_uint64]),
     ("apsm_wait_limit_ns", ctypes.c_uint64, []),
+    ("apsm_measure_ex2_rate", ctypes.c_int, [ctypes.POINTER(ctypes.c_double), _F]),
     # detector pool (batched many-detector form)
     ("apsm_pool_create", ctypes.c_int, [ctypes.c_char_p, ctypes.c_uint64, _U32, ctypes.POINTER(_P), ctypes.c_char_p,
                                         ctypes.c_size_t]),
