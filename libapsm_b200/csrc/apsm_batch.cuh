@@ -209,11 +209,11 @@ int batch_detect_chunk(); // dictionary pairs per chunk of launch_batch_detect
 // packing and the Gram kernel, whose CTA t works on tile t - tile_prefix[j]
 // of job j.
 int batch_gram_tile();        // samples per tile
-int batch_gram_chunk_pairs(); // dictionary pairs per chunk
+int batch_gram_chunk_pairs(int mode, int Kp); // dictionary pairs per chunk (64, or 32 for TF32 hi/lo above 32 features)
 int batch_gram_kp(int mode, int N);
 size_t batch_gram_a_bytes(int mode, int Kp);
 size_t batch_gram_b_bytes(int mode, int Kp);
-size_t batch_gram_bx_floats();
+size_t batch_gram_bx_floats(int mode, int Kp);
 // stages: dictionary chunks in flight, 2 or 3 (0: the built-in choice; 3 only where it fits)
 cudaError_t launch_batch_gram(int mode, const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
                               const int* d_tile_prefix, int total_tiles, int Kp_max, float wL, float wG, int* d_err,

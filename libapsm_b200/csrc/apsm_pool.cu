@@ -648,7 +648,8 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
                 d.Kp = batch_gram_kp(gram_mode, int(d.det->N));
                 d.cls = gram_class(d.Kp);
                 d.tiles = int((d.S + batch_gram_tile() - 1) / batch_gram_tile());
-                d.chunks = int((d.Mp + batch_gram_chunk_pairs() - 1) / batch_gram_chunk_pairs());
+                const int cp = batch_gram_chunk_pairs(gram_mode, d.Kp);
+                d.chunks = int((d.Mp + cp - 1) / cp);
             } else {
                 d.cls = detect_class(d.det->N);
             }
@@ -797,7 +798,7 @@ apsm_status apsm_pool::run(uint32_t lane_id, const apsm_job* jobs, uint32_t n, i
         if (d.gram) {
             d.off_aops = o; o = align_up(o + batch_gram_a_bytes(gram_mode, d.Kp) * d.tiles, 256);
             d.off_bops = o; o = align_up(o + batch_gram_b_bytes(gram_mode, d.Kp) * std::max(d.chunks, 1), 256);
-            d.off_bx = o; o = align_up(o + sizeof(float) * batch_gram_bx_floats() * std::max(d.chunks, 1), 256);
+            d.off_bx = o; o = align_up(o + sizeof(float) * batch_gram_bx_floats(gram_mode, d.Kp) * std::max(d.chunks, 1), 256);
             d.off_lin = o; o = align_up(o + sizeof(float2) * d.S, 256);
         }
     }

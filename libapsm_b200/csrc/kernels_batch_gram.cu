@@ -9,7 +9,9 @@
 // and B = two rows per dictionary pair, [Re y; Im y] and [-Im y; Re y], the
 // product A B^T holds r and m in adjacent columns.  One CTA takes a tile of
 // 128 samples of one job against every chunk of 64 dictionary pairs
-// (UMMA M=128, N=128, FP32 accumulators in tensor memory, double-buffered);
+// (UMMA M=128, N=128, FP32 accumulators in tensor memory, double-buffered;
+// for the TF32 split form above 32 features, chunks of 32 pairs, N=64, with
+// the sample tile in tensor memory: two CTAs per SM instead of one);
 // the epilogue forms the three distances with FP32 norms, exponentiates on
 // the SFU and accumulates a_2b K(2b, .) + a_2b+1 K(2b+1, .) for the two soft
 // outputs of the sample (reference model cpp/lib/apsm/apsm_detect.cu:690-876).
@@ -44,14 +46,21 @@ namespace {
 using namespace tc;
 
 constexpr int kTileM = 128;      // samples per tile (UMMA M)
-constexpr int kChunkPairs = 64;  // dictionary pairs per chunk
-constexpr int kChunkN = 128;     // accumulator columns per chunk (UMMA N)
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = (kEpiWarps + 2) * 32;
-// per chunk: a*wG (128, column order), ew log2(e) * pair norms (64), fix weights fw (64), then
-// max fw and max fw * |ew log2(e) * pair norm| (padded to 4)
-constexpr int kBxAw = 0, kBxNrm = 2 * kChunkPairs, kBxFw = 3 * kChunkPairs, kBxGate = 4 * kChunkPairs;
-constexpr int kBx = 4 * kChunkPairs + 4;
+
+// Dictionary chunk of CN accumulator columns (UMMA N; two per pair) and its data: a*wG (CN, column
+// order), ew log2(e) * pair norms (CN/2), fix weights fw (CN/2), then max fw and
+// max fw * |ew log2(e) * pair norm| (padded to 4).  CN = 128, or 64 for the TF32 split form above
+// 32 features, whose sample tile then lives in tensor memory so that two CTAs share an SM.
+template <int CN> struct Chunk {
+    static constexpr int kN = CN;
+    static constexpr int kPairs = CN / 2;
+    static constexpr int kAw = 0, kNrm = CN, kFw = CN + CN / 2, kGate = 2 * CN;
+    static constexpr int kBx = 2 * CN + 4;
+    static constexpr bool kAtm = CN == 64; // sample tile in tensor memory
+};
+__host__ __device__ constexpr int chunk_cols(int mode, int Kp) { return (mode == kTF32x3 && Kp > 32) ? 64 : 128; }
 // chunk data ring: the epilogue releases a chunk's data on its own, so an operand stage is free again
 // as soon as its products are done (the epilogue never reads the operands)
 constexpr int kXRing = 4;
@@ -141,17 +150,18 @@ __global__ void __launch_bounds__(256) batch_gram_pack_a_kernel(const BatchGramJ
 
 // B operand chunks of the job's dictionary (two rows per pair) and per chunk
 // the coefficients a*wG and the pair norms.
-template <int MODE>
+template <int MODE, int CN>
 __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJob* __restrict__ jobs, float wG)
 {
+    using C = Chunk<CN>;
     const BatchGramJob& jb = jobs[blockIdx.y];
     const int c = blockIdx.x;
     if (c >= jb.n_chunks) return;
     const int N = jb.N, Np = jb.Np, Kp = jb.Kp;
-    uint8_t* chunk = jb.b_ops + size_t(c) * tile_bytes<MODE>(kChunkN, Kp);
-    for (int idx = threadIdx.x; idx < kChunkN * Kp; idx += blockDim.x) {
+    uint8_t* chunk = jb.b_ops + size_t(c) * tile_bytes<MODE>(CN, Kp);
+    for (int idx = threadIdx.x; idx < CN * Kp; idx += blockDim.x) {
         const int r = idx / Kp, k = idx % Kp;
-        const int b = c * kChunkPairs + (r >> 1);
+        const int b = c * C::kPairs + (r >> 1);
         float x = 0.f;
         if (b < jb.Mp && k < 2 * N) {
             const float2 v = jb.Yd[size_t(b) * Np + (k < N ? k : k - N)];
@@ -160,17 +170,17 @@ __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJ
         }
         float hi, lo;
         split_operand<MODE>(x, &hi, &lo);
-        put_operand<MODE>(chunk, kChunkN, r, k, hi);
-        if constexpr (OpTraits<MODE>::kSplit) put_operand<MODE>(chunk, kChunkN, r, Kp + k, lo);
+        put_operand<MODE>(chunk, CN, r, k, hi);
+        if constexpr (OpTraits<MODE>::kSplit) put_operand<MODE>(chunk, CN, r, Kp + k, lo);
     }
-    float* bx = jb.bx + size_t(c) * kBx;
-    for (int i = threadIdx.x; i < kBxFw; i += blockDim.x) {
+    float* bx = jb.bx + size_t(c) * C::kBx;
+    for (int i = threadIdx.x; i < C::kFw; i += blockDim.x) {
         float v = 0.f;
-        if (i < kBxNrm) {
-            const int b = c * kChunkPairs + (i >> 1);
+        if (i < C::kNrm) {
+            const int b = c * C::kPairs + (i >> 1);
             v = b < jb.Mp ? jb.a[2 * b + (i & 1)] * wG : 0.f;
         } else {
-            const int b = c * kChunkPairs + (i - kBxNrm);
+            const int b = c * C::kPairs + (i - C::kNrm);
             v = b < jb.Mp ? jb.ew2 * jb.nrm_d[b] : 0.f; // norms pre-scaled by ew log2(e)
         }
         bx[i] = v;
@@ -178,14 +188,14 @@ __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJ
     // fix weights of the pairs and the chunk's gate values (warp 0; 0 in the split forms)
     if (threadIdx.x < 32) {
         float g0 = 0.f, g1 = 0.f;
-        for (int p = threadIdx.x; p < kChunkPairs; p += 32) {
-            const int b = c * kChunkPairs + p;
+        for (int p = threadIdx.x; p < C::kPairs; p += 32) {
+            const int b = c * C::kPairs + p;
             float fw = 0.f, en = 0.f;
             if (b < jb.Mp) {
                 fw = (fabsf(jb.a[2 * b] * wG) + fabsf(jb.a[2 * b + 1] * wG)) * fix_scale<MODE>();
                 en = -jb.ew2 * jb.nrm_d[b];
             }
-            bx[kBxFw + p] = fw;
+            bx[C::kFw + p] = fw;
             g0 = fmaxf(g0, fw);
             g1 = fmaxf(g1, fw * en);
         }
@@ -194,7 +204,7 @@ __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJ
             g0 = fmaxf(g0, __shfl_xor_sync(0xffffffffu, g0, o));
             g1 = fmaxf(g1, __shfl_xor_sync(0xffffffffu, g1, o));
         }
-        if (threadIdx.x < 4) bx[kBxGate + threadIdx.x] = threadIdx.x == 0 ? g0 : (threadIdx.x == 1 ? g1 : 0.f);
+        if (threadIdx.x < 4) bx[C::kGate + threadIdx.x] = threadIdx.x == 0 ? g0 : (threadIdx.x == 1 ? g1 : 0.f);
     }
 }
 
@@ -202,7 +212,7 @@ __global__ void __launch_bounds__(256) batch_gram_pack_b_kernel(const BatchGramJ
 // cross terms, contracted with the pairs' coefficients into the two soft
 // outputs.  CHECK: pairs whose error bound exceeds kFixEps are left out and
 // returned as bits of the mask (pair j -> bit j).
-template <bool CHECK>
+template <bool CHECK, int CN>
 __device__ __forceinline__ uint32_t epilogue_pairs16(const float* gv, const float* xs, int p0, float exn, float m2,
                                                      float& f0, float& f1)
 {
@@ -210,10 +220,10 @@ __device__ __forceinline__ uint32_t epilogue_pairs16(const float* gv, const floa
 #pragma unroll
     for (int j = 0; j < 16; j += 2) {
         const int pj = p0 + j; // pair index within the chunk
-        const float4 aw = *reinterpret_cast<const float4*>(xs + kBxAw + 2 * pj); // pairs pj, pj+1
-        const float2 nb = *reinterpret_cast<const float2*>(xs + kBxNrm + pj);
+        const float4 aw = *reinterpret_cast<const float4*>(xs + Chunk<CN>::kAw + 2 * pj); // pairs pj, pj+1
+        const float2 nb = *reinterpret_cast<const float2*>(xs + Chunk<CN>::kNrm + pj);
         float2 fw = make_float2(0.f, 0.f);
-        if constexpr (CHECK) fw = *reinterpret_cast<const float2*>(xs + kBxFw + pj);
+        if constexpr (CHECK) fw = *reinterpret_cast<const float2*>(xs + Chunk<CN>::kFw + pj);
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const float es = exn + (e ? nb.y : nb.x), re = gv[2 * (j + e)], im = gv[2 * (j + e) + 1];
@@ -235,12 +245,18 @@ __device__ __forceinline__ uint32_t epilogue_pairs16(const float* gv, const floa
     return mask;
 }
 
-template <int MODE>
+// kAtm (CN = 64): the sample tile's operand lives in tensor memory, copied there once by the
+// epilogue warps from the packed tile; the UMMAs read only B from shared memory, and the tile's
+// shared memory is free: with 64-column chunks two CTAs share an SM (tensor memory: accumulators
+// at columns 0-127, A hi from 128, A lo from 128 + Kp).
+template <int MODE, int CN>
 __global__ void __launch_bounds__(kThreads, 2)
     batch_gram_kernel(const BatchGramJob* __restrict__ jobs, int n_jobs, const int* __restrict__ tile_prefix, int Kpmax,
                       int stages, int* err, unsigned long long wait_ns)
 {
     using T = OpTraits<MODE>;
+    using C = Chunk<CN>;
+    constexpr bool ATM = C::kAtm;
     // job of this CTA: tile_prefix[j] <= blockIdx.x < tile_prefix[j + 1]
     int lo = 0, hi = n_jobs;
     while (hi - lo > 1) {
@@ -254,12 +270,12 @@ __global__ void __launch_bounds__(kThreads, 2)
 
     extern __shared__ __align__(1024) uint8_t smem[];
     const uint32_t a_bytes = uint32_t(tile_bytes<MODE>(kTileM, jb.Kp));
-    const uint32_t b_bytes = uint32_t(tile_bytes<MODE>(kChunkN, jb.Kp));
-    const uint32_t b_stride = uint32_t(tile_bytes<MODE>(kChunkN, Kpmax));
+    const uint32_t b_bytes = uint32_t(tile_bytes<MODE>(CN, jb.Kp));
+    const uint32_t b_stride = uint32_t(tile_bytes<MODE>(CN, Kpmax));
     uint8_t* sA = smem;
-    uint8_t* sB = sA + tile_bytes<MODE>(kTileM, Kpmax);
-    float* sX = reinterpret_cast<float*>(sB + size_t(stages) * b_stride); // [kXRing][kBx]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sX + size_t(kXRing) * kBx);
+    uint8_t* sB = sA + (ATM ? 0 : tile_bytes<MODE>(kTileM, Kpmax));
+    float* sX = reinterpret_cast<float*>(sB + size_t(stages) * b_stride); // [kXRing][C::kBx]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sX + size_t(kXRing) * C::kBx);
     uint64_t* full = bars;                // [stages]
     uint64_t* empty = bars + stages;      // [stages]
     uint64_t* xfull = bars + 2 * stages;  // [kXRing]
@@ -273,7 +289,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     float2* red = reinterpret_cast<float2*>(tmem_slot + 4); // [kTileM]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr uint32_t kCols = 2 * kChunkN;
+    constexpr uint32_t kCols = ATM ? 4 * CN : 2 * CN; // a power of two: 256
+    constexpr uint32_t kAcol = 2 * CN;                // first tensor-memory column of A (ATM)
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; ++s) {
@@ -288,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             mbar_init(&tfull[s], 1);
             mbar_init(&tempty[s], kEpiWarps);
         }
-        mbar_init(afull, 1);
+        mbar_init(afull, ATM ? kEpiWarps : 1);
         mbar_init(done, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -306,8 +323,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (warp == kEpiWarps) {
         // ---------------- producer ----------------
         if (lane == 0) {
-            mbar_expect_tx(afull, a_bytes);
-            bulk_g2s(sA, jb.a_ops + size_t(tile) * a_bytes, a_bytes, afull);
+            if constexpr (!ATM) {
+                mbar_expect_tx(afull, a_bytes);
+                bulk_g2s(sA, jb.a_ops + size_t(tile) * a_bytes, a_bytes, afull);
+            }
             int issued = 0, xissued = 0;
             for (int i = 0; i < nch; ++i) {
                 const int s = i % stages, j = i % kXRing;
@@ -317,18 +336,18 @@ __global__ void __launch_bounds__(kThreads, 2)
                 bulk_g2s(sB + size_t(s) * b_stride, jb.b_ops + size_t(i) * b_bytes, b_bytes, &full[s]);
                 if (i >= kXRing && !mbar_wait(&xempty[j], ((i / kXRing) - 1) & 1, abort_flag, wait_ns)) break;
                 ++xissued;
-                mbar_expect_tx(&xfull[j], kBx * 4);
-                bulk_g2s(sX + size_t(j) * kBx, jb.bx + size_t(i) * kBx, kBx * 4, &xfull[j]);
+                mbar_expect_tx(&xfull[j], C::kBx * 4);
+                bulk_g2s(sX + size_t(j) * C::kBx, jb.bx + size_t(i) * C::kBx, C::kBx * 4, &xfull[j]);
             }
-            mbar_drain(afull, 0);
+            if constexpr (!ATM) mbar_drain(afull, 0);
             for (int i = max(0, issued - stages); i < issued; ++i) mbar_drain(&full[i % stages], (i / stages) & 1);
             for (int i = max(0, xissued - kXRing); i < xissued; ++i) mbar_drain(&xfull[i % kXRing], (i / kXRing) & 1);
         }
     } else if (warp == kEpiWarps + 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0 && nch > 0 && mbar_wait(afull, 0, abort_flag, wait_ns)) {
-            const uint32_t idesc = instr_desc<MODE>(kTileM, kChunkN);
-            const uint32_t lbo_a = kTileM * 16, lbo_b = kChunkN * 16;
+            const uint32_t idesc = instr_desc<MODE>(kTileM, CN);
+            const uint32_t lbo_a = kTileM * 16, lbo_b = CN * 16;
             const int ksteps = jb.Kp / T::kStepK; // 32 bytes of K per UMMA
             const int lo_off = jb.Kp / T::kChunk; // 16-byte K chunks to the lo half
             for (int i = 0; i < nch; ++i) {
@@ -337,16 +356,25 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if (i >= 2 && !mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1, abort_flag, wait_ns)) break;
                 tc_fence_after();
                 const uint8_t* b = sB + size_t(s) * b_stride;
-                const uint32_t d = tmem + uint32_t(buf * kChunkN);
+                const uint32_t d = tmem + uint32_t(buf * CN);
                 for (int kk = 0; kk < ksteps; ++kk) {
-                    const uint64_t ah = smem_desc(sA + size_t(2 * kk) * lbo_a, lbo_a, 128);
                     const uint64_t bh = smem_desc(b + size_t(2 * kk) * lbo_b, lbo_b, 128);
-                    umma<MODE>(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
-                    if constexpr (T::kSplit) {
-                        const uint64_t al = smem_desc(sA + size_t(lo_off + 2 * kk) * lbo_a, lbo_a, 128);
+                    if constexpr (ATM) {
+                        // A hi / lo of this K step: T::kStepK tensor-memory columns each
+                        const uint32_t ah = tmem + kAcol + uint32_t(kk * T::kStepK);
                         const uint64_t bl = smem_desc(b + size_t(lo_off + 2 * kk) * lbo_b, lbo_b, 128);
-                        umma<MODE>(d, ah, bl, idesc, 1u);
-                        umma<MODE>(d, al, bh, idesc, 1u);
+                        umma_ts<MODE>(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
+                        umma_ts<MODE>(d, ah, bl, idesc, 1u);
+                        umma_ts<MODE>(d, ah + uint32_t(jb.Kp), bh, idesc, 1u);
+                    } else {
+                        const uint64_t ah = smem_desc(sA + size_t(2 * kk) * lbo_a, lbo_a, 128);
+                        umma<MODE>(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
+                        if constexpr (T::kSplit) {
+                            const uint64_t al = smem_desc(sA + size_t(lo_off + 2 * kk) * lbo_a, lbo_a, 128);
+                            const uint64_t bl = smem_desc(b + size_t(lo_off + 2 * kk) * lbo_b, lbo_b, 128);
+                            umma<MODE>(d, ah, bl, idesc, 1u);
+                            umma<MODE>(d, al, bh, idesc, 1u);
+                        }
                     }
                 }
                 umma_commit(&tfull[buf]);
@@ -360,6 +388,25 @@ __global__ void __launch_bounds__(kThreads, 2)
     } else {
         // ---------------- epilogue ----------------
         const int q = warp & 3, h = warp >> 2;
+        if constexpr (ATM) {
+            // this warp's 32 rows of the packed sample tile (h = 0: hi half, 1: lo half) into its
+            // tensor-memory lanes, 8 columns (two 16-byte K chunks) per store; the MMA waits for all
+            const int r = q * 32 + lane;
+            const int nck = jb.Kp / T::kChunk;
+            const uint8_t* at = jb.a_ops + size_t(tile) * a_bytes + size_t(h * nck) * (kTileM * 16) + (r >> 3) * 128 +
+                                (r & 7) * 16;
+            const uint32_t tcol = tmem + (uint32_t(q * 32) << 16) + kAcol + uint32_t(h * jb.Kp);
+            for (int c = 0; c < nck; c += 2) {
+                const uint4 v0 = *reinterpret_cast<const uint4*>(at + size_t(c) * (kTileM * 16));
+                const uint4 v1 = *reinterpret_cast<const uint4*>(at + size_t(c + 1) * (kTileM * 16));
+                const uint32_t w[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+                tmem_st8(tcol + uint32_t(c * T::kChunk), w);
+            }
+            tmem_st_wait();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(afull);
+        }
         const int row = tile * kTileM + q * 32 + lane;
         const bool valid = row < jb.S;
         const float xn = valid ? jb.nrm_s[row] : 0.f;
@@ -379,26 +426,26 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (!mbar_wait(&xfull[j], (i / kXRing) & 1, abort_flag, wait_ns)) break;
             if (!mbar_wait(&tfull[buf], (i >> 1) & 1, abort_flag, wait_ns)) break;
             tc_fence_after();
-            const float* xs = sX + size_t(j) * kBx;
+            const float* xs = sX + size_t(j) * C::kBx;
             // can any pair of this chunk exceed the bound for a sample of this warp?  (warp-uniform)
-            const bool check = fix_scale<MODE>() > 0.f && fmaf(exn_max, xs[kBxGate], xs[kBxGate + 1]) > 1.f;
+            const bool check = fix_scale<MODE>() > 0.f && fmaf(exn_max, xs[C::kGate], xs[C::kGate + 1]) > 1.f;
 #pragma unroll 1
-            for (int cb = 0; cb < kChunkN / 2; cb += 32) {
-                const int col = h * (kChunkN / 2) + cb; // 32 columns = 16 pairs
+            for (int cb = 0; cb < CN / 2; cb += 32) {
+                const int col = h * (CN / 2) + cb; // 32 columns = 16 pairs
                 float gv[32];
-                tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * kChunkN + col), gv);
+                tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(buf * CN + col), gv);
                 if (!check) {
-                    epilogue_pairs16<false>(gv, xs, col >> 1, exn, m2, f0, f1);
+                    epilogue_pairs16<false, CN>(gv, xs, col >> 1, exn, m2, f0, f1);
                     continue;
                 }
-                uint32_t mask = epilogue_pairs16<true>(gv, xs, col >> 1, exn, m2, f0, f1);
+                uint32_t mask = epilogue_pairs16<true, CN>(gv, xs, col >> 1, exn, m2, f0, f1);
                 if (!valid) mask = 0u;
                 // flagged pairs: r = Re(y^H x), m = Im(y^H x) in FP32 from the samples themselves
                 while (mask) {
                     const int j = __ffs(mask) - 1;
                     mask &= mask - 1u;
                     const int pj = (col >> 1) + j;
-                    const float2* yb = jb.Yd + size_t(i * kChunkPairs + pj) * jb.Np;
+                    const float2* yb = jb.Yd + size_t(i * C::kPairs + pj) * jb.Np;
                     float re = 0.f, im = 0.f;
                     for (int k = 0; k < jb.N; ++k) {
                         const float2 x = jb.rx[size_t(k) * jb.S + row];
@@ -406,8 +453,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                         re = fmaf(y.x, x.x, fmaf(y.y, x.y, re));
                         im = fmaf(y.x, x.y, fmaf(-y.y, x.x, im));
                     }
-                    const float es = exn + xs[kBxNrm + pj];
-                    const float a0 = xs[kBxAw + 2 * pj], a1 = xs[kBxAw + 2 * pj + 1];
+                    const float es = exn + xs[C::kNrm + pj];
+                    const float a0 = xs[C::kAw + 2 * pj], a1 = xs[C::kAw + 2 * pj + 1];
                     const float kA = ex2(fminf(fmaf(m2, re, es), 0.f));
                     const float kP = ex2(fminf(fmaf(m2, im, es), 0.f));
                     const float kM = ex2(fminf(fmaf(-m2, im, es), 0.f));
@@ -441,11 +488,37 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (threadIdx.x == 0 && *abort_flag) atomicExch(err, 1);
 }
 
-template <int MODE> size_t gram_smem(int Kpmax, int stages)
+template <int MODE, int CN> size_t gram_smem(int Kpmax, int stages)
 {
-    return tile_bytes<MODE>(kTileM, Kpmax) + size_t(stages) * tile_bytes<MODE>(kChunkN, Kpmax) +
-           size_t(kXRing) * kBx * 4 + sizeof(uint64_t) * (2 * stages + 2 * kXRing + 6) + 16 + sizeof(float2) * kTileM +
-           1024;
+    return (Chunk<CN>::kAtm ? 0 : tile_bytes<MODE>(kTileM, Kpmax)) + size_t(stages) * tile_bytes<MODE>(CN, Kpmax) +
+           size_t(kXRing) * Chunk<CN>::kBx * 4 + sizeof(uint64_t) * (2 * stages + 2 * kXRing + 6) + 16 +
+           sizeof(float2) * kTileM + 1024;
+}
+
+template <int MODE, int CN>
+cudaError_t launch_cn(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks, const int* d_tile_prefix,
+                      int total_tiles, int Kp, float wL, float wG, int* d_err, int stages_req, cudaStream_t s)
+{
+    // the tile's samples in shared memory: N <= Kp / 2 antennas
+    if (max_tiles > 0)
+        batch_gram_pack_a_kernel<MODE><<<dim3(max_tiles, n_jobs), 256, sizeof(float2) * kTileM * (Kp / 2 + 1), s>>>(
+            d_jobs, wL);
+    if (max_chunks > 0) batch_gram_pack_b_kernel<MODE, CN><<<dim3(max_chunks, n_jobs), 256, 0, s>>>(d_jobs, wG);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || total_tiles <= 0) return e;
+    // two pipeline stages when that lets two CTAs share an SM, else three if they fit
+    // (stages_req 2 or 3 overrides the choice where that many fit)
+    constexpr size_t kSmemMax = 227 * 1024;
+    int stages = (2 * gram_smem<MODE, CN>(Kp, 3) > kSmemMax) ? 2 : 3;
+    if (stages_req == 2 || (stages_req == 3 && gram_smem<MODE, CN>(Kp, 3) <= kSmemMax)) stages = stages_req;
+    // every CTA holds 256 TMEM columns: at most two CTAs per SM (512 columns), so
+    // shared memory is padded to more than a third of the SM's
+    const size_t smem = std::max<size_t>(gram_smem<MODE, CN>(Kp, stages), 80 * 1024);
+    e = cudaFuncSetAttribute(batch_gram_kernel<MODE, CN>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    batch_gram_kernel<MODE, CN><<<total_tiles, kThreads, smem, s>>>(d_jobs, n_jobs, d_tile_prefix, Kp, stages, d_err,
+                                                                    wait_limit_ns());
+    return cudaGetLastError();
 }
 
 template <int MODE>
@@ -454,31 +527,19 @@ cudaError_t launch_mode(const BatchGramJob* d_jobs, int n_jobs, int max_tiles, i
                         int stages_req, cudaStream_t s)
 {
     if (Kp % OpTraits<MODE>::kStepK != 0 || Kp > 64) return cudaErrorInvalidValue;
-    // the tile's samples in shared memory: N <= Kp / 2 antennas
-    if (max_tiles > 0)
-        batch_gram_pack_a_kernel<MODE><<<dim3(max_tiles, n_jobs), 256, sizeof(float2) * kTileM * (Kp / 2 + 1), s>>>(
-            d_jobs, wL);
-    if (max_chunks > 0) batch_gram_pack_b_kernel<MODE><<<dim3(max_chunks, n_jobs), 256, 0, s>>>(d_jobs, wG);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || total_tiles <= 0) return e;
-    // two pipeline stages when that lets two CTAs share an SM, else three if they fit
-    // (stages_req 2 or 3 overrides the choice where that many fit)
-    int stages = (2 * gram_smem<MODE>(Kp, 3) > 227 * 1024) ? 2 : 3;
-    if (stages_req == 2 || (stages_req == 3 && gram_smem<MODE>(Kp, 3) <= 227 * 1024)) stages = stages_req;
-    // every CTA holds 256 TMEM columns: at most two CTAs per SM (512 columns), so
-    // shared memory is padded to more than a third of the SM's
-    const size_t smem = std::max<size_t>(gram_smem<MODE>(Kp, stages), 80 * 1024);
-    e = cudaFuncSetAttribute(batch_gram_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    batch_gram_kernel<MODE><<<total_tiles, kThreads, smem, s>>>(d_jobs, n_jobs, d_tile_prefix, Kp, stages, d_err,
-                                                                wait_limit_ns());
-    return cudaGetLastError();
+    if constexpr (MODE == kTF32x3) {
+        if (chunk_cols(MODE, Kp) == 64)
+            return launch_cn<MODE, 64>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG,
+                                       d_err, stages_req, s);
+    }
+    return launch_cn<MODE, 128>(d_jobs, n_jobs, max_tiles, max_chunks, d_tile_prefix, total_tiles, Kp, wL, wG, d_err,
+                                stages_req, s);
 }
 
 } // namespace
 
 int batch_gram_tile() { return kTileM; }
-int batch_gram_chunk_pairs() { return kChunkPairs; }
+int batch_gram_chunk_pairs(int mode, int Kp) { return chunk_cols(mode, Kp) / 2; }
 int batch_gram_kp(int mode, int N)
 {
     const int step = (mode == kTF32 || mode == kTF32x3) ? tc::OpTraits<kTF32>::kStepK : tc::OpTraits<kBF16>::kStepK;
@@ -491,9 +552,9 @@ size_t batch_gram_a_bytes(int mode, int Kp)
 }
 size_t batch_gram_b_bytes(int mode, int Kp)
 {
-    return batch_gram_a_bytes(mode, Kp) / kTileM * kChunkN;
+    return batch_gram_a_bytes(mode, Kp) / kTileM * chunk_cols(mode, Kp);
 }
-size_t batch_gram_bx_floats() { return kBx; }
+size_t batch_gram_bx_floats(int mode, int Kp) { return 2 * chunk_cols(mode, Kp) + 4; }
 
 cudaError_t launch_batch_gram(int mode, const BatchGramJob* d_jobs, int n_jobs, int max_tiles, int max_chunks,
                               const int* d_tile_prefix, int total_tiles, int Kp, float wL, float wG, int* d_err,
