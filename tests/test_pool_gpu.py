@@ -354,14 +354,15 @@ def test_pool_pageable_detection_samples_staged_while_training(native_lib):
     """A batch that trains and detects from ordinary (pageable) buffers with >= 4 MB of
     detection samples stages and uploads them per detection segment while it trains; the
     estimates equal those of the same training and detection run as two batches (the second
-    one stages everything before its upload)."""
+    one stages everything before its upload).  The 48-antenna detectors run the CUDA-core
+    detection (a segment of its own) beside the tensor-core classes."""
     from libapsm_b200 import DetectorPool, PoolJob
 
-    frames = [(N,) + _frame(800 + i, N, 300, 6000) for i, N in enumerate([4, 8, 16, 32])]
+    frames = [(N,) + _frame(800 + i, N, 300, 6000) for i, N in enumerate([4, 8, 16, 32, 48])]
     outs = {}
     for mode in ("one batch", "two batches"):
         pool = DetectorPool(dict(CFG, detectVersion="gram_tf32x3"))
-        dets = [(pool.add(f[0]), f) for _ in range(4) for f in frames]  # 16 detectors, 11.5 MB of samples
+        dets = [(pool.add(f[0]), f) for _ in range(4) for f in frames]  # 20 detectors, 20.7 MB of samples
         train = [PoolJob(d, f[1], f[2], fresh=True) for d, f in dets]
         detect = [PoolJob(d, f[3]) for d, f in dets]
         if mode == "one batch":
