@@ -55,7 +55,9 @@ def test_pool_matches_oracle_per_detector(native_lib, oracle_mod, cfg):
     from libapsm_b200 import DetectorPool, PoolJob
 
     pool = DetectorPool(cfg)
-    specs = [(3, 120, 200), (4, 300, 96), (8, 60, 50), (16, 250, 300), (2, 31, 17), (32, 150, 128)]
+    # (24 and 28 antennas: 48 / 56 features, the widest class's 32-pair chunks at K below 64)
+    specs = [(3, 120, 200), (4, 300, 96), (8, 60, 50), (16, 250, 300), (2, 31, 17), (32, 150, 128), (24, 90, 140),
+             (28, 70, 61)]
     dets, jobs, frames = [], [], []
     for i, (N, P, S) in enumerate(specs):
         d = pool.add(N)
@@ -88,7 +90,8 @@ def test_pool_gram_forms_match_oracle(native_lib, oracle_mod, dv, narrow):
     if narrow:
         cfg.update(windowSize=80, dictionarySize=2000, gaussianKernelVariance=0.05, eB=0.001)
     pool = DetectorPool(cfg)
-    specs = [(3, 120, 200), (4, 300, 96), (8, 60, 50), (16, 250, 300), (2, 31, 17), (32, 150, 128)]
+    specs = [(3, 120, 200), (4, 300, 96), (8, 60, 50), (16, 250, 300), (2, 31, 17), (32, 150, 128), (24, 90, 140),
+             (28, 70, 61)]
     dets, frames = [], []
     for i, (N, P, S) in enumerate(specs):
         dets.append(pool.add(N))
